@@ -1,0 +1,109 @@
+/*
+ * loop_tool_b200: C ABI of the B200 (sm_100a) "cuda" backend for loop_tool.
+ *
+ * The boundary is the reference plugin surface, loop_tool's
+ * include/loop_tool/backend.h: a Backend compiles a LoopTree into a
+ * Compiled, whose run(memory, sync) executes it over caller-owned buffers.
+ * A LoopTree crosses this ABI as the text serialize() writes
+ * (src/core/serialization.cpp:175-237): the IR, its per-node loop orders
+ * (splits, tails), reuse flags and loop annotations, from which the
+ * reference rebuilds the identical LoopTree (include/loop_tool/ir.h:402).
+ *
+ * Conventions (same as the reference):
+ *  - memory[] = [inputs in IR input order..., outputs in IR output order...]
+ *    as float* (src/core/compile.cpp:506-525).  Pointers may be device,
+ *    managed or plain host memory; host buffers are staged through HBM.
+ *  - scratch is owned by the compiled object (src/backends/cpu/cpp.cpp:482).
+ *  - errors: the reference throws std::runtime_error through ASSERT
+ *    (include/loop_tool/error.h:47-61); here every call returns a status and
+ *    ltb_last_error() holds the message for the calling thread.
+ */
+#ifndef LOOP_TOOL_B200_H_
+#define LOOP_TOOL_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LTB_OK 0
+#define LTB_ERR_INVALID 1      /* malformed IR text or bad argument */
+#define LTB_ERR_UNSUPPORTED 2  /* IR outside what the backend lowers */
+#define LTB_ERR_CUDA 3         /* CUDA runtime / launch failure */
+#define LTB_ERR_NO_DEVICE 4    /* no usable sm_100 device */
+#define LTB_ERR_TIMEOUT 5      /* a bounded device wait gave up */
+
+typedef struct ltb_compiled ltb_compiled;
+
+/* ABI version (increments on incompatible change). */
+int ltb_abi_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* ltb_last_error(void);
+
+/* Number of visible sm_100 devices.  The reference registers its "cuda"
+ * backend and hardware only when a device is present
+ * (src/backends/cuda/cuda.cpp:1030-1041); callers do the same with this. */
+int ltb_device_count(void);
+
+/* Lowering only, no device needed: writes the kernel plan chosen for the
+ * serialized LoopTree into buf (NUL-terminated, truncated to len).
+ * Replaces the host-side analysis of cuda_code_and_dispatch /
+ * calc_cuda_aux (src/backends/cuda/cuda.cpp:776-792, 973-1028).
+ * options: "precision=fp32|bf16|bf16x3;fuse_rows=0|1;tensor_cores=0|1". */
+int ltb_plan(const char* ir_text, const char* options, char* buf, size_t len);
+
+/* Backend::compile(const LoopTree&) (include/loop_tool/backend.h:62-67),
+ * i.e. CudaBackend::compile_impl (src/backends/cuda/cuda.cpp:875-879):
+ * lowers the serialized LoopTree, uploads kernel descriptors and allocates
+ * scratch on the current device. */
+int ltb_compile(const char* ir_text, const char* options, ltb_compiled** out);
+
+/* Compiled::run(const std::vector<void*>& memory, bool sync)
+ * (include/loop_tool/backend.h:20-21; CudaCompiled::run,
+ * src/backends/cuda/cuda.cpp:837-850).  stream: a cudaStream_t or NULL for
+ * the legacy default stream.  With sync == 0 the call returns after
+ * enqueueing (Compiled::async, backend.h:41-44); host buffers force sync. */
+int ltb_run(ltb_compiled* c, void* const* memory, int n, int sync,
+            void* stream);
+
+/* Like ltb_run with caller-provided scratch (ltb_int_property
+ * "scratch_bytes" bytes, 256-byte aligned device memory), so concurrent runs
+ * of one compiled object on different streams do not share scratch. */
+int ltb_run_with_scratch(ltb_compiled* c, void* const* memory, int n,
+                         int sync, void* stream, void* scratch);
+
+/* Compiled destructor. */
+int ltb_release(ltb_compiled* c);
+
+/* Compiled::dump() / string_properties["code"]
+ * (src/backends/cuda/cuda.cpp:970): the kernel plan, not PTX. */
+int ltb_dump(ltb_compiled* c, char* buf, size_t len);
+
+/* Compiled::int_properties (src/backends/cuda/cuda.cpp:960-969):
+ * "bandwidth" (theoretical GB/s, 2*memclk*buswidth/8 as the reference
+ * computes it), plus "stages", "launches", "scratch_bytes", "inputs",
+ * "outputs", "algorithmic_bytes", "flops". */
+int ltb_int_property(ltb_compiled* c, const char* name, int64_t* value);
+
+/* Element counts of the I/O buffers: elems[0..n_in+n_out). */
+int ltb_io_sizes(ltb_compiled* c, int* n_in, int* n_out, int64_t* elems,
+                 int cap);
+
+/* Hardware "cuda" (CudaGPUHardware, src/backends/cuda/cuda.cpp:800-816):
+ * alloc with managed != 0 is cudaMallocManaged like the reference (CPU
+ * compatible); managed == 0 is plain device memory. */
+int ltb_alloc(size_t bytes, int managed, void** out);
+int ltb_free(void* ptr);
+
+/* Stream synchronisation helper (cuCtxSynchronize in the reference,
+ * src/backends/cuda/cuda.cpp:847-849, when stream is NULL). */
+int ltb_synchronize(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOOP_TOOL_B200_H_ */

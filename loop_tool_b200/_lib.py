@@ -1,0 +1,77 @@
+"""ctypes binding of libloop_tool_b200.so (the C ABI in include/loop_tool_b200.h).
+
+The shared library is built in-tree (loop_tool_b200/_lib/) by
+``python -m loop_tool_b200.build``.  Importing this module without it raises:
+there is no CPU fallback for the CUDA path.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libloop_tool_b200.so")
+
+OK = 0
+ERR_INVALID = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_NO_DEVICE = 4
+ERR_TIMEOUT = 5
+
+# every symbol include/loop_tool_b200.h declares, with its ctypes signature
+SIGNATURES = {
+    "ltb_abi_version": (ctypes.c_int, []),
+    "ltb_last_error": (ctypes.c_char_p, []),
+    "ltb_device_count": (ctypes.c_int, []),
+    "ltb_plan": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "ltb_compile": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "ltb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                               ctypes.c_int, ctypes.c_void_p]),
+    "ltb_run_with_scratch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+    "ltb_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "ltb_dump": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "ltb_int_property": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p,
+                                        ctypes.POINTER(ctypes.c_int64)]),
+    "ltb_io_sizes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64),
+                                    ctypes.c_int]),
+    "ltb_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "ltb_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "ltb_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+}
+
+
+class LoopToolError(RuntimeError):
+    """Raised for every failed call, like the reference's ASSERT throwing
+    std::runtime_error (include/loop_tool/error.h:47-61)."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build the CUDA extension with "
+                "`python -m loop_tool_b200.build` (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != OK:
+        msg = lib().ltb_last_error().decode(errors="replace")
+        raise LoopToolError(rc, msg)
+    return rc

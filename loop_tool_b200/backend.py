@@ -1,0 +1,177 @@
+"""Host-side mirror of the reference's backend plugin surface.
+
+Reference: include/loop_tool/backend.h (Backend::compile -> Compiled,
+Compiled::run(memory, sync)), and the Python binding src/frontends/python.cpp
+where each registered backend becomes ``lt.<name>(loop_tree)`` (:208-218) and
+``Compiled.__call__`` runs it on a list of tensors (:182-196).
+
+Here the loop tree crosses the C ABI as serialized IR text; ``cuda`` accepts
+that text, an object with ``serialize()`` (this package's IR / LoopTree) or
+a lazy Tensor.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+_OPT_KEYS = ("precision", "fuse_rows", "tensor_cores", "kahan_threshold")
+
+
+def _options(opts):
+    parts = []
+    for k, v in opts.items():
+        if k not in _OPT_KEYS:
+            raise ValueError(f"unknown option {k}")
+        if isinstance(v, bool):
+            v = int(v)
+        parts.append(f"{k}={v}")
+    return ";".join(parts).encode()
+
+
+def _ir_text(obj):
+    if isinstance(obj, str):
+        return obj
+    if isinstance(obj, bytes):
+        return obj.decode()
+    if hasattr(obj, "serialize"):
+        return obj.serialize()
+    raise TypeError(f"cannot take a loop tree from {type(obj).__name__}")
+
+
+def plan(loop_tree, **opts):
+    """The kernel plan for a loop tree, computed on the host (no device)."""
+    buf = ctypes.create_string_buffer(1 << 20)
+    _lib.check(_lib.lib().ltb_plan(_ir_text(loop_tree).encode(), _options(opts), buf, len(buf)))
+    return buf.value.decode()
+
+
+def device_count():
+    return _lib.lib().ltb_device_count()
+
+
+def _ptr_and_keep(t):
+    """Raw pointer of a buffer-like; returns (ptr, keepalive, host_array)."""
+    if hasattr(t, "data_ptr"):  # torch.Tensor
+        if t.dtype.__repr__() != "torch.float32":
+            raise TypeError("loop_tool buffers are float32")
+        if not t.is_contiguous():
+            raise ValueError("buffers must be contiguous")
+        return t.data_ptr(), t, None
+    if isinstance(t, RawTensor):
+        return t.ptr, t, None
+    if isinstance(t, np.ndarray):
+        if t.dtype != np.float32 or not t.flags.c_contiguous:
+            raise TypeError("numpy buffers must be contiguous float32")
+        return t.ctypes.data, t, t
+    if isinstance(t, int):
+        return t, None, None
+    raise TypeError(f"unsupported buffer type {type(t).__name__}")
+
+
+class Compiled:
+    """A loop tree compiled for the B200 (CudaCompiled, cuda.cpp:818-851)."""
+
+    def __init__(self, loop_tree, **opts):
+        self.ir_text = _ir_text(loop_tree)
+        self.options = dict(opts)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ltb_compile(self.ir_text.encode(), _options(opts), ctypes.byref(h)))
+        self._h = h
+        n_in, n_out = ctypes.c_int(), ctypes.c_int()
+        elems = (ctypes.c_int64 * 256)()
+        _lib.check(_lib.lib().ltb_io_sizes(h, ctypes.byref(n_in), ctypes.byref(n_out), elems, 256))
+        self.n_inputs, self.n_outputs = n_in.value, n_out.value
+        self.io_sizes = [elems[i] for i in range(self.n_inputs + self.n_outputs)]
+        self.name = "cuda"
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib._lib is not None:
+            _lib.lib().ltb_release(h)
+            self._h = None
+
+    # Compiled::run(memory, sync)
+    def run(self, memory, sync=True, stream=None, scratch=None):
+        ptrs, keep = [], []
+        for t in memory:
+            p, k, _ = _ptr_and_keep(t)
+            ptrs.append(p)
+            keep.append(k)
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        if stream is None:
+            stream = _current_stream()
+        if scratch is None:
+            rc = _lib.lib().ltb_run(self._h, arr, len(ptrs), int(bool(sync)), stream)
+        else:
+            rc = _lib.lib().ltb_run_with_scratch(self._h, arr, len(ptrs), int(bool(sync)),
+                                                 stream, scratch)
+        _lib.check(rc)
+
+    def __call__(self, tensors, sync=True):
+        self.run(tensors, sync)
+
+    def int_property(self, name):
+        v = ctypes.c_int64()
+        _lib.check(_lib.lib().ltb_int_property(self._h, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    @property
+    def int_properties(self):
+        keys = ("bandwidth", "stages", "launches", "scratch_bytes", "inputs", "outputs",
+                "algorithmic_bytes", "flops")
+        return {k: self.int_property(k) for k in keys}
+
+    @property
+    def string_properties(self):
+        return {"code": self.code}
+
+    @property
+    def code(self):
+        buf = ctypes.create_string_buffer(1 << 20)
+        _lib.check(_lib.lib().ltb_dump(self._h, buf, len(buf)))
+        return buf.value.decode()
+
+    def dump(self):
+        return self.code
+
+    def __getattr__(self, name):  # python.cpp:197-207 exposes properties
+        if name.startswith("_"):
+            raise AttributeError(name)
+        if name in ("bandwidth", "stages", "launches", "scratch_bytes", "flops",
+                    "algorithmic_bytes"):
+            return self.int_property(name)
+        raise AttributeError(name)
+
+
+def _current_stream():
+    try:
+        import torch
+
+        if torch.cuda.is_available() and torch.cuda.is_initialized():
+            return torch.cuda.current_stream().cuda_stream
+    except Exception:
+        pass
+    return None
+
+
+def cuda(loop_tree, **opts):
+    """lt.cuda(loop_tree) -> Compiled (python.cpp:208-218)."""
+    return Compiled(loop_tree, **opts)
+
+
+class RawTensor:
+    """Device buffer from the backend's "cuda" hardware allocator
+    (CudaGPUHardware::alloc/free, cuda.cpp:800-816)."""
+
+    def __init__(self, size, managed=False):
+        self.size = int(size)
+        p = ctypes.c_void_p()
+        _lib.check(_lib.lib().ltb_alloc(max(self.size, 1) * 4, int(managed), ctypes.byref(p)))
+        self.ptr = p.value
+        self.managed = managed
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _lib._lib is not None:
+            _lib.lib().ltb_free(self.ptr)
+            self.ptr = None

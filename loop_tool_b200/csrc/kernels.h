@@ -1,0 +1,46 @@
+// Host-side launchers of the sm_100a kernel families.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "stage.h"
+
+// (a) elementwise nests and (b) serial reductions
+cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
+                            const LtbBufTable& bt, int sms, cudaStream_t st);
+// (b) block-parallel reductions; splits > 1 writes split-K partials to the
+// stage's partial buffer and combines them in order
+cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,
+                              const LtbBufTable& bt, int splits, int sms,
+                              cudaStream_t st);
+// (b) fused per-row chain of stages (d_stages contiguous, final one
+// elementwise)
+cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, int nsteps,
+                                 const LtbStage& final_stage,
+                                 const LtbBufTable& bt, int sms,
+                                 cudaStream_t st);
+
+// (c) contractions.  Operand element (i, k) of A lives at
+// a_rowoff[i] + a_koff[k] (B: b_rowoff[j] + b_koff[k]); guards are kept as
+// per-row / per-k partial sums so padded convolutions gather implicitly.
+struct LtbGemmOperand {
+  const float* base;
+  const int64_t* rowoff;  // [rows]
+  const int64_t* koff;    // [K]
+  int nguard;
+  const int32_t* grow;    // [nguard][rows] guard partial from the row coords
+  const int32_t* gk;      // [nguard][K]   guard partial from the k coords
+  const int32_t* gub;     // [nguard]      valid iff 0 <= grow + gk < gub
+};
+
+struct LtbGemmProblem {
+  LtbGemmOperand a, b;
+  float* c;
+  const int64_t* crow;  // [M] output offset per row
+  const int64_t* ccol;  // [N] output offset per column
+  int64_t M, N, K;
+};
+
+// FP32 CUDA-core path (exact fp32 FMA): the "plain FP32" baseline family.
+cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms,
+                                 cudaStream_t st);

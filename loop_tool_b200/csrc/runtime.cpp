@@ -1,0 +1,503 @@
+// C ABI of the B200 backend: compile (lower + upload), run (launch the plan
+// on a stream), properties, and the "cuda" hardware allocator.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/loop_tool_b200.h"
+#include "kernels.h"
+#include "lower.hpp"
+
+static_assert(sizeof(LtbStage) % 16 == 0, "stage descriptor must be 16B-sized");
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                     \
+  do {                                                                     \
+    cudaError_t _e = (expr);                                               \
+    if (_e != cudaSuccess)                                                 \
+      throw CudaFailure(std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+struct CudaFailure : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+ltb::LowerOptions parse_options(const char* s) {
+  ltb::LowerOptions o;
+  if (!s) return o;
+  std::istringstream ss(s);
+  for (std::string kv; std::getline(ss, kv, ';');) {
+    auto p = kv.find('=');
+    if (p == std::string::npos) continue;
+    auto k = kv.substr(0, p), v = kv.substr(p + 1);
+    if (k == "precision") {
+      if (v == "fp32") o.precision = ltb::Precision::fp32;
+      else if (v == "bf16") o.precision = ltb::Precision::bf16;
+      else if (v == "bf16x3") o.precision = ltb::Precision::bf16x3;
+      else throw ltb::Error("unknown precision '" + v + "'");
+    } else if (k == "fuse_rows") {
+      o.fuse_rows = v != "0";
+    } else if (k == "tensor_cores") {
+      o.use_tensor_cores = v != "0";
+    } else if (k == "kahan_threshold") {
+      o.kahan_threshold = std::stoi(v);
+    } else {
+      throw ltb::Error("unknown option '" + k + "'");
+    }
+  }
+  return o;
+}
+
+struct GemmTables {
+  int stage = -1;
+  int64_t nbatch = 1;
+  std::vector<int64_t> a_boff, b_boff, c_boff;  // per batch
+  int64_t *a_row = nullptr, *a_k = nullptr, *b_row = nullptr, *b_k = nullptr;
+  int64_t *c_row = nullptr, *c_col = nullptr;
+  int32_t *ag_row = nullptr, *ag_k = nullptr, *ag_ub = nullptr;
+  int32_t *bg_row = nullptr, *bg_k = nullptr, *bg_ub = nullptr;
+  int a_ng = 0, b_ng = 0;
+};
+
+template <typename T>
+T* upload(const std::vector<T>& v, std::vector<void*>& owned) {
+  if (v.empty()) return nullptr;
+  void* p = nullptr;
+  CUDA_TRY(cudaMalloc(&p, v.size() * sizeof(T)));
+  CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  owned.push_back(p);
+  return static_cast<T*>(p);
+}
+
+}  // namespace
+
+struct ltb_compiled {
+  std::string ir_text;
+  ltb::IRGraph ir;
+  ltb::Plan plan;
+  ltb::LowerOptions opt;
+  int device = 0;
+  int sms = 148;
+  LtbStage* d_stages = nullptr;
+  std::vector<int> split_of;          // per stage split count
+  std::vector<size_t> scratch_off;    // byte offsets within scratch block
+  size_t scratch_bytes = 0;
+  void* scratch = nullptr;            // default scratch block
+  std::vector<GemmTables> gemms;      // per contraction stage
+  std::vector<int> gemm_of;           // stage -> index into gemms (or -1)
+  std::vector<void*> owned;           // device allocations to free
+  std::mutex mu;                      // guards the default scratch block
+  int64_t bandwidth_gbs = 0;
+  int launches = 0;
+};
+
+namespace {
+
+int64_t stage_outs(const LtbStage& d) {
+  int64_t o = 1;
+  for (int k = 0; k < d.nout; ++k) o *= d.size[k];
+  return o;
+}
+
+// Split a contraction's affine operand loads into per-row / per-k tables.
+void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
+  const ltb::PlanStage& ps = c->plan.stages[si];
+  const LtbStage& d = ps.dev;
+  const ltb::Contraction& con = ps.con;
+  auto dim_of = [&](int var) {
+    auto it = std::find(ps.dim_vars.begin(), ps.dim_vars.end(), var);
+    return (int)(it - ps.dim_vars.begin());
+  };
+  std::vector<int> bd, md, nd, kd;
+  for (int v : con.bvars) bd.push_back(dim_of(v));
+  for (int v : con.mvars) md.push_back(dim_of(v));
+  for (int v : con.nvars) nd.push_back(dim_of(v));
+  for (int v : con.kvars) kd.push_back(dim_of(v));
+  // enumerate a role's coordinates row-major and evaluate coef . x
+  auto table = [&](const std::vector<int>& dims, const int64_t* coef,
+                   int64_t off) {
+    int64_t n = 1;
+    for (int k : dims) n *= d.size[k];
+    std::vector<int64_t> out(n);
+    std::vector<int64_t> x(dims.size(), 0);
+    for (int64_t i = 0; i < n; ++i) {
+      int64_t v = off;
+      for (size_t q = 0; q < dims.size(); ++q) v += coef[dims[q]] * x[q];
+      out[i] = v;
+      for (int q = (int)dims.size() - 1; q >= 0; --q) {
+        if (++x[q] < d.size[dims[q]]) break;
+        x[q] = 0;
+      }
+    }
+    return out;
+  };
+  const LtbLoad& A = d.loads[con.a_load];
+  const LtbLoad& B = d.loads[con.b_load];
+  for (int g = A.g0; g < A.g0 + A.ng; ++g)
+    for (int k : bd)
+      if (d.guards[g].coef[k]) throw ltb::Error("guard over batch dims");
+  t.a_boff = table(bd, A.coef, 0);
+  t.b_boff = table(bd, B.coef, 0);
+  t.c_boff = table(bd, d.out_coef, 0);
+  t.nbatch = (int64_t)t.a_boff.size();
+  t.a_row = upload(table(md, A.coef, A.off), c->owned);
+  t.a_k = upload(table(kd, A.coef, 0), c->owned);
+  t.b_row = upload(table(nd, B.coef, B.off), c->owned);
+  t.b_k = upload(table(kd, B.coef, 0), c->owned);
+  t.c_row = upload(table(md, d.out_coef, d.out_off), c->owned);
+  t.c_col = upload(table(nd, d.out_coef, 0), c->owned);
+  auto guards = [&](const LtbLoad& L, const std::vector<int>& rd,
+                    int32_t** grow, int32_t** gk, int32_t** gub, int* ng) {
+    std::vector<int32_t> vr, vk, vu;
+    for (int g = L.g0; g < L.g0 + L.ng; ++g) {
+      const LtbGuard& G = d.guards[g];
+      for (auto v : table(rd, G.coef, G.off)) vr.push_back((int32_t)v);
+      for (auto v : table(kd, G.coef, 0)) vk.push_back((int32_t)v);
+      vu.push_back((int32_t)G.ub);
+    }
+    *ng = L.ng;
+    *grow = upload(vr, c->owned);
+    *gk = upload(vk, c->owned);
+    *gub = upload(vu, c->owned);
+  };
+  guards(A, md, &t.ag_row, &t.ag_k, &t.ag_ub, &t.a_ng);
+  guards(B, nd, &t.bg_row, &t.bg_k, &t.bg_ub, &t.b_ng);
+}
+
+void compile_device(ltb_compiled* c) {
+  CUDA_TRY(cudaGetDevice(&c->device));
+  CUDA_TRY(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device));
+  int memclk_khz = 0, bus_bits = 0;
+  cudaDeviceGetAttribute(&memclk_khz, cudaDevAttrMemoryClockRate, c->device);
+  cudaDeviceGetAttribute(&bus_bits, cudaDevAttrGlobalMemoryBusWidth, c->device);
+  cudaGetLastError();
+  c->bandwidth_gbs = (int64_t)(2.0 * memclk_khz * 1e3 * (bus_bits / 8) / 1e9);
+  auto& P = c->plan;
+  const int ns = (int)P.stages.size();
+  c->split_of.assign(ns, 1);
+  c->gemm_of.assign(ns, -1);
+  for (int i = 0; i < ns; ++i) {
+    auto& st = P.stages[i];
+    if (st.family == ltb::Family::reduce_split) {
+      const int64_t outs = stage_outs(st.dev);
+      int64_t splits = (4LL * c->sms + outs - 1) / outs;
+      splits = std::min<int64_t>(splits, std::max<int64_t>(1, st.dev.red_total / 4096));
+      splits = std::max<int64_t>(1, std::min<int64_t>(splits, 2048));
+      c->split_of[i] = (int)splits;
+      st.dev.split = (int)splits;
+      st.dev.partial_buf = P.num_slots();
+      P.scratch_elems.push_back(outs * splits);
+    } else {
+      st.dev.split = 1;
+    }
+  }
+  // scratch: one block, every slot 256-byte aligned
+  c->scratch_off.clear();
+  size_t off = 0;
+  for (auto e : P.scratch_elems) {
+    c->scratch_off.push_back(off);
+    off += ((size_t)std::max<int64_t>(e, 1) * 4 + 255) / 256 * 256;
+  }
+  c->scratch_bytes = off;
+  if (off) {
+    CUDA_TRY(cudaMalloc(&c->scratch, off));
+    c->owned.push_back(c->scratch);
+  }
+  std::vector<LtbStage> hs;
+  for (auto& st : P.stages) hs.push_back(st.dev);
+  if (!hs.empty()) c->d_stages = upload(hs, c->owned);
+  for (int i = 0; i < ns; ++i) {
+    if (P.stages[i].family != ltb::Family::contraction) continue;
+    GemmTables t;
+    t.stage = i;
+    build_gemm(c, i, t);
+    c->gemm_of[i] = (int)c->gemms.size();
+    c->gemms.push_back(t);
+  }
+  int launches = 0;
+  for (int i = 0; i < ns; ++i) {
+    auto& st = P.stages[i];
+    if (st.family == ltb::Family::row_chain) {
+      if (st.rows_from == i) launches++;
+    } else if (st.family == ltb::Family::contraction) {
+      launches += (int)c->gemms[c->gemm_of[i]].nbatch;
+    } else {
+      launches += c->split_of[i] > 1 ? 2 : 1;
+    }
+  }
+  c->launches = launches;
+}
+
+bool is_device_accessible(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
+  auto& P = c->plan;
+  const int ns = (int)P.stages.size();
+  for (int i = 0; i < ns; ++i) {
+    const auto& s = P.stages[i];
+    const LtbStage* d = c->d_stages + i;
+    cudaError_t e = cudaSuccess;
+    switch (s.family) {
+      case ltb::Family::elementwise:
+      case ltb::Family::reduce_serial:
+        e = ltb_launch_nest(d, s.dev, bt, c->sms, st);
+        break;
+      case ltb::Family::reduce_parallel:
+      case ltb::Family::reduce_split:
+        e = ltb_launch_reduce(d, s.dev, bt, c->split_of[i], c->sms, st);
+        break;
+      case ltb::Family::row_chain: {
+        if (s.rows_from != i) break;
+        int n = 0;
+        while (i + n < ns && P.stages[i + n].family == ltb::Family::row_chain &&
+               P.stages[i + n].rows_from == i)
+          n++;
+        e = ltb_launch_row_chain(d, n, P.stages[i + n - 1].dev, bt, c->sms, st);
+        break;
+      }
+      case ltb::Family::contraction: {
+        const GemmTables& t = c->gemms[c->gemm_of[i]];
+        for (int64_t b = 0; b < t.nbatch && e == cudaSuccess; ++b) {
+          LtbGemmProblem p{};
+          const LtbLoad& A = s.dev.loads[s.con.a_load];
+          const LtbLoad& B = s.dev.loads[s.con.b_load];
+          p.a = {bt.p[A.buf] + t.a_boff[b], t.a_row, t.a_k, t.a_ng, t.ag_row, t.ag_k, t.ag_ub};
+          p.b = {bt.p[B.buf] + t.b_boff[b], t.b_row, t.b_k, t.b_ng, t.bg_row, t.bg_k, t.bg_ub};
+          p.c = bt.p[s.dev.out_buf] + t.c_boff[b];
+          p.crow = t.c_row;
+          p.ccol = t.c_col;
+          p.M = s.con.M;
+          p.N = s.con.N;
+          p.K = s.con.K;
+          e = ltb_launch_gemm_simt(p, c->sms, st);
+        }
+        break;
+      }
+    }
+    if (e != cudaSuccess)
+      throw CudaFailure(std::string("launch of stage ") + std::to_string(i) +
+                        " (" + s.text + "): " + cudaGetErrorString(e));
+  }
+}
+
+int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
+             void* stream, void* scratch) {
+  if (!c) return fail(LTB_ERR_INVALID, "null compiled object");
+  auto& P = c->plan;
+  if (n != P.n_in + P.n_out)
+    return fail(LTB_ERR_INVALID, "expected " + std::to_string(P.n_in + P.n_out) +
+                                     " buffers, got " + std::to_string(n));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::unique_lock<std::mutex> lock(c->mu, std::defer_lock);
+  if (!scratch) {
+    lock.lock();
+    scratch = c->scratch;
+  }
+  LtbBufTable bt{};
+  if (P.num_slots() > LTB_MAXBUF)
+    return fail(LTB_ERR_UNSUPPORTED, "too many buffers for one launch table");
+  std::vector<std::pair<int, void*>> staged;  // slot, host pointer
+  std::vector<void*> temps;
+  try {
+    CUDA_TRY(cudaSetDevice(c->device));
+    for (int i = 0; i < n; ++i) {
+      if (!memory[i]) return fail(LTB_ERR_INVALID, "null buffer " + std::to_string(i));
+      if (is_device_accessible(memory[i])) {
+        bt.p[i] = static_cast<float*>(memory[i]);
+        continue;
+      }
+      const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[i], 1) * 4;
+      void* d = nullptr;
+      CUDA_TRY(cudaMallocAsync(&d, bytes, st));
+      temps.push_back(d);
+      if (i < P.n_in)
+        CUDA_TRY(cudaMemcpyAsync(d, memory[i], bytes, cudaMemcpyHostToDevice, st));
+      else
+        staged.push_back({i, memory[i]});
+      bt.p[i] = static_cast<float*>(d);
+    }
+    for (size_t k = 0; k < P.scratch_elems.size(); ++k)
+      bt.p[P.n_in + P.n_out + k] =
+          reinterpret_cast<float*>(static_cast<char*>(scratch) + c->scratch_off[k]);
+    launch_plan(c, bt, st);
+    for (auto& s : staged) {
+      const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[s.first], 1) * 4;
+      CUDA_TRY(cudaMemcpyAsync(s.second, bt.p[s.first], bytes, cudaMemcpyDeviceToHost, st));
+    }
+    for (void* d : temps) CUDA_TRY(cudaFreeAsync(d, st));
+    if (sync || !temps.empty()) CUDA_TRY(cudaStreamSynchronize(st));
+  } catch (const CudaFailure& e) {
+    return fail(LTB_ERR_CUDA, e.what());
+  } catch (const std::exception& e) {
+    return fail(LTB_ERR_INVALID, e.what());
+  }
+  return LTB_OK;
+}
+
+int copy_out(const std::string& s, char* buf, size_t len) {
+  if (!buf || !len) return fail(LTB_ERR_INVALID, "empty output buffer");
+  size_t m = std::min(len - 1, s.size());
+  memcpy(buf, s.data(), m);
+  buf[m] = 0;
+  return LTB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ltb_abi_version(void) { return 1; }
+
+const char* ltb_last_error(void) { return g_err.c_str(); }
+
+int ltb_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int ok = 0;
+  for (int i = 0; i < n; ++i) {
+    cudaDeviceProp p{};
+    if (cudaGetDeviceProperties(&p, i) == cudaSuccess && p.major == 10) ok++;
+  }
+  return ok;
+}
+
+int ltb_plan(const char* ir_text, const char* options, char* buf, size_t len) {
+  if (!ir_text) return fail(LTB_ERR_INVALID, "null IR text");
+  try {
+    auto opt = parse_options(options);
+    auto g = ltb::parse_ir(ir_text);
+    auto p = ltb::lower(g, opt);
+    return copy_out(p.dump, buf, len);
+  } catch (const ltb::Error& e) {
+    return fail(LTB_ERR_UNSUPPORTED, e.what());
+  } catch (const std::exception& e) {
+    return fail(LTB_ERR_INVALID, e.what());
+  }
+}
+
+int ltb_compile(const char* ir_text, const char* options, ltb_compiled** out) {
+  if (!ir_text || !out) return fail(LTB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  auto c = new ltb_compiled();
+  try {
+    c->ir_text = ir_text;
+    c->opt = parse_options(options);
+    c->ir = ltb::parse_ir(c->ir_text);
+    c->plan = ltb::lower(c->ir, c->opt);
+  } catch (const std::exception& e) {
+    delete c;
+    return fail(LTB_ERR_UNSUPPORTED, e.what());
+  }
+  if (ltb_device_count() == 0) {
+    delete c;
+    return fail(LTB_ERR_NO_DEVICE, "no sm_100 CUDA device visible");
+  }
+  try {
+    compile_device(c);
+  } catch (const std::exception& e) {
+    for (void* p : c->owned) cudaFree(p);
+    delete c;
+    return fail(LTB_ERR_CUDA, e.what());
+  }
+  *out = c;
+  return LTB_OK;
+}
+
+int ltb_run(ltb_compiled* c, void* const* memory, int n, int sync, void* stream) {
+  return run_impl(c, memory, n, sync, stream, nullptr);
+}
+
+int ltb_run_with_scratch(ltb_compiled* c, void* const* memory, int n, int sync,
+                         void* stream, void* scratch) {
+  if (c && c->scratch_bytes && !scratch)
+    return fail(LTB_ERR_INVALID, "scratch pointer required");
+  return run_impl(c, memory, n, sync, stream, scratch ? scratch : c->scratch);
+}
+
+int ltb_release(ltb_compiled* c) {
+  if (!c) return LTB_OK;
+  for (void* p : c->owned) cudaFree(p);
+  delete c;
+  return LTB_OK;
+}
+
+int ltb_dump(ltb_compiled* c, char* buf, size_t len) {
+  if (!c) return fail(LTB_ERR_INVALID, "null compiled object");
+  return copy_out(c->plan.dump, buf, len);
+}
+
+int ltb_int_property(ltb_compiled* c, const char* name, int64_t* value) {
+  if (!c || !name || !value) return fail(LTB_ERR_INVALID, "null argument");
+  std::string k = name;
+  if (k == "bandwidth") *value = c->bandwidth_gbs;
+  else if (k == "stages") *value = (int64_t)c->plan.stages.size();
+  else if (k == "launches") *value = c->launches;
+  else if (k == "scratch_bytes") *value = (int64_t)c->scratch_bytes;
+  else if (k == "inputs") *value = c->plan.n_in;
+  else if (k == "outputs") *value = c->plan.n_out;
+  else if (k == "algorithmic_bytes") *value = c->plan.algorithmic_bytes;
+  else if (k == "flops") *value = (int64_t)c->plan.flops;
+  else return fail(LTB_ERR_INVALID, "unknown property " + k);
+  return LTB_OK;
+}
+
+int ltb_io_sizes(ltb_compiled* c, int* n_in, int* n_out, int64_t* elems, int cap) {
+  if (!c) return fail(LTB_ERR_INVALID, "null compiled object");
+  if (n_in) *n_in = c->plan.n_in;
+  if (n_out) *n_out = c->plan.n_out;
+  for (int i = 0; elems && i < cap && i < (int)c->plan.io_elems.size(); ++i)
+    elems[i] = c->plan.io_elems[i];
+  return LTB_OK;
+}
+
+int ltb_alloc(size_t bytes, int managed, void** out) {
+  if (!out) return fail(LTB_ERR_INVALID, "null output pointer");
+  cudaError_t e = managed ? cudaMallocManaged(out, bytes, cudaMemAttachGlobal)
+                          : cudaMalloc(out, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(LTB_ERR_CUDA, std::string("allocation failed: ") + cudaGetErrorString(e));
+  }
+  return LTB_OK;
+}
+
+int ltb_free(void* ptr) {
+  cudaError_t e = cudaFree(ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(LTB_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return LTB_OK;
+}
+
+int ltb_synchronize(void* stream) {
+  cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(LTB_ERR_CUDA, cudaGetErrorString(e));
+  return LTB_OK;
+}
+
+}  // extern "C"
