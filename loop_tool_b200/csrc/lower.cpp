@@ -387,6 +387,44 @@ struct Builder {
     }
   }
 
+  // Load modes, the linear fast path and 32-bit division constants.
+  static void finalize(LtbStage& d) {
+    bool linear = d.ndim == d.nout && d.nout > 0;
+    for (int i = 0; i < d.nload; ++i) {
+      LtbLoad& L = d.loads[i];
+      L.mode = LTB_L_GENERAL;
+      if (L.nq || L.ng) {
+        linear = false;
+        continue;
+      }
+      bool same = true, zero = true;
+      for (int k = 0; k < d.ndim; ++k) {
+        same = same && L.coef[k] == (k < d.nout ? d.out_coef[k] : 0);
+        zero = zero && L.coef[k] == 0;
+      }
+      if (zero) L.mode = LTB_L_SCALAR;
+      else if (same && d.ndim == d.nout) L.mode = LTB_L_LINEAR;
+      else linear = false;
+    }
+    d.linear = linear ? 1 : 0;
+    const int64_t lim = int64_t(1) << 31;
+    int64_t outs = 1;
+    bool small = true;
+    for (int k = 0; k < d.ndim; ++k) {
+      int64_t n = d.size[k];
+      small = small && n < lim;
+      if (k < d.nout) outs *= n;
+      uint32_t l = 0;
+      while (l < 32 && (int64_t(1) << l) < n) ++l;
+      uint64_t m = n < lim && n > 0
+                       ? (((uint64_t(1) << 32) * ((uint64_t(1) << l) - n)) / n) + 1
+                       : 1;
+      d.dm_mul[k] = (uint32_t)m;
+      d.dm_shr[k] = l;
+    }
+    d.small = small && outs < lim && d.red_total < lim;
+  }
+
   // ------------------------------------------------------------- lowering
   void detect_contraction(StageCtx& s, int R) {
     const auto& d = s.ps.dev;
@@ -565,6 +603,7 @@ struct Builder {
           s.ps.family = Family::elementwise;
         }
       }
+      finalize(s.ps.dev);
       s.ps.text = stage_text(s);
       plan.stages.push_back(s.ps);
     }
@@ -585,6 +624,45 @@ struct Builder {
       ss << " }\n";
     }
     plan.dump = ss.str();
+  }
+
+  // m = max_n x; s = sum_n exp(x - m); y = exp(x - m) / s over the same x
+  // row with a unit inner stride: the fused row-softmax pattern.
+  bool is_softmax(const std::vector<int>& grp) const {
+    if (grp.size() != 3) return false;
+    const auto& a = plan.stages[grp[0]].dev;
+    const auto& b = plan.stages[grp[1]].dev;
+    const auto& c = plan.stages[grp[2]].dev;
+    auto ops = [](const LtbStage& d, std::vector<int> want) {
+      if (d.ninstr != (int)want.size()) return false;
+      for (int i = 0; i < d.ninstr; ++i)
+        if (d.code[i].op != want[i]) return false;
+      return true;
+    };
+    if (a.red_op != LTB_R_MAX || b.red_op != LTB_R_ADD) return false;
+    if (!ops(a, {LTB_V_LOAD, LTB_V_FOLD})) return false;
+    if (!ops(b, {LTB_V_LOAD, LTB_V_LOAD, LTB_V_SUB, LTB_V_EXP, LTB_V_FOLD})) return false;
+    if (!ops(c, {LTB_V_LOAD, LTB_V_LOAD, LTB_V_SUB, LTB_V_EXP, LTB_V_LOAD, LTB_V_DIV}))
+      return false;
+    auto same_x = [](const LtbStage& p, int pi, const LtbStage& q, int qi) {
+      const LtbLoad& x = p.loads[p.code[pi].arg];
+      const LtbLoad& y = q.loads[q.code[qi].arg];
+      if (x.buf != y.buf || x.off != y.off || x.nq || y.nq || x.ng || y.ng) return false;
+      for (int k = 0; k < p.ndim; ++k)
+        if (x.coef[k] != y.coef[k]) return false;
+      return true;
+    };
+    // x loads agree (row dims then the inner dim, same positions in all
+    // three stages by construction of the group)
+    if (!same_x(a, 0, b, 0) || !same_x(a, 0, c, 0)) return false;
+    const LtbLoad& x = a.loads[a.code[0].arg];
+    if (x.coef[a.ndim - 1] != 1) return false;
+    // m and s are the first two stages' per-row outputs
+    if (b.loads[b.code[1].arg].buf != a.out_buf) return false;
+    if (c.loads[c.code[1].arg].buf != a.out_buf) return false;
+    if (c.loads[c.code[4].arg].buf != b.out_buf) return false;
+    if (c.out_coef[c.nout - 1] != 1) return false;
+    return true;
   }
 
   // Consecutive stages that iterate the same outer "row" vars and only
@@ -634,6 +712,8 @@ struct Builder {
         plan.row_groups.push_back(grp);
         for (int k : grp) st[k].family = Family::row_chain;
         for (size_t k = 0; k < grp.size(); ++k) st[grp[k]].rows_from = grp[0];
+        if (is_softmax(grp))
+          for (int k : grp) st[k].dev.pattern = LTB_P_SOFTMAX;
         i = j;
       } else {
         ++i;

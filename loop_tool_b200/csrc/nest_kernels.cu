@@ -91,9 +91,14 @@ __device__ __forceinline__ Lanes<VEC> load_lanes(const LtbStage& S,
 // Generic nest kernel: elementwise stages and serial reductions.  One thread
 // produces VEC consecutive outputs along the innermost output dim and
 // walks the reduced dims in order (exact sequential fold semantics).
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, uint32_t mul, uint32_t shr) {
+  return (__umulhi(n, mul) + n) >> shr;
+}
+
 template <int VEC>
 __global__ void __launch_bounds__(256)
-    k_nest(const LtbStage* __restrict__ gst, LtbBufTable bt) {
+    k_nest(const LtbStage* __restrict__ gst, LtbBufTable bt, uint32_t nvec_mul,
+           uint32_t nvec_shr) {
   __shared__ __align__(16) LtbStage S;
   load_stage(gst, S);
   const int nd = S.ndim, no = S.nout;
@@ -110,13 +115,28 @@ __global__ void __launch_bounds__(256)
   for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < total;
        w += (int64_t)gridDim.x * blockDim.x) {
     int64_t x[LTB_MAXD];
-    int64_t o = w / nvec;
-    const int64_t iv = w - o * nvec;
-    for (int k = ki - 1; k >= 0; --k) {
-      const int64_t q = o / S.size[k];
-      x[k] = o - q * S.size[k];
-      o = q;
+    int64_t o, iv;
+    if (S.small) {  // 32-bit multiply-high division
+      const uint32_t o32 = fdiv((uint32_t)w, nvec_mul, nvec_shr);
+      iv = (uint32_t)w - o32 * (uint32_t)nvec;
+      uint32_t r = o32;
+      for (int k = ki - 1; k >= 0; --k) {
+        const uint32_t q = fdiv(r, S.dm_mul[k], S.dm_shr[k]);
+        x[k] = r - q * (uint32_t)S.size[k];
+        r = q;
+      }
+      o = o32;
+    } else {
+      o = w / nvec;
+      iv = w - o * nvec;
+      int64_t r = o;
+      for (int k = ki - 1; k >= 0; --k) {
+        const int64_t q = r / S.size[k];
+        x[k] = r - q * S.size[k];
+        r = q;
+      }
     }
+    (void)o;
     if (ki >= 0) x[ki] = iv * VEC;
     const int nv = (int)(inner - iv * VEC < VEC ? inner - iv * VEC : VEC);
     for (int k = no; k < nd; ++k) x[k] = 0;
@@ -567,6 +587,322 @@ __global__ void __launch_bounds__(512)
   }
 }
 
+// ---------------------------------------------------------------- linear
+template <int VEC>
+__device__ __forceinline__ Lanes<VEC> linear_load(const LtbLoad& L, const LtbBufTable& bt,
+                                                  int64_t i0, bool full, int nv) {
+  Lanes<VEC> t;
+  const float* __restrict__ p = bt.p[L.buf] + L.off;
+  if (L.mode == LTB_L_SCALAR) {
+    const float c = __ldg(p);
+#pragma unroll
+    for (int j = 0; j < VEC; ++j) t.v[j] = c;
+  } else if (full) {
+#pragma unroll
+    for (int j = 0; j < VEC; j += 4) {
+      const float4 q = __ldcs(reinterpret_cast<const float4*>(p + i0 + j));
+      t.v[j] = q.x; t.v[j + 1] = q.y; t.v[j + 2] = q.z; t.v[j + 3] = q.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < VEC; ++j) t.v[j] = j < nv ? p[i0 + j] : 0.f;
+  }
+  return t;
+}
+
+// Binary / unary maps over two (one) linear operands: the dominant
+// elementwise shapes, kept small (few registers, full occupancy) with two
+// 128-bit loads per operand in flight per thread.
+template <int OP>
+__global__ void __launch_bounds__(256)
+    k_lin_bin(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ c,
+              int64_t total) {
+  const int64_t n8 = total / 8;
+  const float4* A = reinterpret_cast<const float4*>(a);
+  const float4* B = reinterpret_cast<const float4*>(b);
+  float4* C = reinterpret_cast<float4*>(c);
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n8;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const float4 a0 = __ldcs(A + 2 * v), a1 = __ldcs(A + 2 * v + 1);
+    const float4 b0 = __ldcs(B + 2 * v), b1 = __ldcs(B + 2 * v + 1);
+    __stcs(C + 2 * v, make_float4(vm_bin(OP, a0.x, b0.x), vm_bin(OP, a0.y, b0.y),
+                                  vm_bin(OP, a0.z, b0.z), vm_bin(OP, a0.w, b0.w)));
+    __stcs(C + 2 * v + 1, make_float4(vm_bin(OP, a1.x, b1.x), vm_bin(OP, a1.y, b1.y),
+                                      vm_bin(OP, a1.z, b1.z), vm_bin(OP, a1.w, b1.w)));
+  }
+  // ragged tail (< 8 elements)
+  const int64_t t = n8 * 8 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < total) c[t] = vm_bin(OP, a[t], b[t]);
+}
+
+template <int OP>
+__global__ void __launch_bounds__(256)
+    k_lin_un(const float* __restrict__ a, float* __restrict__ c, int64_t total) {
+  const int64_t n8 = total / 8;
+  const float4* A = reinterpret_cast<const float4*>(a);
+  float4* C = reinterpret_cast<float4*>(c);
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n8;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const float4 a0 = __ldcs(A + 2 * v), a1 = __ldcs(A + 2 * v + 1);
+    __stcs(C + 2 * v, make_float4(vm_un(OP, a0.x), vm_un(OP, a0.y), vm_un(OP, a0.z),
+                                  vm_un(OP, a0.w)));
+    __stcs(C + 2 * v + 1, make_float4(vm_un(OP, a1.x), vm_un(OP, a1.y), vm_un(OP, a1.z),
+                                      vm_un(OP, a1.w)));
+  }
+  const int64_t t = n8 * 8 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < total) c[t] = vm_un(OP, a[t]);
+}
+
+// Elementwise stages whose every load reads the output's own flat index (or
+// one broadcast scalar): a pure 1-D map.  Each thread moves VEC consecutive
+// floats per operand with 128-bit accesses; no index decomposition.
+template <int VEC>
+__global__ void __launch_bounds__(256)
+    k_linear(const LtbStage* __restrict__ gst, LtbBufTable bt, int64_t total) {
+  __shared__ __align__(16) LtbStage S;
+  load_stage(gst, S);
+  float* __restrict__ out = bt.p[S.out_buf] + S.out_off;
+  bool aligned = (S.out_off & 3) == 0;
+  for (int i = 0; i < S.nload; ++i)
+    aligned = aligned && (S.loads[i].mode == LTB_L_SCALAR || (S.loads[i].off & 3) == 0);
+  const int64_t nv_total = (total + VEC - 1) / VEC;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv_total;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i0 = v * VEC;
+    const bool full = aligned && i0 + VEC <= total;
+    const int nv = (int)(total - i0 < VEC ? total - i0 : VEC);
+    // issue every operand load before the program runs: the stack moves
+    // below would otherwise wait on each load in turn
+    Lanes<VEC> pre[2];
+#pragma unroll
+    for (int li = 0; li < 2; ++li) {
+      if (li < S.nload) pre[li] = linear_load<VEC>(S.loads[li], bt, i0, full, nv);
+    }
+    Lanes<VEC> s0{}, s1{}, s2{}, s3{}, s4{}, s5{};
+    for (int i = 0; i < S.ninstr; ++i) {
+      const LtbVInstr in = S.code[i];
+      const int op = in.op;
+      if (op == LTB_V_LOAD || op == LTB_V_CONST) {
+        Lanes<VEC> t;
+        if (op == LTB_V_CONST) {
+#pragma unroll
+          for (int j = 0; j < VEC; ++j) t.v[j] = S.consts[in.arg];
+        } else if (in.arg < 2) {
+          t = in.arg == 0 ? pre[0] : pre[1];
+        } else {
+          t = linear_load<VEC>(S.loads[in.arg], bt, i0, full, nv);
+        }
+        s5 = s4; s4 = s3; s3 = s2; s2 = s1; s1 = s0; s0 = t;
+      } else if (op >= LTB_V_EXP) {
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) s0.v[j] = vm_un(op, s0.v[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) s0.v[j] = vm_bin(op, s1.v[j], s0.v[j]);
+        s1 = s2; s2 = s3; s3 = s4; s4 = s5;
+      }
+    }
+    if (full) {
+#pragma unroll
+      for (int j = 0; j < VEC; j += 4)
+        __stcs(reinterpret_cast<float4*>(out + i0 + j),
+               make_float4(s0.v[j], s0.v[j + 1], s0.v[j + 2], s0.v[j + 3]));
+    } else {
+#pragma unroll
+      for (int j = 0; j < VEC; ++j)
+        if (j < nv) out[i0 + j] = s0.v[j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- window
+// Small-window reductions of one operand (pooling): out[..., o] folds
+// x[... S*o + q] over q < K and the other reduced dims.  A thread makes 4
+// consecutive outputs; for each outer reduced coordinate it loads the
+// contiguous span of 3S+K inputs those outputs cover with 128-bit loads,
+// then folds in the reference's sequential order (exact for max/min).
+template <int S_, int K_>
+__global__ void __launch_bounds__(256)
+    k_window(const LtbStage* __restrict__ gst, LtbBufTable bt, uint32_t nvec_mul,
+             uint32_t nvec_shr) {
+  __shared__ __align__(16) LtbStage S;
+  __shared__ int64_t roff[64];
+  load_stage(gst, S);
+  constexpr int N = 3 * S_ + K_;
+  const int no = S.nout, nd = S.ndim, ki = no - 1;
+  const LtbLoad& L = S.loads[0];
+  // offsets of every combination of the outer reduced dims
+  const int64_t RC = S.red_total / K_;
+  for (int64_t rc = threadIdx.x; rc < RC; rc += blockDim.x) {
+    int64_t r = rc, o = 0;
+    for (int k = nd - 2; k >= no; --k) {
+      const int64_t q = r / S.size[k];
+      o += L.coef[k] * (r - q * S.size[k]);
+      r = q;
+    }
+    roff[rc] = o;
+  }
+  __syncthreads();
+  const uint32_t inner = (uint32_t)S.size[ki];
+  const uint32_t nvec = (inner + 3) / 4;
+  uint32_t outer = 1;
+  for (int k = 0; k < ki; ++k) outer *= (uint32_t)S.size[k];
+  const uint32_t total = outer * nvec;
+  const float* __restrict__ src = bt.p[L.buf];
+  float* __restrict__ out = bt.p[S.out_buf];
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < total;
+       w += gridDim.x * blockDim.x) {
+    const uint32_t o32 = fdiv(w, nvec_mul, nvec_shr);
+    const uint32_t iv = w - o32 * nvec;
+    int64_t base = L.off, obase = S.out_off;
+    uint32_t r = o32;
+    for (int k = ki - 1; k >= 0; --k) {
+      const uint32_t q = fdiv(r, S.dm_mul[k], S.dm_shr[k]);
+      const int64_t c = r - q * (uint32_t)S.size[k];
+      base += L.coef[k] * c;
+      obase += S.out_coef[k] * c;
+      r = q;
+    }
+    const int64_t o0 = (int64_t)iv * 4;
+    base += L.coef[ki] * o0;
+    obase += o0;
+    const int nv = (int)(inner - o0 < 4 ? inner - o0 : 4);
+    float acc[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[j] = S.red_init;
+    for (int64_t rc = 0; rc < RC; ++rc) {
+      const float* p = src + base + roff[rc];
+      float span[N];
+      if (nv == 4 && ((base + roff[rc]) & 3) == 0) {
+#pragma unroll
+        for (int q = 0; q + 4 <= N; q += 4) {
+          const float4 t = __ldg(reinterpret_cast<const float4*>(p + q));
+          span[q] = t.x; span[q + 1] = t.y; span[q + 2] = t.z; span[q + 3] = t.w;
+        }
+#pragma unroll
+        for (int q = N & ~3; q < N; ++q) span[q] = __ldg(p + q);
+      } else {
+#pragma unroll
+        for (int q = 0; q < N; ++q) span[q] = q <= (nv - 1) * S_ + K_ - 1 ? __ldg(p + q) : 0.f;
+      }
+#pragma unroll
+      for (int q = 0; q < K_; ++q)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[j] = fold(S.red_op, acc[j], span[j * S_ + q]);
+    }
+    if (nv == 4 && (obase & 3) == 0) {
+      *reinterpret_cast<float4*>(out + obase) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < nv) out[obase + j] = acc[j];
+    }
+  }
+}
+
+// ----------------------------------------------------------- row softmax
+// Fused pattern m = max_n x, s = sum_n exp(x - m), y = exp(x - m) / s.
+// One CTA per row, the row held in registers (EPT floats per thread, loaded
+// and stored as float4), so HBM sees one read and one write per element.
+// The max is the reference's ternary fold from -FLT_MAX; its tie and NaN
+// order cannot change y (a NaN anywhere makes s, hence every y, NaN).
+template <int EPT, int NT>
+__global__ void __launch_bounds__(NT)
+    k_row_softmax(const LtbStage* __restrict__ gst, LtbBufTable bt, int64_t nrows) {
+  __shared__ __align__(16) LtbStage S[3];
+  __shared__ float red[NT / 32];
+  {
+    const int4* src = reinterpret_cast<const int4*>(gst);
+    int4* dst = reinterpret_cast<int4*>(S);
+    for (int i = threadIdx.x; i < 3 * (int)(sizeof(LtbStage) / 16); i += NT) dst[i] = src[i];
+    __syncthreads();
+  }
+  const LtbStage& A = S[0];  // max over n
+  const LtbStage& B = S[1];  // sum over n
+  const LtbStage& C = S[2];  // elementwise output
+  const LtbLoad& X = A.loads[A.code[0].arg];
+  const int nrd = C.nout - 1;
+  const int64_t n = C.size[nrd];
+  const float* __restrict__ xb = bt.p[X.buf];
+  float* __restrict__ yb = bt.p[C.out_buf];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool vec_ok = (n & 3) == 0;
+  for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x) {
+    int64_t xoff = X.off, yoff = C.out_off, moff = A.out_off, soff = B.out_off;
+    {
+      int64_t r = row;
+      for (int k = nrd - 1; k >= 0; --k) {
+        const int64_t q = r / C.size[k];
+        const int64_t c = r - q * C.size[k];
+        r = q;
+        xoff += X.coef[k] * c;
+        yoff += C.out_coef[k] * c;
+        moff += A.out_coef[k] * c;
+        soff += B.out_coef[k] * c;
+      }
+    }
+    const bool v4 = vec_ok && ((xoff | yoff) & 3) == 0;
+    float v[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT / 4; ++q) {
+      const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
+      if (v4 && j < n) {
+        const float4 t = __ldcs(reinterpret_cast<const float4*>(xb + xoff + j));
+        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) v[4 * q + e] = j + e < n ? xb[xoff + j + e] : -INFINITY;
+      }
+    }
+    // max (ternary fold; padding lanes hold -inf, which never wins)
+    float m = -FLT_MAX;
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) m = m > v[e] ? m : v[e];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float o = __shfl_xor_sync(0xffffffffu, m, off);
+      m = m > o ? m : o;
+    }
+    if (lane == 0) red[wid] = m;
+    __syncthreads();
+    m = red[0];
+#pragma unroll
+    for (int w = 1; w < NT / 32; ++w) m = m > red[w] ? m : red[w];
+    __syncthreads();
+    float sum = 0.f;
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      v[e] = expf(v[e] - m);
+      sum += v[e];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    if (lane == 0) red[wid] = sum;
+    __syncthreads();
+    sum = 0.f;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) sum += red[w];
+    __syncthreads();
+    if (threadIdx.x == 0) {  // per-row results stay visible to later stages
+      bt.p[A.out_buf][moff] = m;
+      bt.p[B.out_buf][soff] = sum;
+    }
+#pragma unroll
+    for (int q = 0; q < EPT / 4; ++q) {
+      const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
+      if (v4 && j < n) {
+        __stcs(reinterpret_cast<float4*>(yb + yoff + j),
+               make_float4(v[4 * q] / sum, v[4 * q + 1] / sum, v[4 * q + 2] / sum,
+                           v[4 * q + 3] / sum));
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (j + e < n) yb[yoff + j + e] = v[4 * q + e] / sum;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ launchers
@@ -584,14 +920,74 @@ cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
   const int64_t inner = no ? h.size[no - 1] : 1;
   int64_t outer = 1;
   for (int k = 0; k < no - 1; ++k) outer *= h.size[k];
-  const bool vec = inner >= 4;
-  const int64_t work = outer * (vec ? (inner + 3) / 4 : inner);
   const int threads = 256;
+  if (h.linear) {
+    int64_t total = outer * inner;
+    const int grid = grid_for((total + 7) / 8, threads, sms);
+    // [LOAD a, LOAD b, op] / [LOAD a, op] over linear, 16B-aligned operands
+    auto lin = [&](int i) {
+      const LtbLoad& L = h.loads[h.code[i].arg];
+      return L.mode == LTB_L_LINEAR && (L.off & 3) == 0;
+    };
+    float* out = bt.p[h.out_buf] + h.out_off;
+    if (total >= 8 && (h.out_off & 3) == 0 && h.ninstr == 3 && h.code[0].op == LTB_V_LOAD &&
+        h.code[1].op == LTB_V_LOAD && lin(0) && lin(1) && h.code[2].op >= LTB_V_ADD &&
+        h.code[2].op <= LTB_V_MAX) {
+      const float* a = bt.p[h.loads[h.code[0].arg].buf] + h.loads[h.code[0].arg].off;
+      const float* b = bt.p[h.loads[h.code[1].arg].buf] + h.loads[h.code[1].arg].off;
+      switch (h.code[2].op) {
+#define LTB_BIN(O) \
+  case O: k_lin_bin<O><<<grid, threads, 0, st>>>(a, b, out, total); break;
+        LTB_BIN(LTB_V_ADD) LTB_BIN(LTB_V_SUB) LTB_BIN(LTB_V_MUL) LTB_BIN(LTB_V_DIV)
+        LTB_BIN(LTB_V_MIN) LTB_BIN(LTB_V_MAX)
+#undef LTB_BIN
+      }
+      return cudaGetLastError();
+    }
+    if (total >= 8 && (h.out_off & 3) == 0 && h.ninstr == 2 && h.code[0].op == LTB_V_LOAD &&
+        lin(0) && h.code[1].op >= LTB_V_EXP && h.code[1].op <= LTB_V_RECIP) {
+      const float* a = bt.p[h.loads[h.code[0].arg].buf] + h.loads[h.code[0].arg].off;
+      switch (h.code[1].op) {
+#define LTB_UN(O) \
+  case O: k_lin_un<O><<<grid, threads, 0, st>>>(a, out, total); break;
+        LTB_UN(LTB_V_EXP) LTB_UN(LTB_V_LOG) LTB_UN(LTB_V_SQRT) LTB_UN(LTB_V_ABS)
+        LTB_UN(LTB_V_NEG) LTB_UN(LTB_V_RECIP)
+#undef LTB_UN
+      }
+      return cudaGetLastError();
+    }
+    k_linear<4><<<grid_for((total + 3) / 4, threads, sms), threads, 0, st>>>(d_stage, bt, total);
+    return cudaGetLastError();
+  }
+  const bool vec = inner >= 4;
+  const int64_t nvec = vec ? (inner + 3) / 4 : inner;
+  const int64_t work = outer * nvec;
+  uint32_t l = 0;
+  while (l < 32 && (int64_t(1) << l) < nvec) ++l;
+  const uint32_t mul =
+      (uint32_t)((((uint64_t(1) << 32) * ((uint64_t(1) << l) - (uint64_t)nvec)) / (uint64_t)nvec) + 1);
   const int grid = grid_for(work, threads, sms);
+  // pooling-shaped reductions: one operand, unit-stride innermost window
+  const LtbLoad& L0 = h.loads[0];
+  if (vec && h.small && h.nout >= 1 && h.ndim > h.nout && h.nload == 1 && h.ninstr == 2 &&
+      h.code[0].op == LTB_V_LOAD && h.code[1].op == LTB_V_FOLD && L0.nq == 0 && L0.ng == 0 &&
+      h.out_coef[h.nout - 1] == 1 && L0.coef[h.ndim - 1] == 1 &&
+      h.red_total / h.size[h.ndim - 1] <= 64 && h.red_op != LTB_R_SUB && h.red_op != LTB_R_DIV &&
+      !h.kahan) {
+    const int64_t s = L0.coef[h.nout - 1], k = h.size[h.ndim - 1];
+#define LTB_WIN(SS, KK)                                                      \
+  if (s == SS && k == KK) {                                                  \
+    k_window<SS, KK><<<grid, threads, 0, st>>>(d_stage, bt, mul, l);         \
+    return cudaGetLastError();                                               \
+  }
+    LTB_WIN(2, 2) LTB_WIN(1, 2) LTB_WIN(1, 3) LTB_WIN(2, 3) LTB_WIN(3, 3) LTB_WIN(1, 1)
+    LTB_WIN(2, 1)
+#undef LTB_WIN
+  }
   if (vec)
-    k_nest<4><<<grid, threads, 0, st>>>(d_stage, bt);
+    k_nest<4><<<grid, threads, 0, st>>>(d_stage, bt, mul, l);
   else
-    k_nest<1><<<grid, threads, 0, st>>>(d_stage, bt);
+    k_nest<1><<<grid, threads, 0, st>>>(d_stage, bt, mul, l);
   return cudaGetLastError();
 }
 
@@ -620,6 +1016,20 @@ cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, int nsteps,
   int64_t rows = 1;
   for (int k = 0; k < final_stage.nout - 1; ++k) rows *= final_stage.size[k];
   const int64_t inner = final_stage.size[final_stage.nout - 1];
+  if (final_stage.pattern == LTB_P_SOFTMAX && nsteps == 3 && inner <= 256 * 32) {
+    const unsigned grid = (unsigned)(rows < (int64_t)sms * 64 ? rows : (int64_t)sms * 64);
+    if (inner <= 128 * 4)
+      k_row_softmax<4, 128><<<grid, 128, 0, st>>>(d_stages, bt, rows);
+    else if (inner <= 256 * 4)
+      k_row_softmax<4, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
+    else if (inner <= 256 * 8)
+      k_row_softmax<8, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
+    else if (inner <= 256 * 16)
+      k_row_softmax<16, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
+    else
+      k_row_softmax<32, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
+    return cudaGetLastError();
+  }
   const int threads = inner >= 4096 ? 512 : (inner >= 1024 ? 256 : 128);
   int64_t grid = rows < (int64_t)sms * 8 ? rows : (int64_t)sms * 8;
   if (grid < 1) grid = 1;

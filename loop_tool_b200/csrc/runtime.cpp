@@ -186,6 +186,14 @@ void compile_device(ltb_compiled* c) {
   cudaDeviceGetAttribute(&bus_bits, cudaDevAttrGlobalMemoryBusWidth, c->device);
   cudaGetLastError();
   c->bandwidth_gbs = (int64_t)(2.0 * memclk_khz * 1e3 * (bus_bits / 8) / 1e9);
+  // host buffers are staged through the stream-ordered pool; keep what it
+  // reserved across synchronisations instead of unmapping it every time
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   auto& P = c->plan;
   const int ns = (int)P.stages.size();
   c->split_of.assign(ns, 1);

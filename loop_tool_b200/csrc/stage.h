@@ -74,11 +74,17 @@ typedef struct {
   int64_t ub;  // valid iff 0 <= coef.x + off < ub
 } LtbGuard;
 
+enum LtbLoadMode {
+  LTB_L_GENERAL = 0,  // coef . x + off (with guards / index program)
+  LTB_L_LINEAR = 1,   // same flat index as the output: off + out_flat
+  LTB_L_SCALAR = 2,   // one element broadcast: off
+};
+
 typedef struct {
   int32_t buf;      // buffer slot
   int32_t g0, ng;   // guards [g0, g0+ng) (affine loads)
   int32_t q0, nq;   // index program words (quasi-affine loads), nq == 0 => affine
-  int32_t pad_;
+  int32_t mode;     // LtbLoadMode
   int64_t coef[LTB_MAXD];  // flat index = coef.x + off (affine loads)
   int64_t off;
 } LtbLoad;
@@ -92,6 +98,8 @@ typedef struct {
   int32_t out_buf;
   int32_t split;      // >1: partial reductions go to partial_buf
   int32_t partial_buf;
+  int32_t linear;     // elementwise stage whose loads are all LINEAR/SCALAR
+  int32_t pattern;    // LtbPattern of a recognised fused chain (row_chain)
   int64_t size[LTB_MAXD];
   int64_t out_coef[LTB_MAXD];
   int64_t out_off;
@@ -103,8 +111,18 @@ typedef struct {
   LtbVInstr code[LTB_MAXI];
   float consts[LTB_MAXC];
   LtbQWord q[LTB_MAXQ];
-  int64_t pad3_;  // keeps sizeof a multiple of 16 (int4 staging copies)
+  // 32-bit division by size[k] as (umulhi(n, mul) + n) >> shr
+  // (Granlund-Montgomery), valid for n < 2^31
+  uint32_t dm_mul[LTB_MAXD];
+  uint32_t dm_shr[LTB_MAXD];
+  int32_t small;      // every size and flat extent < 2^31: 32-bit indexing
+  int32_t pad3_[3];   // keeps sizeof a multiple of 16 (int4 staging copies)
 } LtbStage;
+
+enum LtbPattern {
+  LTB_P_NONE = 0,
+  LTB_P_SOFTMAX = 1,  // m = max_n x; s = sum_n exp(x - m); y = exp(x - m) / s
+};
 
 // Buffer pointers of one run, passed by value to every launch.
 typedef struct {

@@ -108,11 +108,12 @@ static Tensor build(const std::string& prog, const std::vector<int64_t>& p) {
     if (prog == "recip") return a.reciprocal();
     return a.abs();
   }
-  if (prog == "chain") {  // (a*b + c).sqrt() / -(a) : fused elementwise tree
+  if (prog == "chain") {  // a fused elementwise tree over three inputs
     Symbol N("N");
     Tensor A(P(p, 0)), B(P(p, 0)), C(P(p, 0));
     auto a = A.as(N), b = B.as(N), c = C.as(N);
-    return ((a * b + c).abs().sqrt() / (-a)).max(c);
+    auto t = a * b + c;
+    return ((t * t).sqrt() / (-a)).max(c) - b.reciprocal();
   }
   if (prog == "mm") {  // (A.to(m,k) * B.to(k,n)).sum(k)
     Symbol M("m"), K("k"), N("n");

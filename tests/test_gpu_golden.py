@@ -7,7 +7,16 @@ goes through the C ABI (ltb_compile / ltb_run) on cuda:0.
 import numpy as np
 import pytest
 
-from golden_util import EXACT_PROGRAMS, assert_parity, load, manifest
+from golden_util import EXACT_PROGRAMS, assert_accuracy, assert_parity, fp64_oracle, load, manifest
+
+
+def check(got, case, name):
+    """Bit-exact against the reference where its arithmetic is exact, else
+    measured against the FP64 oracle (and never worse than the reference)."""
+    if case["program"] in EXACT_PROGRAMS:
+        assert_parity(got, case["expected"], True, what=name)
+    else:
+        assert_accuracy(got, case["expected"], fp64_oracle(case), what=name)
 
 CASES = [m["name"] for m in manifest()]
 
@@ -25,8 +34,7 @@ def test_golden_device_buffers(name, cuda_dev):
     out = torch.full((c.io_sizes[-1],), 1337.0, device=cuda_dev)
     c(ins + [out])
     torch.cuda.synchronize()
-    assert_parity(out.cpu().numpy(), case["expected"],
-                  case["program"] in EXACT_PROGRAMS, what=name)
+    check(out.cpu().numpy(), case, name)
 
 
 @pytest.mark.gpu
@@ -41,4 +49,4 @@ def test_golden_host_buffers(name, cuda_dev):
     c = lt.cuda(case["ir"])
     out = np.full(c.io_sizes[-1], 1337.0, np.float32)
     c([np.ascontiguousarray(a) for a in case["inputs"]] + [out])
-    assert_parity(out, case["expected"], case["program"] in EXACT_PROGRAMS, what=name)
+    check(out, case, name)
