@@ -52,7 +52,9 @@ int ltb_device_count(void);
  * serialized LoopTree into buf (NUL-terminated, truncated to len).
  * Replaces the host-side analysis of cuda_code_and_dispatch /
  * calc_cuda_aux (src/backends/cuda/cuda.cpp:776-792, 973-1028).
- * options: "precision=fp32|bf16|bf16x3;fuse_rows=0|1;tensor_cores=0|1". */
+ * options: "precision=fp32|bf16|bf16x3|bf16x4;fuse_rows=0|1;tensor_cores=0|1".
+ * fp32: CUDA-core FP32 contractions; bf16: BF16 tensor cores, FP32
+ * accumulation; bf16x3 / bf16x4: split-BF16 with 3 / 4 products. */
 int ltb_plan(const char* ir_text, const char* options, char* buf, size_t len);
 
 /* Backend::compile(const LoopTree&) (include/loop_tool/backend.h:62-67),

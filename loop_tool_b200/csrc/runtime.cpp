@@ -13,6 +13,7 @@
 #include "../../include/loop_tool_b200.h"
 #include "kernels.h"
 #include "lower.hpp"
+#include "tc_api.h"
 
 static_assert(sizeof(LtbStage) % 16 == 0, "stage descriptor must be 16B-sized");
 
@@ -48,6 +49,7 @@ ltb::LowerOptions parse_options(const char* s) {
       if (v == "fp32") o.precision = ltb::Precision::fp32;
       else if (v == "bf16") o.precision = ltb::Precision::bf16;
       else if (v == "bf16x3") o.precision = ltb::Precision::bf16x3;
+      else if (v == "bf16x4") o.precision = ltb::Precision::bf16x4;
       else throw ltb::Error("unknown precision '" + v + "'");
     } else if (k == "fuse_rows") {
       o.fuse_rows = v != "0";
@@ -71,6 +73,14 @@ struct GemmTables {
   int32_t *ag_row = nullptr, *ag_k = nullptr, *ag_ub = nullptr;
   int32_t *bg_row = nullptr, *bg_k = nullptr, *bg_ub = nullptr;
   int a_ng = 0, b_ng = 0;
+  // tensor-core path: packed K-major BF16 operands and their tensor maps
+  bool tc = false;
+  int nseg = 1, a_mask = 1, b_mask = 1;
+  int64_t Kp = 0, tiles = 0;
+  void *a_pack = nullptr, *b_pack = nullptr;
+  void* d_maps = nullptr;             // two CUtensorMaps in device memory
+  LtbTcProblem* d_prob = nullptr;     // one problem entry per batch index
+  bool a_kcontig = true, b_kcontig = true, unit_cols = false;
 };
 
 template <typename T>
@@ -101,6 +111,7 @@ struct ltb_compiled {
   std::vector<int> gemm_of;           // stage -> index into gemms (or -1)
   std::vector<void*> owned;           // device allocations to free
   std::mutex mu;                      // guards the default scratch block
+  int* d_err = nullptr;               // device-side timeout flag
   int64_t bandwidth_gbs = 0;
   int launches = 0;
 };
@@ -176,6 +187,59 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
   };
   guards(A, md, &t.ag_row, &t.ag_k, &t.ag_ub, &t.a_ng);
   guards(B, nd, &t.bg_row, &t.bg_k, &t.bg_ub, &t.b_ng);
+
+  auto ktab_a = table(kd, A.coef, 0), ktab_b = table(kd, B.coef, 0);
+  t.a_kcontig = ktab_a.size() < 2 || ktab_a[1] - ktab_a[0] == 1;
+  t.b_kcontig = ktab_b.size() < 2 || ktab_b[1] - ktab_b[0] == 1;
+  auto ctab = table(nd, d.out_coef, 0);
+  t.unit_cols = true;
+  for (size_t j = 0; j < ctab.size(); ++j) t.unit_cols = t.unit_cols && ctab[j] == (int64_t)j;
+  if (c->opt.precision != ltb::Precision::fp32 && c->opt.use_tensor_cores &&
+      con.M < (1LL << 31) && con.N < (1LL << 31)) {
+    t.tc = true;
+    // split-BF16 along K: bit s of a mask selects hi (1) or lo (0) for
+    // segment s.  bf16x3: A' = [Ah|Al|Ah], B' = [Bh|Bh|Bl] (Al*Bl dropped);
+    // bf16x4 adds Al*Bl: A' = [Ah|Al|Ah|Al], B' = [Bh|Bh|Bl|Bl].
+    switch (c->opt.precision) {
+      case ltb::Precision::bf16x3: t.nseg = 3; t.a_mask = 0x5; t.b_mask = 0x3; break;
+      case ltb::Precision::bf16x4: t.nseg = 4; t.a_mask = 0x5; t.b_mask = 0x3; break;
+      default: t.nseg = 1; t.a_mask = 0x1; t.b_mask = 0x1; break;
+    }
+    t.Kp = (t.nseg * con.K + 7) / 8 * 8;
+    const size_t abytes = (size_t)con.M * t.Kp * 2, bbytes = (size_t)con.N * t.Kp * 2;
+    CUDA_TRY(cudaMalloc(&t.a_pack, abytes));
+    c->owned.push_back(t.a_pack);
+    CUDA_TRY(cudaMalloc(&t.b_pack, bbytes));
+    c->owned.push_back(t.b_pack);
+    // K padding columns stay zero for the life of the buffers
+    CUDA_TRY(cudaMemset(t.a_pack, 0, abytes));
+    CUDA_TRY(cudaMemset(t.b_pack, 0, bbytes));
+    alignas(64) unsigned char maps[256];
+    CUDA_TRY(ltb_make_tmap(maps, t.a_pack, con.M, t.Kp, ltb_tc_tile_m()));
+    CUDA_TRY(ltb_make_tmap(maps + 128, t.b_pack, con.N, t.Kp, ltb_tc_tile_n()));
+    CUDA_TRY(cudaMalloc(&t.d_maps, 256));
+    c->owned.push_back(t.d_maps);
+    CUDA_TRY(cudaMemcpy(t.d_maps, maps, 256, cudaMemcpyHostToDevice));
+    const int tm = (int)((con.M + ltb_tc_tile_m() - 1) / ltb_tc_tile_m());
+    const int64_t tn = (con.N + ltb_tc_tile_n() - 1) / ltb_tc_tile_n();
+    t.tiles = tm * tn;
+    // per-batch problem entries; the output pointer is patched in per run
+    std::vector<LtbTcProblem> pe(t.nbatch);
+    for (auto& e : pe) {
+      e.map_a = t.d_maps;
+      e.map_b = static_cast<char*>(t.d_maps) + 128;
+      e.c = nullptr;
+      e.crow = t.c_row;
+      e.ccol = t.c_col;
+      e.Kp = t.Kp;
+      e.tile_start = 0;
+      e.M = (int)con.M;
+      e.N = (int)con.N;
+      e.tiles_m = tm;
+      e.unit_cols = t.unit_cols ? 1 : 0;
+    }
+    t.d_prob = upload(pe, c->owned);
+  }
 }
 
 void compile_device(ltb_compiled* c) {
@@ -228,6 +292,9 @@ void compile_device(ltb_compiled* c) {
   std::vector<LtbStage> hs;
   for (auto& st : P.stages) hs.push_back(st.dev);
   if (!hs.empty()) c->d_stages = upload(hs, c->owned);
+  CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&c->d_err), sizeof(int)));
+  c->owned.push_back(c->d_err);
+  CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
   for (int i = 0; i < ns; ++i) {
     if (P.stages[i].family != ltb::Family::contraction) continue;
     GemmTables t;
@@ -242,7 +309,8 @@ void compile_device(ltb_compiled* c) {
     if (st.family == ltb::Family::row_chain) {
       if (st.rows_from == i) launches++;
     } else if (st.family == ltb::Family::contraction) {
-      launches += (int)c->gemms[c->gemm_of[i]].nbatch;
+      const auto& t = c->gemms[c->gemm_of[i]];
+      launches += (int)t.nbatch * (t.tc ? 3 : 1);
     } else {
       launches += c->split_of[i] > 1 ? 2 : 1;
     }
@@ -298,7 +366,15 @@ void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
           p.M = s.con.M;
           p.N = s.con.N;
           p.K = s.con.K;
-          e = ltb_launch_gemm_simt(p, c->sms, st);
+          if (!t.tc) {
+            e = ltb_launch_gemm_simt(p, c->sms, st);
+            continue;
+          }
+          e = ltb_launch_pack(p.a, p.M, p.K, t.a_pack, t.Kp, t.nseg, t.a_mask, t.a_kcontig, st);
+          if (e == cudaSuccess)
+            e = ltb_launch_pack(p.b, p.N, p.K, t.b_pack, t.Kp, t.nseg, t.b_mask, t.b_kcontig, st);
+          if (e == cudaSuccess)
+            e = ltb_launch_gemm_tc(t.d_prob + b, 1, t.tiles, p.c, c->sms, c->d_err, st);
         }
         break;
       }
@@ -354,7 +430,15 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
       CUDA_TRY(cudaMemcpyAsync(s.second, bt.p[s.first], bytes, cudaMemcpyDeviceToHost, st));
     }
     for (void* d : temps) CUDA_TRY(cudaFreeAsync(d, st));
-    if (sync || !temps.empty()) CUDA_TRY(cudaStreamSynchronize(st));
+    if (sync || !temps.empty()) {
+      CUDA_TRY(cudaStreamSynchronize(st));
+      int flag = 0;
+      CUDA_TRY(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (flag) {
+        CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
+        return fail(LTB_ERR_TIMEOUT, "a bounded wait in a tensor-core kernel gave up");
+      }
+    }
   } catch (const CudaFailure& e) {
     return fail(LTB_ERR_CUDA, e.what());
   } catch (const std::exception& e) {

@@ -1,0 +1,39 @@
+// Host API of the tcgen05 contraction kernels (gemm_tc.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.h"
+
+// One GEMM problem of a (possibly grouped) persistent launch.  Lives in
+// device memory; map_a / map_b point at CUtensorMaps in device memory.
+struct LtbTcProblem {
+  const void* map_a;     // CUtensorMap over A' [M, Kp] BF16 K-major
+  const void* map_b;     // CUtensorMap over B' [N, Kp] BF16 K-major
+  float* c;
+  const int64_t* crow;   // [M] output row offsets
+  const int64_t* ccol;   // [N] output column offsets (unused if unit_cols)
+  int64_t Kp;
+  int64_t tile_start;    // first global tile index of this problem
+  int M, N;
+  int tiles_m;
+  int unit_cols;         // ccol[j] == j
+};
+
+// CUtensorMap (128 bytes, 64-byte aligned) over a K-major BF16 matrix
+// [rows, Kp] (Kp a multiple of 8 so the row pitch is 16-byte aligned),
+// boxes of 64 x box_rows with 128-byte swizzle.
+cudaError_t ltb_make_tmap(void* map, const void* base, int64_t rows, int64_t Kp, int box_rows);
+
+// FP32 operand -> BF16 K-major segments (hi / lo split per segment).
+cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
+                            int64_t Kp, int nseg, int seg_mask, int k_contig, cudaStream_t st);
+
+// Persistent grouped launch over every tile of every problem
+// (tiles_m * ceil(N / tile_n) tiles per problem).  c_override, if not null,
+// replaces every problem's output pointer (single-problem launches).
+cudaError_t ltb_launch_gemm_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
+                               float* c_override, int sms, int* err, cudaStream_t st);
+int ltb_tc_tile_m();
+int ltb_tc_tile_n();
+size_t ltb_tc_smem_bytes();
