@@ -13,6 +13,7 @@ constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8, NT = 256;
 __device__ __forceinline__ float gather(const LtbGemmOperand& op, int64_t r,
                                         int64_t k, int64_t rows, int64_t K) {
   if (r >= rows || k >= K) return 0.f;
+  if (op.dense) return __ldg(op.base + r * op.ld_row + k * op.ld_k);
   for (int g = 0; g < op.nguard; ++g) {
     const int32_t v = op.grow[(int64_t)g * rows + r] + op.gk[(int64_t)g * K + k];
     if (v < 0 || v >= op.gub[g]) return 0.f;

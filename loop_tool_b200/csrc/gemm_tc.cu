@@ -151,6 +151,19 @@ __device__ __forceinline__ int find_problem(const LtbTcProblem* __restrict__ P, 
   return lo;
 }
 
+// Grouped raster: tiles advance along M in groups of kGroupM row blocks, so
+// the ~148 tiles in flight cover a compact 16 x 9 block region whose A and
+// B panels stay resident in L2.
+constexpr int kGroupM = 16;
+__device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, int* m0, int* n0) {
+  const int64_t per_group = (int64_t)kGroupM * p.tiles_n;
+  const int g = (int)(lt / per_group);
+  const int idx = (int)(lt - (int64_t)g * per_group);
+  const int gm = p.tiles_m - g * kGroupM < kGroupM ? p.tiles_m - g * kGroupM : kGroupM;
+  *m0 = (g * kGroupM + idx % gm) * BM;
+  *n0 = (idx / gm) * BN;
+}
+
 __global__ void __launch_bounds__(NT, 1)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
               float* c_override, int* err) {
@@ -193,8 +206,8 @@ __global__ void __launch_bounds__(NT, 1)
     bool alive = true;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       const LtbTcProblem& p = probs[find_problem(probs, nprob, t)];
-      const int64_t lt = t - p.tile_start;
-      const int m0 = (int)(lt % p.tiles_m) * BM, n0 = (int)(lt / p.tiles_m) * BN;
+      int m0, n0;
+      tile_coords(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % STAGES;
@@ -252,8 +265,8 @@ __global__ void __launch_bounds__(NT, 1)
     bool alive = true;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       const LtbTcProblem& p = probs[find_problem(probs, nprob, t)];
-      const int64_t lt = t - p.tile_start;
-      const int m0 = (int)(lt % p.tiles_m) * BM, n0 = (int)(lt / p.tiles_m) * BN;
+      int m0, n0;
+      tile_coords(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
       float run[128];
 #pragma unroll
@@ -310,31 +323,81 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 // ------------------------------------------------------------ packing
-// Gathers an operand tile through its separable description and writes the
-// BF16 split of every element into nseg K-segments of a K-major matrix:
-// bit s of seg_mask selects the hi part (1) or the lo part (0, x - hi
-// rounded to BF16) for segment s.
+// Gathers an operand through its separable description and writes the BF16
+// split of every element into nseg K-segments of a K-major matrix: bit s of
+// seg_mask selects the hi part (1) or the lo part (0, x - hi rounded to
+// BF16) for segment s.
+__device__ __forceinline__ float pack_fetch(const LtbGemmOperand& op, int64_t rows, int64_t K,
+                                            int64_t r, int64_t k) {
+  if (r >= rows || k >= K) return 0.f;
+  if (op.dense) return __ldg(op.base + r * op.ld_row + k * op.ld_k);
+  for (int g = 0; g < op.nguard; ++g) {
+    const int32_t v = op.grow[(int64_t)g * rows + r] + op.gk[(int64_t)g * K + k];
+    if (v < 0 || v >= op.gub[g]) return 0.f;
+  }
+  return __ldg(op.base + op.rowoff[r] + op.koff[k]);
+}
+
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// Operands contiguous along k: 4 consecutive k per thread, 128-bit loads and
+// 64-bit stores when the dense layout allows.
 __global__ void __launch_bounds__(256)
-    k_pack(LtbGemmOperand op, int64_t rows, int64_t K, __nv_bfloat16* __restrict__ out,
-           int64_t Kp, int nseg, int seg_mask, int k_contig) {
+    k_pack_k(LtbGemmOperand op, int64_t rows, int64_t K, __nv_bfloat16* __restrict__ out,
+             int64_t Kp, int nseg, int seg_mask) {
+  const int64_t k4n = (K + 3) / 4;
+  const bool vec = op.dense && op.ld_k == 1 && (op.ld_row & 3) == 0 &&
+                   ((reinterpret_cast<uintptr_t>(op.base) & 15) == 0) && (K & 3) == 0;
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < rows * k4n;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = w / k4n, k = (w - r * k4n) * 4;
+    float x[4];
+    if (vec) {
+      const float4 t = __ldg(reinterpret_cast<const float4*>(op.base + r * op.ld_row + k));
+      x[0] = t.x; x[1] = t.y; x[2] = t.z; x[3] = t.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) x[e] = pack_fetch(op, rows, K, r, k + e);
+    }
+    __nv_bfloat16 hi[4], lo[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) split_bf16(x[e], hi[e], lo[e]);
+    __nv_bfloat16* dst = out + r * Kp + k;
+    for (int s = 0; s < nseg; ++s) {
+      const __nv_bfloat16* v = (seg_mask >> s) & 1 ? hi : lo;
+      __nv_bfloat16* d = dst + s * K;
+      if (vec && ((r * Kp + s * K + k) & 3) == 0) {
+        __nv_bfloat162 a, b;
+        a.x = v[0]; a.y = v[1]; b.x = v[2]; b.y = v[3];
+        uint2 u;
+        u.x = *reinterpret_cast<uint32_t*>(&a);
+        u.y = *reinterpret_cast<uint32_t*>(&b);
+        *reinterpret_cast<uint2*>(d) = u;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (k + e < K) d[e] = v[e];
+      }
+    }
+  }
+}
+
+// Operands contiguous along rows (e.g. B[k, n] feeding B'[n, k]): a 32 x 32
+// tile transposed through shared memory, reads coalesced along rows, writes
+// coalesced along k.
+__global__ void __launch_bounds__(256)
+    k_pack_r(LtbGemmOperand op, int64_t rows, int64_t K, __nv_bfloat16* __restrict__ out,
+             int64_t Kp, int nseg, int seg_mask) {
   __shared__ float tile[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 32;
-  auto fetch = [&](int64_t r, int64_t k) -> float {
-    if (r >= rows || k >= K) return 0.f;
-    for (int g = 0; g < op.nguard; ++g) {
-      const int32_t v = op.grow[(int64_t)g * rows + r] + op.gk[(int64_t)g * K + k];
-      if (v < 0 || v >= op.gub[g]) return 0.f;
-    }
-    return __ldg(op.base + op.rowoff[r] + op.koff[k]);
-  };
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int a = ty + 8 * q;
-    if (k_contig)
-      tile[a][tx] = fetch(r0 + a, k0 + tx);  // coalesced along k
-    else
-      tile[tx][a] = fetch(r0 + tx, k0 + a);  // coalesced along rows
+    tile[tx][a] = pack_fetch(op, rows, K, r0 + tx, k0 + a);
   }
   __syncthreads();
 #pragma unroll
@@ -342,9 +405,8 @@ __global__ void __launch_bounds__(256)
     const int a = ty + 8 * q;
     const int64_t r = r0 + a, k = k0 + tx;
     if (r >= rows || k >= K) continue;
-    const float x = tile[a][tx];
-    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+    __nv_bfloat16 hi, lo;
+    split_bf16(tile[a][tx], hi, lo);
     __nv_bfloat16* dst = out + r * Kp + k;
     for (int s = 0; s < nseg; ++s) dst[s * K] = (seg_mask >> s) & 1 ? hi : lo;
   }
@@ -384,10 +446,17 @@ int ltb_tc_tile_n() { return BN; }
 
 cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
                             int64_t Kp, int nseg, int seg_mask, int k_contig, cudaStream_t st) {
-  dim3 grid((unsigned)((K + 31) / 32), (unsigned)((rows + 31) / 32));
-  if (grid.y > 65535) return cudaErrorInvalidConfiguration;
-  k_pack<<<grid, 256, 0, st>>>(op, rows, K, static_cast<__nv_bfloat16*>(out), Kp, nseg, seg_mask,
-                               k_contig);
+  __nv_bfloat16* o = static_cast<__nv_bfloat16*>(out);
+  if (k_contig) {
+    const int64_t work = rows * ((K + 3) / 4);
+    int64_t blocks = (work + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_pack_k<<<(unsigned)blocks, 256, 0, st>>>(op, rows, K, o, Kp, nseg, seg_mask);
+  } else {
+    dim3 grid((unsigned)((K + 31) / 32), (unsigned)((rows + 31) / 32));
+    if (grid.y > 65535) return cudaErrorInvalidConfiguration;
+    k_pack_r<<<grid, 256, 0, st>>>(op, rows, K, o, Kp, nseg, seg_mask);
+  }
   return cudaGetLastError();
 }
 

@@ -27,6 +27,10 @@ struct LtbGemmOperand {
   const float* base;
   const int64_t* rowoff;  // [rows]
   const int64_t* koff;    // [K]
+  // dense operands (no guards, rowoff[i] = i*ld_row, koff[k] = k*ld_k):
+  // addresses are computed instead of read from the tables
+  int dense;
+  int64_t ld_row, ld_k;
   int nguard;
   const int32_t* grow;    // [nguard][rows] guard partial from the row coords
   const int32_t* gk;      // [nguard][K]   guard partial from the k coords

@@ -73,6 +73,8 @@ struct GemmTables {
   int32_t *ag_row = nullptr, *ag_k = nullptr, *ag_ub = nullptr;
   int32_t *bg_row = nullptr, *bg_k = nullptr, *bg_ub = nullptr;
   int a_ng = 0, b_ng = 0;
+  bool a_dense = false, b_dense = false;
+  int64_t a_ldr = 0, a_ldk = 0, b_ldr = 0, b_ldk = 0;
   // tensor-core path: packed K-major BF16 operands and their tensor maps
   bool tc = false;
   int nseg = 1, a_mask = 1, b_mask = 1;
@@ -189,6 +191,18 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
   guards(B, nd, &t.bg_row, &t.bg_k, &t.bg_ub, &t.b_ng);
 
   auto ktab_a = table(kd, A.coef, 0), ktab_b = table(kd, B.coef, 0);
+  // dense = offsets are an arithmetic progression in the flat row / k index
+  auto arith = [](const std::vector<int64_t>& v, int64_t* step) {
+    *step = v.size() > 1 ? v[1] - v[0] : 0;
+    for (size_t i = 1; i < v.size(); ++i)
+      if (v[i] - v[i - 1] != *step) return false;
+    return true;
+  };
+  {
+    auto ra = table(md, A.coef, A.off), rb = table(nd, B.coef, B.off);
+    t.a_dense = A.ng == 0 && ra[0] == 0 && arith(ra, &t.a_ldr) && arith(ktab_a, &t.a_ldk);
+    t.b_dense = B.ng == 0 && rb[0] == 0 && arith(rb, &t.b_ldr) && arith(ktab_b, &t.b_ldk);
+  }
   t.a_kcontig = ktab_a.size() < 2 || ktab_a[1] - ktab_a[0] == 1;
   t.b_kcontig = ktab_b.size() < 2 || ktab_b[1] - ktab_b[0] == 1;
   auto ctab = table(nd, d.out_coef, 0);
@@ -236,6 +250,7 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
       e.M = (int)con.M;
       e.N = (int)con.N;
       e.tiles_m = tm;
+      e.tiles_n = (int)tn;
       e.unit_cols = t.unit_cols ? 1 : 0;
     }
     t.d_prob = upload(pe, c->owned);
@@ -358,8 +373,10 @@ void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
           LtbGemmProblem p{};
           const LtbLoad& A = s.dev.loads[s.con.a_load];
           const LtbLoad& B = s.dev.loads[s.con.b_load];
-          p.a = {bt.p[A.buf] + t.a_boff[b], t.a_row, t.a_k, t.a_ng, t.ag_row, t.ag_k, t.ag_ub};
-          p.b = {bt.p[B.buf] + t.b_boff[b], t.b_row, t.b_k, t.b_ng, t.bg_row, t.bg_k, t.bg_ub};
+          p.a = {bt.p[A.buf] + t.a_boff[b], t.a_row, t.a_k, t.a_dense ? 1 : 0, t.a_ldr, t.a_ldk,
+                 t.a_ng, t.ag_row, t.ag_k, t.ag_ub};
+          p.b = {bt.p[B.buf] + t.b_boff[b], t.b_row, t.b_k, t.b_dense ? 1 : 0, t.b_ldr, t.b_ldk,
+                 t.b_ng, t.bg_row, t.bg_k, t.bg_ub};
           p.c = bt.p[s.dev.out_buf] + t.c_boff[b];
           p.crow = t.c_row;
           p.ccol = t.c_col;

@@ -16,7 +16,7 @@ struct LtbTcProblem {
   int64_t Kp;
   int64_t tile_start;    // first global tile index of this problem
   int M, N;
-  int tiles_m;
+  int tiles_m, tiles_n;
   int unit_cols;         // ccol[j] == j
 };
 
