@@ -251,6 +251,20 @@ static std::string read_file(const std::string& path) {
 }
 
 int main(int argc, char** argv) {
+  // LT_PLUGIN=<backend plugin .so>: load it (backend.cpp:63-65) and make its
+  // "cuda" backend and hardware the defaults, as a user switching backends
+  // would (backend.cpp:53-61, hardware.cpp:61).
+  if (const char* plugin = std::getenv("LT_PLUGIN")) {
+    try {
+      loop_tool::loadLibrary(plugin);
+      loop_tool::setDefaultBackend("cuda");
+      for (auto& hw : loop_tool::getHardware())
+        if (hw->name() == "cuda") loop_tool::setDefaultHardwareId(hw->id());
+    } catch (const std::exception& e) {
+      std::cerr << "plugin error: " << e.what() << "\n";
+      return 5;
+    }
+  }
   if (argc < 3) {
     std::cerr << "usage: lt_ref_harness ir|run|tree|code|sizes ...\n";
     return 2;
