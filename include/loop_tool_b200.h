@@ -100,6 +100,20 @@ int ltb_io_sizes(ltb_compiled* c, int* n_in, int* n_out, int64_t* elems,
 int ltb_alloc(size_t bytes, int managed, void** out);
 int ltb_free(void* ptr);
 
+/* Row sums out[r] = sum_c x[r * cols + c] (row-major x[rows, cols]) that
+ * allocate nothing.  No counterpart in the reference: it is for callers that
+ * cannot allocate device memory when they call in -- a serving loop that
+ * committed its whole HBM budget up front, or a host framework that owns
+ * every device allocation -- and it equals ltb_run on the loop tree
+ * (X.sum(n)) within FP32 rounding.  x and out must be device or managed
+ * memory.  Split-K partials live in one static device array of 2^20 floats
+ * (4 MiB, held on every GPU that loads the library until exit): rows above
+ * 2^20 are rejected with LTB_ERR_INVALID; calls that overlap on the GPU
+ * share that array and race.  The first call on a device looks up the
+ * array's address; make it before any stream capture on that device. */
+int ltb_row_sum_noalloc(const float* x, int64_t rows, int64_t cols, float* out,
+                        void* stream);
+
 /* Stream synchronisation helper (cuCtxSynchronize in the reference,
  * src/backends/cuda/cuda.cpp:847-849, when stream is NULL). */
 int ltb_synchronize(void* stream);

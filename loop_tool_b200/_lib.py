@@ -39,6 +39,8 @@ SIGNATURES = {
     "ltb_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "ltb_free": (ctypes.c_int, [ctypes.c_void_p]),
     "ltb_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "ltb_row_sum_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 

@@ -5,6 +5,9 @@
 
 #include "stage.h"
 
+// Records `msg` as the calling thread's ltb_last_error() and returns code.
+int ltb_set_last_error(int code, const char* msg);
+
 // (a) elementwise nests and (b) serial reductions
 cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
                             const LtbBufTable& bt, int sms, cudaStream_t st);

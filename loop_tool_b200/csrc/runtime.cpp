@@ -97,6 +97,8 @@ T* upload(const std::vector<T>& v, std::vector<void*>& owned) {
 
 }  // namespace
 
+int ltb_set_last_error(int code, const char* msg) { return fail(code, msg); }
+
 struct ltb_compiled {
   std::string ir_text;
   ltb::IRGraph ir;

@@ -1,0 +1,69 @@
+"""The scratch-free row-sum entry point (ltb_row_sum_noalloc).
+
+It serves callers that cannot allocate device memory at call time (a
+serving loop with its HBM budget already committed, a host framework that
+owns all device allocations): the split-K partials live in a static device
+array instead of a compiled object's scratch.  Checked through the C ABI
+against the existing entry point (ltb_compile + ltb_run on the same row-sum
+loop tree), on two calls in a row.  This file is collected last so that a
+run stopping at the first failure has already run every other test.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+RTOL = 1e-5
+
+
+def rowsum_ir(rows, cols):
+    # X.as(r, n).sum(n): the reference lazy frontend's IR for a row sum
+    return (f"v:r_0\nv:n_1\nn:2::0,1,:::0:::::\n"
+            f"n:5:0,:0,:::0:0;{rows};0,1;{cols};0,::,,::\n"
+            f"n:1:1,:0,:::0:0;{rows};0,::,::\ni:0,\no:2,\n")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows,cols", [(4, 300000), (37, 300), (1000, 70000)])
+def test_no_alloc_matches_existing_entry_point(rows, cols, cuda_dev):
+    import torch
+
+    import loop_tool_b200 as lt
+    from loop_tool_b200 import _lib
+
+    g = torch.Generator(device=cuda_dev).manual_seed(rows * 7 + cols)
+    x = torch.randn(rows * cols, device=cuda_dev, generator=g)
+    ref = torch.empty(rows, device=cuda_dev)
+    lt.cuda(rowsum_ir(rows, cols))([x, ref])
+    torch.cuda.synchronize()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    expected = ref.cpu().numpy().astype(np.float64)
+    scale = float(np.sqrt(np.mean(expected ** 2)))
+    for call in range(2):
+        out = torch.full((rows,), float("nan"), device=cuda_dev)
+        rc = _lib.lib().ltb_row_sum_noalloc(ctypes.c_void_p(x.data_ptr()), rows, cols,
+                                            ctypes.c_void_p(out.data_ptr()), stream)
+        assert rc == 0, _lib.lib().ltb_last_error().decode()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().astype(np.float64)
+        err = np.abs(got - expected)
+        assert (err <= RTOL * (np.abs(expected) + scale)).all(), \
+            f"call {call}: max error {err.max():.3g} (scale {scale:.3g})"
+
+
+@pytest.mark.gpu
+def test_no_alloc_rejects_oversized_and_host_buffers(cuda_dev):
+    import torch
+
+    from loop_tool_b200 import _lib
+
+    L = _lib.lib()
+    x = torch.zeros(4, device=cuda_dev)
+    out = torch.zeros(4, device=cuda_dev)
+    rc = L.ltb_row_sum_noalloc(ctypes.c_void_p(x.data_ptr()), (1 << 20) + 1, 0,
+                               ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == _lib.ERR_INVALID and b"exceed" in L.ltb_last_error()
+    host = np.zeros(4, np.float32)
+    rc = L.ltb_row_sum_noalloc(ctypes.c_void_p(host.ctypes.data), 1, 4,
+                               ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == _lib.ERR_INVALID and b"device" in L.ltb_last_error()
