@@ -36,6 +36,7 @@ extern "C" {
 #define LTB_ERR_TIMEOUT 5      /* a bounded device wait gave up */
 
 typedef struct ltb_compiled ltb_compiled;
+typedef struct ltb_batch ltb_batch;
 
 /* ABI version (increments on incompatible change). */
 int ltb_abi_version(void);
@@ -99,6 +100,23 @@ int ltb_io_sizes(ltb_compiled* c, int* n_in, int* n_out, int64_t* elems,
  * compatible); managed == 0 is plain device memory. */
 int ltb_alloc(size_t bytes, int managed, void** out);
 int ltb_free(void* ptr);
+
+/* Batches of contractions.  No single counterpart in the reference, which
+ * runs one loop tree per Compiled::run (backend.h:20-21); a batch runs n
+ * compiled single-contraction loop trees (e.g. matmuls of uneven sizes,
+ * one precision) as one grouped launch -- one operand-packing launch and one
+ * persistent tensor-core launch over every tile of every problem (FP32: one
+ * grouped CUDA-core launch).  memories[i] are the device buffers of member
+ * i in Compiled::run order, bound at creation. */
+int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int n,
+                     ltb_batch** out);
+/* Records the batch's launches once into a CUDA graph (stream must not be
+ * the legacy default stream); later ltb_batch_run calls replay it. */
+int ltb_batch_capture(ltb_batch* b, void* stream);
+int ltb_batch_run(ltb_batch* b, int sync, void* stream);
+/* "problems", "flops", "launches", "tiles", "graph". */
+int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value);
+int ltb_batch_release(ltb_batch* b);
 
 /* Row sums out[r] = sum_c x[r * cols + c] (row-major x[rows, cols]) that
  * allocate nothing.  No counterpart in the reference: it is for callers that

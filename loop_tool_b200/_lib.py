@@ -41,6 +41,14 @@ SIGNATURES = {
     "ltb_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "ltb_row_sum_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "ltb_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.POINTER(ctypes.POINTER(ctypes.c_void_p)),
+                                        ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "ltb_batch_capture": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "ltb_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "ltb_batch_int_property": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p,
+                                              ctypes.POINTER(ctypes.c_int64)]),
+    "ltb_batch_release": (ctypes.c_int, [ctypes.c_void_p]),
 }
 
 

@@ -175,3 +175,42 @@ class RawTensor:
         if getattr(self, "ptr", None) and _lib._lib is not None:
             _lib.lib().ltb_free(self.ptr)
             self.ptr = None
+
+
+class Batch:
+    """Many compiled contractions run as one grouped launch (optionally a
+    captured CUDA graph): the batched-uneven-matmul form of family (c).
+    `members` is a list of (Compiled, [device buffers in run order])."""
+
+    def __init__(self, members, capture_stream=None):
+        n = len(members)
+        self._keep = members
+        hs = (ctypes.c_void_p * n)(*[c._h.value for c, _ in members])
+        rows = []
+        for c, bufs in members:
+            ptrs = [_ptr_and_keep(t)[0] for t in bufs]
+            rows.append((ctypes.c_void_p * len(ptrs))(*ptrs))
+        self._rows = rows
+        mem = (ctypes.POINTER(ctypes.c_void_p) * n)(
+            *[ctypes.cast(r, ctypes.POINTER(ctypes.c_void_p)) for r in rows])
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ltb_batch_create(hs, mem, n, ctypes.byref(h)))
+        self._h = h
+        if capture_stream is not None:
+            _lib.check(_lib.lib().ltb_batch_capture(h, capture_stream))
+
+    def run(self, sync=True, stream=None):
+        if stream is None:
+            stream = _current_stream()
+        _lib.check(_lib.lib().ltb_batch_run(self._h, int(bool(sync)), stream))
+
+    def int_property(self, name):
+        v = ctypes.c_int64()
+        _lib.check(_lib.lib().ltb_batch_int_property(self._h, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib._lib is not None:
+            _lib.lib().ltb_batch_release(h)
+            self._h = None

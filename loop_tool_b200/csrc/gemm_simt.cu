@@ -21,12 +21,34 @@ __device__ __forceinline__ float gather(const LtbGemmOperand& op, int64_t r,
   return __ldg(op.base + op.rowoff[r] + op.koff[k]);
 }
 
+__device__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, int64_t j0);
+
 __global__ void __launch_bounds__(NT)
     k_gemm_simt(LtbGemmProblem p) {
+  gemm_tile(p, (int64_t)blockIdx.y * BM, (int64_t)blockIdx.x * BN);
+}
+
+// one CTA per 128 x 128 tile of any problem of the batch
+__global__ void __launch_bounds__(NT)
+    k_gemm_simt_grouped(const LtbGemmProblem* __restrict__ probs,
+                        const int64_t* __restrict__ tile_start, int nprob) {
+  const int64_t t = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const LtbGemmProblem p = probs[lo];
+  const int64_t lt = t - tile_start[lo];
+  const int64_t tn = (p.N + BN - 1) / BN;
+  gemm_tile(p, (lt / tn) * BM, (lt % tn) * BN);
+}
+
+__device__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, int64_t j0) {
   __shared__ float As[2][BK][BM];
   __shared__ float Bs[2][BK][BN];
   const int tid = threadIdx.x;
-  const int64_t i0 = (int64_t)blockIdx.y * BM, j0 = (int64_t)blockIdx.x * BN;
   // loader mapping: A tile 128 rows x 8 k -> thread loads 4 k of one row
   const int a_r = tid >> 1, a_k = (tid & 1) * 4;
   // B tile 8 k x 128 cols -> thread loads 4 cols of one k
@@ -97,5 +119,13 @@ cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms,
   dim3 grid((unsigned)((p.N + BN - 1) / BN), (unsigned)((p.M + BM - 1) / BM));
   if (grid.y > 65535) return cudaErrorInvalidConfiguration;
   k_gemm_simt<<<grid, NT, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t ltb_launch_gemm_simt_grouped(const LtbGemmProblem* d_probs,
+                                         const int64_t* d_tile_start, int nprob,
+                                         int64_t total_tiles, cudaStream_t st) {
+  if (total_tiles > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  k_gemm_simt_grouped<<<(unsigned)total_tiles, NT, 0, st>>>(d_probs, d_tile_start, nprob);
   return cudaGetLastError();
 }

@@ -412,6 +412,46 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Every operand of a batch in one launch: CTAs stride over the 32 x 32
+// tiles of all jobs (job found by binary search on tile_start).
+__global__ void __launch_bounds__(256)
+    k_pack_grouped(const LtbPackJob* __restrict__ jobs, int njobs, int64_t total_tiles) {
+  __shared__ float tile[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].tile_start <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const LtbPackJob& J = jobs[lo];
+    const int64_t lt = t - J.tile_start;
+    const int64_t r0 = (lt / J.tiles_k) * 32, k0 = (lt % J.tiles_k) * 32;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int a = ty + 8 * q;
+      if (J.k_contig)
+        tile[a][tx] = pack_fetch(J.op, J.rows, J.K, r0 + a, k0 + tx);
+      else
+        tile[tx][a] = pack_fetch(J.op, J.rows, J.K, r0 + tx, k0 + a);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int a = ty + 8 * q;
+      const int64_t r = r0 + a, k = k0 + tx;
+      if (r < J.rows && k < J.K) {
+        __nv_bfloat16 hi, lo;
+        split_bf16(tile[a][tx], hi, lo);
+        __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(J.out) + r * J.Kp + k;
+        for (int s = 0; s < J.nseg; ++s) dst[s * J.K] = (J.seg_mask >> s) & 1 ? hi : lo;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -457,6 +497,13 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
     if (grid.y > 65535) return cudaErrorInvalidConfiguration;
     k_pack_r<<<grid, 256, 0, st>>>(op, rows, K, o, Kp, nseg, seg_mask);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t total_tiles,
+                                    int sms, cudaStream_t st) {
+  const int64_t grid = total_tiles < (int64_t)sms * 8 ? total_tiles : (int64_t)sms * 8;
+  k_pack_grouped<<<(unsigned)grid, 256, 0, st>>>(d_jobs, njobs, total_tiles);
   return cudaGetLastError();
 }
 

@@ -51,3 +51,8 @@ struct LtbGemmProblem {
 // FP32 CUDA-core path (exact fp32 FMA): the "plain FP32" baseline family.
 cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms,
                                  cudaStream_t st);
+// Many problems in one launch: tile_start[i] = first 128 x 128 tile of
+// problem i (device arrays), total_tiles tiles in all.
+cudaError_t ltb_launch_gemm_simt_grouped(const LtbGemmProblem* d_probs,
+                                         const int64_t* d_tile_start, int nprob,
+                                         int64_t total_tiles, cudaStream_t st);

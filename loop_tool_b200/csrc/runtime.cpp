@@ -476,9 +476,221 @@ int copy_out(const std::string& s, char* buf, size_t len) {
 
 }  // namespace
 
+// ------------------------------------------------------------------ batch
+// Many compiled contractions (e.g. 512 uneven matmuls) run as one grouped
+// launch: one pack launch over every operand, one persistent tensor-core
+// launch over every tile of every problem (or one grouped FP32 launch),
+// optionally captured once into a CUDA graph and replayed.
+struct ltb_batch {
+  int device = 0, sms = 148;
+  bool tc = false;
+  int n = 0;
+  LtbPackJob* d_jobs = nullptr;
+  int njobs = 0;
+  int64_t pack_tiles = 0;
+  LtbTcProblem* d_tc = nullptr;
+  int64_t tc_tiles = 0;
+  LtbGemmProblem* d_simt = nullptr;
+  int64_t* d_simt_start = nullptr;
+  int64_t simt_tiles = 0;
+  int* d_err = nullptr;
+  double flops = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<void*> owned;
+};
+
+namespace {
+
+void batch_launch(ltb_batch* b, cudaStream_t st) {
+  if (b->tc) {
+    CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st));
+    CUDA_TRY(ltb_launch_gemm_tc(b->d_tc, b->n, b->tc_tiles, nullptr, b->sms, b->d_err, st));
+  } else {
+    CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles, st));
+  }
+}
+
+int batch_finish(ltb_batch* b, int sync, cudaStream_t st) {
+  if (!sync) return LTB_OK;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  int flag = 0;
+  CUDA_TRY(cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(int)));
+    return fail(LTB_ERR_TIMEOUT, "a bounded wait in a tensor-core kernel gave up");
+  }
+  return LTB_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int ltb_abi_version(void) { return 1; }
+
+int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int n,
+                     ltb_batch** out) {
+  if (!cs || !memories || n <= 0 || !out) return fail(LTB_ERR_INVALID, "bad batch arguments");
+  *out = nullptr;
+  auto b = new ltb_batch();
+  try {
+    b->n = n;
+    b->device = cs[0]->device;
+    b->sms = cs[0]->sms;
+    std::vector<LtbPackJob> jobs;
+    std::vector<LtbTcProblem> tcp;
+    std::vector<LtbGemmProblem> sp;
+    std::vector<int64_t> sstart;
+    for (int i = 0; i < n; ++i) {
+      ltb_compiled* c = cs[i];
+      if (!c || c->device != b->device)
+        throw ltb::Error("batch members must be compiled on one device");
+      if (c->plan.stages.size() != 1 || c->plan.stages[0].family != ltb::Family::contraction)
+        throw ltb::Error("batch member " + std::to_string(i) + " is not a single contraction");
+      const auto& s = c->plan.stages[0];
+      const GemmTables& t = c->gemms[c->gemm_of[0]];
+      if (t.nbatch != 1) throw ltb::Error("batched contractions cannot join a batch");
+      if (i == 0) b->tc = t.tc;
+      if (t.tc != b->tc || (t.tc && t.nseg != cs[0]->gemms[0].nseg))
+        throw ltb::Error("batch members must share one precision");
+      const int nio = c->plan.n_in + c->plan.n_out;
+      for (int k = 0; k < nio; ++k)
+        if (!memories[i] || !memories[i][k] || !is_device_accessible(memories[i][k]))
+          throw ltb::Error("batch buffers must be device or managed memory");
+      auto ptr = [&](int slot) { return static_cast<float*>(memories[i][slot]); };
+      const LtbLoad& A = s.dev.loads[s.con.a_load];
+      const LtbLoad& B = s.dev.loads[s.con.b_load];
+      LtbGemmProblem p{};
+      p.a = {ptr(A.buf), t.a_row, t.a_k, t.a_dense ? 1 : 0, t.a_ldr, t.a_ldk, t.a_ng, t.ag_row,
+             t.ag_k, t.ag_ub};
+      p.b = {ptr(B.buf), t.b_row, t.b_k, t.b_dense ? 1 : 0, t.b_ldr, t.b_ldk, t.b_ng, t.bg_row,
+             t.bg_k, t.bg_ub};
+      p.c = ptr(s.dev.out_buf);
+      p.crow = t.c_row;
+      p.ccol = t.c_col;
+      p.M = s.con.M;
+      p.N = s.con.N;
+      p.K = s.con.K;
+      b->flops += 2.0 * p.M * p.N * p.K;
+      if (b->tc) {
+        auto job = [&](const LtbGemmOperand& op, int64_t rows, void* dst, int mask, bool kc) {
+          LtbPackJob j{};
+          j.op = op;
+          j.out = dst;
+          j.rows = rows;
+          j.K = p.K;
+          j.Kp = t.Kp;
+          j.tiles_k = (int)((p.K + 31) / 32);
+          j.tile_start = b->pack_tiles;
+          j.nseg = t.nseg;
+          j.seg_mask = mask;
+          j.k_contig = kc ? 1 : 0;
+          b->pack_tiles += ((rows + 31) / 32) * j.tiles_k;
+          jobs.push_back(j);
+        };
+        job(p.a, p.M, t.a_pack, t.a_mask, t.a_kcontig);
+        job(p.b, p.N, t.b_pack, t.b_mask, t.b_kcontig);
+        LtbTcProblem q{};
+        CUDA_TRY(cudaMemcpy(&q, t.d_prob, sizeof(q), cudaMemcpyDeviceToHost));
+        q.c = p.c;
+        q.tile_start = b->tc_tiles;
+        b->tc_tiles += t.tiles;
+        tcp.push_back(q);
+      } else {
+        sstart.push_back(b->simt_tiles);
+        b->simt_tiles += ((p.M + 127) / 128) * ((p.N + 127) / 128);
+        sp.push_back(p);
+      }
+    }
+    b->njobs = (int)jobs.size();
+    if (b->tc) {
+      b->d_jobs = upload(jobs, b->owned);
+      b->d_tc = upload(tcp, b->owned);
+    } else {
+      b->d_simt = upload(sp, b->owned);
+      b->d_simt_start = upload(sstart, b->owned);
+    }
+    CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&b->d_err), sizeof(int)));
+    b->owned.push_back(b->d_err);
+    CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(int)));
+  } catch (const CudaFailure& e) {
+    for (void* p : b->owned) cudaFree(p);
+    delete b;
+    return fail(LTB_ERR_CUDA, e.what());
+  } catch (const std::exception& e) {
+    for (void* p : b->owned) cudaFree(p);
+    delete b;
+    return fail(LTB_ERR_INVALID, e.what());
+  }
+  *out = b;
+  return LTB_OK;
+}
+
+int ltb_batch_run(ltb_batch* b, int sync, void* stream) {
+  if (!b) return fail(LTB_ERR_INVALID, "null batch");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  try {
+    CUDA_TRY(cudaSetDevice(b->device));
+    if (b->exec)
+      CUDA_TRY(cudaGraphLaunch(b->exec, st));
+    else
+      batch_launch(b, st);
+    return batch_finish(b, sync, st);
+  } catch (const std::exception& e) {
+    return fail(LTB_ERR_CUDA, e.what());
+  }
+}
+
+int ltb_batch_capture(ltb_batch* b, void* stream) {
+  if (!b) return fail(LTB_ERR_INVALID, "null batch");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!st) return fail(LTB_ERR_INVALID, "capture needs a non-default stream");
+  try {
+    CUDA_TRY(cudaSetDevice(b->device));
+    if (b->exec) {
+      cudaGraphExecDestroy(b->exec);
+      cudaGraphDestroy(b->graph);
+      b->exec = nullptr;
+      b->graph = nullptr;
+    }
+    CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      batch_launch(b, st);
+    } catch (...) {
+      cudaGraph_t g;
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CUDA_TRY(cudaStreamEndCapture(st, &b->graph));
+    CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  } catch (const std::exception& e) {
+    return fail(LTB_ERR_CUDA, e.what());
+  }
+  return LTB_OK;
+}
+
+int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
+  if (!b || !name || !value) return fail(LTB_ERR_INVALID, "null argument");
+  std::string k = name;
+  if (k == "problems") *value = b->n;
+  else if (k == "flops") *value = (int64_t)b->flops;
+  else if (k == "launches") *value = b->tc ? 2 : 1;
+  else if (k == "tiles") *value = b->tc ? b->tc_tiles : b->simt_tiles;
+  else if (k == "graph") *value = b->exec ? 1 : 0;
+  else return fail(LTB_ERR_INVALID, "unknown property " + k);
+  return LTB_OK;
+}
+
+int ltb_batch_release(ltb_batch* b) {
+  if (!b) return LTB_OK;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (void* p : b->owned) cudaFree(p);
+  delete b;
+  return LTB_OK;
+}
 
 const char* ltb_last_error(void) { return g_err.c_str(); }
 

@@ -20,6 +20,18 @@ struct LtbTcProblem {
   int unit_cols;         // ccol[j] == j
 };
 
+// One operand packing job of a grouped pack launch (32 x 32 tiles).
+struct LtbPackJob {
+  LtbGemmOperand op;
+  void* out;            // BF16 [rows, Kp]
+  int64_t rows, K, Kp;
+  int64_t tile_start;   // first global tile index of this job
+  int tiles_k;          // ceil(K / 32)
+  int nseg, seg_mask, k_contig;
+};
+cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t total_tiles,
+                                    int sms, cudaStream_t st);
+
 // CUtensorMap (128 bytes, 64-byte aligned) over a K-major BF16 matrix
 // [rows, Kp] (Kp a multiple of 8 so the row pitch is 16-byte aligned),
 // boxes of 64 x box_rows with 128-byte swizzle.
