@@ -166,7 +166,11 @@ __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, i
 
 __global__ void __launch_bounds__(NT, 1)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
-              float* c_override, int* err) {
+              float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
+              const __grid_constant__ CUtensorMap single_a,
+              const __grid_constant__ CUtensorMap single_b) {
+  // probs == nullptr: one problem passed by value with its tensor maps as
+  // kernel parameters (encoded at launch over per-run scratch)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -205,7 +209,11 @@ __global__ void __launch_bounds__(NT, 1)
     uint32_t g = 0;  // k blocks issued by this CTA so far
     bool alive = true;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
-      const LtbTcProblem& p = probs[find_problem(probs, nprob, t)];
+      const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
+      const CUtensorMap* ma =
+          probs ? static_cast<const CUtensorMap*>(p.map_a) : &single_a;
+      const CUtensorMap* mb =
+          probs ? static_cast<const CUtensorMap*>(p.map_b) : &single_b;
       int m0, n0;
       tile_coords(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
@@ -219,9 +227,8 @@ __global__ void __launch_bounds__(NT, 1)
         const uint32_t fb = smem_u32(&full[s]);
         mbar_expect_tx(fb, STAGE_BYTES);
         uint8_t* sa = smem + s * STAGE_BYTES;
-        tma_load_2d(smem_u32(sa), static_cast<const CUtensorMap*>(p.map_a), fb, kb * BK, m0);
-        tma_load_2d(smem_u32(sa + A_BYTES), static_cast<const CUtensorMap*>(p.map_b), fb,
-                    kb * BK, n0);
+        tma_load_2d(smem_u32(sa), ma, fb, kb * BK, m0);
+        tma_load_2d(smem_u32(sa + A_BYTES), mb, fb, kb * BK, n0);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -229,7 +236,7 @@ __global__ void __launch_bounds__(NT, 1)
     uint32_t g = 0, q = 0;  // k blocks consumed, chunks produced
     bool alive = true;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
-      const LtbTcProblem& p = probs[find_problem(probs, nprob, t)];
+      const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const int nk = (int)((p.Kp + BK - 1) / BK);
       for (int c0 = 0; c0 < nk && alive; c0 += kChunkBlocks, ++q) {
         const int buf = q & 1;
@@ -264,7 +271,7 @@ __global__ void __launch_bounds__(NT, 1)
     uint32_t q = 0;
     bool alive = true;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
-      const LtbTcProblem& p = probs[find_problem(probs, nprob, t)];
+      const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       int m0, n0;
       tile_coords(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
@@ -366,6 +373,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int e = 0; e < 4; ++e) split_bf16(x[e], hi[e], lo[e]);
     __nv_bfloat16* dst = out + r * Kp + k;
+    if (k == 0)  // K padding of this row: scratch is reused, keep it zero
+      for (int64_t c = nseg * K; c < Kp; ++c) out[r * Kp + c] = __float2bfloat16_rn(0.f);
     for (int s = 0; s < nseg; ++s) {
       const __nv_bfloat16* v = (seg_mask >> s) & 1 ? hi : lo;
       __nv_bfloat16* d = dst + s * K;
@@ -408,6 +417,8 @@ __global__ void __launch_bounds__(256)
     __nv_bfloat16 hi, lo;
     split_bf16(tile[a][tx], hi, lo);
     __nv_bfloat16* dst = out + r * Kp + k;
+    if (k == 0)  // K padding of this row: scratch is reused, keep it zero
+      for (int64_t c = nseg * K; c < Kp; ++c) out[r * Kp + c] = __float2bfloat16_rn(0.f);
     for (int s = 0; s < nseg; ++s) dst[s * K] = (seg_mask >> s) & 1 ? hi : lo;
   }
 }
@@ -444,8 +455,10 @@ __global__ void __launch_bounds__(256)
       if (r < J.rows && k < J.K) {
         __nv_bfloat16 hi, lo;
         split_bf16(tile[a][tx], hi, lo);
-        __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(J.out) + r * J.Kp + k;
-        for (int s = 0; s < J.nseg; ++s) dst[s * J.K] = (J.seg_mask >> s) & 1 ? hi : lo;
+        __nv_bfloat16* row = static_cast<__nv_bfloat16*>(J.out) + r * J.Kp;
+        if (k == 0)
+          for (int64_t c = J.nseg * J.K; c < J.Kp; ++c) row[c] = __float2bfloat16_rn(0.f);
+        for (int s = 0; s < J.nseg; ++s) row[k + s * J.K] = (J.seg_mask >> s) & 1 ? hi : lo;
       }
     }
     __syncthreads();
@@ -510,7 +523,8 @@ cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t
 size_t ltb_tc_smem_bytes() { return (size_t)STAGES * STAGE_BYTES + 1024 + 256; }
 
 cudaError_t ltb_launch_gemm_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
-                               float* c_override, int sms, int* err, cudaStream_t st) {
+                               float* c_override, int sms, int* err, cudaStream_t st,
+                               const LtbTcProblem* single, const void* map_a, const void* map_b) {
   static bool attr = false;
   const size_t smem = ltb_tc_smem_bytes();
   if (!attr) {
@@ -520,6 +534,14 @@ cudaError_t ltb_launch_gemm_tc(const LtbTcProblem* d_probs, int nprob, int64_t t
     attr = true;
   }
   const int grid = (int)(total_tiles < sms ? total_tiles : sms);
-  k_gemm_tc<<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err);
+  LtbTcProblem one{};
+  CUtensorMap ma{}, mb{};
+  if (!d_probs) {
+    if (!single || !map_a || !map_b) return cudaErrorInvalidValue;
+    one = *single;
+    ma = *static_cast<const CUtensorMap*>(map_a);
+    mb = *static_cast<const CUtensorMap*>(map_b);
+  }
+  k_gemm_tc<<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err, one, ma, mb);
   return cudaGetLastError();
 }

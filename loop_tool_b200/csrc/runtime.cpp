@@ -79,9 +79,8 @@ struct GemmTables {
   bool tc = false;
   int nseg = 1, a_mask = 1, b_mask = 1;
   int64_t Kp = 0, tiles = 0;
-  void *a_pack = nullptr, *b_pack = nullptr;
-  void* d_maps = nullptr;             // two CUtensorMaps in device memory
-  LtbTcProblem* d_prob = nullptr;     // one problem entry per batch index
+  int a_slot = -1, b_slot = -1;       // scratch slots of the packed operands
+  LtbTcProblem prob{};                // launch template (maps/c bound per run)
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
 };
 
@@ -222,40 +221,27 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
       default: t.nseg = 1; t.a_mask = 0x1; t.b_mask = 0x1; break;
     }
     t.Kp = (t.nseg * con.K + 7) / 8 * 8;
-    const size_t abytes = (size_t)con.M * t.Kp * 2, bbytes = (size_t)con.N * t.Kp * 2;
-    CUDA_TRY(cudaMalloc(&t.a_pack, abytes));
-    c->owned.push_back(t.a_pack);
-    CUDA_TRY(cudaMalloc(&t.b_pack, bbytes));
-    c->owned.push_back(t.b_pack);
-    // K padding columns stay zero for the life of the buffers
-    CUDA_TRY(cudaMemset(t.a_pack, 0, abytes));
-    CUDA_TRY(cudaMemset(t.b_pack, 0, bbytes));
-    alignas(64) unsigned char maps[256];
-    CUDA_TRY(ltb_make_tmap(maps, t.a_pack, con.M, t.Kp, ltb_tc_tile_m()));
-    CUDA_TRY(ltb_make_tmap(maps + 128, t.b_pack, con.N, t.Kp, ltb_tc_tile_n()));
-    CUDA_TRY(cudaMalloc(&t.d_maps, 256));
-    c->owned.push_back(t.d_maps);
-    CUDA_TRY(cudaMemcpy(t.d_maps, maps, 256, cudaMemcpyHostToDevice));
+    // packed BF16 operands live in the run's scratch (2 BF16 per float slot)
+    auto& P = c->plan;
+    t.a_slot = P.num_slots();
+    P.scratch_elems.push_back((con.M * t.Kp + 1) / 2);
+    t.b_slot = P.num_slots();
+    P.scratch_elems.push_back((con.N * t.Kp + 1) / 2);
     const int tm = (int)((con.M + ltb_tc_tile_m() - 1) / ltb_tc_tile_m());
     const int64_t tn = (con.N + ltb_tc_tile_n() - 1) / ltb_tc_tile_n();
     t.tiles = tm * tn;
-    // per-batch problem entries; the output pointer is patched in per run
-    std::vector<LtbTcProblem> pe(t.nbatch);
-    for (auto& e : pe) {
-      e.map_a = t.d_maps;
-      e.map_b = static_cast<char*>(t.d_maps) + 128;
-      e.c = nullptr;
-      e.crow = t.c_row;
-      e.ccol = t.c_col;
-      e.Kp = t.Kp;
-      e.tile_start = 0;
-      e.M = (int)con.M;
-      e.N = (int)con.N;
-      e.tiles_m = tm;
-      e.tiles_n = (int)tn;
-      e.unit_cols = t.unit_cols ? 1 : 0;
-    }
-    t.d_prob = upload(pe, c->owned);
+    LtbTcProblem& e = t.prob;
+    e.map_a = e.map_b = nullptr;
+    e.c = nullptr;
+    e.crow = t.c_row;
+    e.ccol = t.c_col;
+    e.Kp = t.Kp;
+    e.tile_start = 0;
+    e.M = (int)con.M;
+    e.N = (int)con.N;
+    e.tiles_m = tm;
+    e.tiles_n = (int)tn;
+    e.unit_cols = t.unit_cols ? 1 : 0;
   }
 }
 
@@ -294,6 +280,14 @@ void compile_device(ltb_compiled* c) {
       st.dev.split = 1;
     }
   }
+  for (int i = 0; i < ns; ++i) {
+    if (P.stages[i].family != ltb::Family::contraction) continue;
+    GemmTables t;
+    t.stage = i;
+    build_gemm(c, i, t);
+    c->gemm_of[i] = (int)c->gemms.size();
+    c->gemms.push_back(t);
+  }
   // scratch: one block, every slot 256-byte aligned
   c->scratch_off.clear();
   size_t off = 0;
@@ -312,14 +306,6 @@ void compile_device(ltb_compiled* c) {
   CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&c->d_err), sizeof(int)));
   c->owned.push_back(c->d_err);
   CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
-  for (int i = 0; i < ns; ++i) {
-    if (P.stages[i].family != ltb::Family::contraction) continue;
-    GemmTables t;
-    t.stage = i;
-    build_gemm(c, i, t);
-    c->gemm_of[i] = (int)c->gemms.size();
-    c->gemms.push_back(t);
-  }
   int launches = 0;
   for (int i = 0; i < ns; ++i) {
     auto& st = P.stages[i];
@@ -389,11 +375,20 @@ void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
             e = ltb_launch_gemm_simt(p, c->sms, st);
             continue;
           }
-          e = ltb_launch_pack(p.a, p.M, p.K, t.a_pack, t.Kp, t.nseg, t.a_mask, t.a_kcontig, st);
+          void* ap = bt.p[t.a_slot];
+          void* bp = bt.p[t.b_slot];
+          e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, st);
           if (e == cudaSuccess)
-            e = ltb_launch_pack(p.b, p.N, p.K, t.b_pack, t.Kp, t.nseg, t.b_mask, t.b_kcontig, st);
-          if (e == cudaSuccess)
-            e = ltb_launch_gemm_tc(t.d_prob + b, 1, t.tiles, p.c, c->sms, c->d_err, st);
+            e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, st);
+          alignas(64) unsigned char maps[256];
+          if (e == cudaSuccess) e = ltb_make_tmap(maps, ap, p.M, t.Kp, ltb_tc_tile_m());
+          if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, ltb_tc_tile_n());
+          if (e == cudaSuccess) {
+            LtbTcProblem one = t.prob;
+            one.c = p.c;
+            e = ltb_launch_gemm_tc(nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st, &one,
+                                   maps, maps + 128);
+          }
         }
         break;
       }
@@ -540,6 +535,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->sms = cs[0]->sms;
     std::vector<LtbPackJob> jobs;
     std::vector<LtbTcProblem> tcp;
+    std::vector<unsigned char> maps;  // two 128-byte CUtensorMaps per problem
     std::vector<LtbGemmProblem> sp;
     std::vector<int64_t> sstart;
     for (int i = 0; i < n; ++i) {
@@ -589,10 +585,18 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
           b->pack_tiles += ((rows + 31) / 32) * j.tiles_k;
           jobs.push_back(j);
         };
-        job(p.a, p.M, t.a_pack, t.a_mask, t.a_kcontig);
-        job(p.b, p.N, t.b_pack, t.b_mask, t.b_kcontig);
-        LtbTcProblem q{};
-        CUDA_TRY(cudaMemcpy(&q, t.d_prob, sizeof(q), cudaMemcpyDeviceToHost));
+        void *ap = nullptr, *bp = nullptr;
+        CUDA_TRY(cudaMalloc(&ap, (size_t)p.M * t.Kp * 2));
+        b->owned.push_back(ap);
+        CUDA_TRY(cudaMalloc(&bp, (size_t)p.N * t.Kp * 2));
+        b->owned.push_back(bp);
+        job(p.a, p.M, ap, t.a_mask, t.a_kcontig);
+        job(p.b, p.N, bp, t.b_mask, t.b_kcontig);
+        maps.resize(maps.size() + 256);
+        unsigned char* m = maps.data() + maps.size() - 256;
+        CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
+        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, ltb_tc_tile_n()));
+        LtbTcProblem q = t.prob;
         q.c = p.c;
         q.tile_start = b->tc_tiles;
         b->tc_tiles += t.tiles;
@@ -606,6 +610,12 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->njobs = (int)jobs.size();
     if (b->tc) {
       b->d_jobs = upload(jobs, b->owned);
+      // tensor maps in device memory (cudaMalloc is 256-byte aligned)
+      unsigned char* d_maps = upload(maps, b->owned);
+      for (size_t i = 0; i < tcp.size(); ++i) {
+        tcp[i].map_a = d_maps + 256 * i;
+        tcp[i].map_b = d_maps + 256 * i + 128;
+      }
       b->d_tc = upload(tcp, b->owned);
     } else {
       b->d_simt = upload(sp, b->owned);

@@ -44,8 +44,12 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
 // Persistent grouped launch over every tile of every problem
 // (tiles_m * ceil(N / tile_n) tiles per problem).  c_override, if not null,
 // replaces every problem's output pointer (single-problem launches).
+// d_probs == nullptr: a single problem passed by value with its two tensor
+// maps (host copies, passed as kernel parameters).
 cudaError_t ltb_launch_gemm_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
-                               float* c_override, int sms, int* err, cudaStream_t st);
+                               float* c_override, int sms, int* err, cudaStream_t st,
+                               const LtbTcProblem* single = nullptr,
+                               const void* map_a = nullptr, const void* map_b = nullptr);
 int ltb_tc_tile_m();
 int ltb_tc_tile_n();
 size_t ltb_tc_smem_bytes();
