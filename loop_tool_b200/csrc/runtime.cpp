@@ -84,6 +84,31 @@ struct GemmTables {
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
 };
 
+// All of a compiled object's constant device data (stage descriptors,
+// contraction offset tables, the timeout flag) in one allocation and one
+// copy: pointers are recorded as (slot, offset) and patched at finalize.
+struct Arena {
+  std::vector<unsigned char> host;
+  std::vector<std::pair<void**, size_t>> fix;
+  template <typename T>
+  void add(const std::vector<T>& v, T** slot) {
+    *slot = nullptr;
+    if (v.empty()) return;
+    const size_t off = (host.size() + 255) / 256 * 256;
+    host.resize(off + v.size() * sizeof(T));
+    memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+    fix.push_back({reinterpret_cast<void**>(slot), off});
+  }
+  void finalize(std::vector<void*>& owned) {
+    if (host.empty()) return;
+    void* base = nullptr;
+    CUDA_TRY(cudaMalloc(&base, host.size()));
+    owned.push_back(base);
+    CUDA_TRY(cudaMemcpy(base, host.data(), host.size(), cudaMemcpyHostToDevice));
+    for (auto& f : fix) *f.first = static_cast<unsigned char*>(base) + f.second;
+  }
+};
+
 template <typename T>
 T* upload(const std::vector<T>& v, std::vector<void*>& owned) {
   if (v.empty()) return nullptr;
@@ -128,7 +153,7 @@ int64_t stage_outs(const LtbStage& d) {
 }
 
 // Split a contraction's affine operand loads into per-row / per-k tables.
-void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
+void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
   const ltb::PlanStage& ps = c->plan.stages[si];
   const LtbStage& d = ps.dev;
   const ltb::Contraction& con = ps.con;
@@ -168,12 +193,12 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
   t.b_boff = table(bd, B.coef, 0);
   t.c_boff = table(bd, d.out_coef, 0);
   t.nbatch = (int64_t)t.a_boff.size();
-  t.a_row = upload(table(md, A.coef, A.off), c->owned);
-  t.a_k = upload(table(kd, A.coef, 0), c->owned);
-  t.b_row = upload(table(nd, B.coef, B.off), c->owned);
-  t.b_k = upload(table(kd, B.coef, 0), c->owned);
-  t.c_row = upload(table(md, d.out_coef, d.out_off), c->owned);
-  t.c_col = upload(table(nd, d.out_coef, 0), c->owned);
+  ar.add(table(md, A.coef, A.off), &t.a_row);
+  ar.add(table(kd, A.coef, 0), &t.a_k);
+  ar.add(table(nd, B.coef, B.off), &t.b_row);
+  ar.add(table(kd, B.coef, 0), &t.b_k);
+  ar.add(table(md, d.out_coef, d.out_off), &t.c_row);
+  ar.add(table(nd, d.out_coef, 0), &t.c_col);
   auto guards = [&](const LtbLoad& L, const std::vector<int>& rd,
                     int32_t** grow, int32_t** gk, int32_t** gub, int* ng) {
     std::vector<int32_t> vr, vk, vu;
@@ -184,9 +209,9 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
       vu.push_back((int32_t)G.ub);
     }
     *ng = L.ng;
-    *grow = upload(vr, c->owned);
-    *gk = upload(vk, c->owned);
-    *gub = upload(vu, c->owned);
+    ar.add(vr, grow);
+    ar.add(vk, gk);
+    ar.add(vu, gub);
   };
   guards(A, md, &t.ag_row, &t.ag_k, &t.ag_ub, &t.a_ng);
   guards(B, nd, &t.bg_row, &t.bg_k, &t.bg_ub, &t.b_ng);
@@ -233,8 +258,9 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t) {
     LtbTcProblem& e = t.prob;
     e.map_a = e.map_b = nullptr;
     e.c = nullptr;
-    e.crow = t.c_row;
-    e.ccol = t.c_col;
+    // crow / ccol point into the arena, which is only placed at finalize:
+    // bound at launch time
+    e.crow = e.ccol = nullptr;
     e.Kp = t.Kp;
     e.tile_start = 0;
     e.M = (int)con.M;
@@ -280,13 +306,15 @@ void compile_device(ltb_compiled* c) {
       st.dev.split = 1;
     }
   }
+  Arena ar;
+  c->gemms.reserve(ns);  // table pointers are patched in place: no realloc
   for (int i = 0; i < ns; ++i) {
     if (P.stages[i].family != ltb::Family::contraction) continue;
-    GemmTables t;
-    t.stage = i;
-    build_gemm(c, i, t);
     c->gemm_of[i] = (int)c->gemms.size();
-    c->gemms.push_back(t);
+    c->gemms.emplace_back();
+    GemmTables& t = c->gemms.back();
+    t.stage = i;
+    build_gemm(c, i, t, ar);
   }
   // scratch: one block, every slot 256-byte aligned
   c->scratch_off.clear();
@@ -295,17 +323,12 @@ void compile_device(ltb_compiled* c) {
     c->scratch_off.push_back(off);
     off += ((size_t)std::max<int64_t>(e, 1) * 4 + 255) / 256 * 256;
   }
-  c->scratch_bytes = off;
-  if (off) {
-    CUDA_TRY(cudaMalloc(&c->scratch, off));
-    c->owned.push_back(c->scratch);
-  }
+  c->scratch_bytes = off;  // allocated on the first run without caller scratch
   std::vector<LtbStage> hs;
   for (auto& st : P.stages) hs.push_back(st.dev);
-  if (!hs.empty()) c->d_stages = upload(hs, c->owned);
-  CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&c->d_err), sizeof(int)));
-  c->owned.push_back(c->d_err);
-  CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
+  ar.add(hs, &c->d_stages);
+  ar.add(std::vector<int>{0}, &c->d_err);
+  ar.finalize(c->owned);
   int launches = 0;
   for (int i = 0; i < ns; ++i) {
     auto& st = P.stages[i];
@@ -386,6 +409,8 @@ void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
           if (e == cudaSuccess) {
             LtbTcProblem one = t.prob;
             one.c = p.c;
+            one.crow = t.c_row;
+            one.ccol = t.c_col;
             e = ltb_launch_gemm_tc(nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st, &one,
                                    maps, maps + 128);
           }
@@ -410,6 +435,13 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
   std::unique_lock<std::mutex> lock(c->mu, std::defer_lock);
   if (!scratch) {
     lock.lock();
+    if (!c->scratch && c->scratch_bytes) {
+      if (cudaMalloc(&c->scratch, c->scratch_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LTB_ERR_CUDA, "scratch allocation failed");
+      }
+      c->owned.push_back(c->scratch);
+    }
     scratch = c->scratch;
   }
   LtbBufTable bt{};
@@ -598,6 +630,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, ltb_tc_tile_n()));
         LtbTcProblem q = t.prob;
         q.c = p.c;
+        q.crow = t.c_row;
+        q.ccol = t.c_col;
         q.tile_start = b->tc_tiles;
         b->tc_tiles += t.tiles;
         tcp.push_back(q);
@@ -768,7 +802,7 @@ int ltb_run_with_scratch(ltb_compiled* c, void* const* memory, int n, int sync,
                          void* stream, void* scratch) {
   if (c && c->scratch_bytes && !scratch)
     return fail(LTB_ERR_INVALID, "scratch pointer required");
-  return run_impl(c, memory, n, sync, stream, scratch ? scratch : c->scratch);
+  return run_impl(c, memory, n, sync, stream, scratch);
 }
 
 int ltb_release(ltb_compiled* c) {

@@ -1,0 +1,224 @@
+"""Continuous-batching request loop over the B200 backend.
+
+Requests are lazy-tensor programs (this package's lazy frontend) of varying
+symbolic sizes.  The loop:
+  * admits a request as soon as a slot (a CUDA stream) is free and its bytes
+    (inputs + output + scratch, from the compiled plan) fit the HBM budget;
+    requests that arrive while others run are admitted in arrival order as
+    slots and memory free up, so their kernels overlap on the device;
+  * reuses compiled loop trees through the IR-text kernel cache
+    (loop_tool_b200.lazy.compiled), one entry per distinct program + sizes
+    (the reference's lazy cache is keyed the same way, lazy.h:82-115);
+  * keeps every buffer device-resident: inputs are produced on the device,
+    buffers come from torch's stream-ordered caching allocator, and each run
+    gets its own scratch (ltb_run_with_scratch), so concurrent runs of one
+    compiled object never share scratch;
+  * reports throughput and p50 / p99 latency (arrival -> completion).
+
+The reference has no serving loop; its lazy frontend runs one program at a
+time, synchronously (lazy.h:255-258).
+"""
+import math
+import time
+from collections import deque
+
+import numpy as np
+
+from . import lazy as lt
+from . import nn
+
+KINDS = ("matmul", "conv", "softmax")
+
+
+def make_trace(n, rate, seed=501, mix=(0.5, 0.3, 0.2), mm_range=(64, 4096),
+               conv_batch=(1, 64), softmax_rows=(1, 8192)):
+    """Seeded request trace with Poisson arrivals at `rate` requests/s:
+    matmuls with M, N, K log-uniform in mm_range rounded to multiples of 16,
+    3x3 pad-1 convolutions [b,64,56,56] * [128,64,3,3] with b uniform in
+    conv_batch, row softmaxes [rows, 4096] with rows uniform in softmax_rows."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    kinds = rng.choice(3, size=n, p=list(mix))
+    out = []
+    lo, hi = math.log(mm_range[0]), math.log(mm_range[1])
+    for i in range(n):
+        k = KINDS[kinds[i]]
+        if k == "matmul":
+            m, nn_, kk = (int(max(16, 16 * round(math.exp(rng.uniform(lo, hi)) / 16)))
+                          for _ in range(3))
+            params = (m, kk, nn_)
+        elif k == "conv":
+            params = (int(rng.integers(conv_batch[0], conv_batch[1] + 1)),)
+        else:
+            params = (int(rng.integers(softmax_rows[0], softmax_rows[1] + 1)),)
+        out.append(Request(i, k, params, float(t[i]), seed * 1000003 + i))
+    return out
+
+
+class Request:
+    __slots__ = ("rid", "kind", "params", "arrival", "seed", "admitted", "done", "out",
+                 "bytes", "event", "hold")
+
+    def __init__(self, rid, kind, params, arrival, seed):
+        self.rid, self.kind, self.params, self.arrival, self.seed = rid, kind, params, arrival, seed
+        self.admitted = self.done = None
+        self.out = None
+        self.bytes = 0
+        self.event = None
+        self.hold = None
+
+
+def _program(kind, params):
+    """The request's loop tree, built with the lazy frontend."""
+    if kind == "matmul":
+        M, K, N = params
+        A, B = lt.Tensor(M, K), lt.Tensor(K, N)
+        m, k, n = lt.Symbol("m"), lt.Symbol("k"), lt.Symbol("n")
+        return (A.to(m, k) * B.to(k, n)).sum(k)
+    if kind == "conv":
+        (b,) = params
+        X, W = lt.Tensor(b, 64, 56, 56), lt.Tensor(128, 64, 3, 3)
+        n_, c, h, w, co, kh, kw = (lt.Symbol(x) for x in ("n", "c", "h", "w", "co", "kh", "kw"))
+        x = X.to(n_, c, h, w).pad(h, 1)
+        x = x.pad(x.shape[3], 1)
+        return nn.conv(x, W.to(co, c, kh, kw), [x.shape[2], x.shape[3]], [kh, kw])
+    (rows,) = params
+    X = lt.Tensor(rows, 4096)
+    r, n = lt.Symbol("r"), lt.Symbol("n")
+    x = X.to(r, n)
+    e = (x - x.max_reduce(n)).exp()
+    return e / e.sum(n)
+
+
+class Server:
+    """slots: concurrent requests (one CUDA stream each); hbm_budget: bytes of
+    request buffers admitted at once; precision: contraction mode."""
+
+    def __init__(self, slots=8, hbm_budget=16 << 30, precision="bf16x3", device=0,
+                 keep_outputs=False):
+        import torch
+
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.streams = [torch.cuda.Stream(self.dev) for _ in range(slots)]
+        self.free = list(range(slots))
+        self.budget = hbm_budget
+        self.used = 0
+        self.precision = precision
+        self.keep = keep_outputs
+        self._ir = {}
+        self.compiles = 0
+
+    def _compiled(self, req):
+        key = (req.kind, req.params)
+        text = self._ir.get(key)
+        if text is None:
+            text = _program(req.kind, req.params).ir
+            self._ir[key] = text
+        before = lt.cache_info()["entries"]
+        c = lt.compiled(text, precision=self.precision)
+        self.compiles += lt.cache_info()["entries"] > before
+        return c
+
+    def _inputs(self, req, c, gen):
+        torch = self.torch
+        ins = []
+        for i, n in enumerate(c.io_sizes[:c.n_inputs]):
+            x = torch.randn(n, device=self.dev, generator=gen)
+            if req.kind == "matmul":
+                x /= math.sqrt(req.params[1])  # N(0,1)/sqrt(K)
+            elif req.kind == "conv" and i == 1:
+                x *= math.sqrt(6.0 / 576) / math.sqrt(3.0)  # Kaiming-uniform scale
+            elif req.kind == "softmax":
+                x *= 4.0
+            ins.append(x)
+        return ins
+
+    def _launch(self, req, slot, now):
+        torch = self.torch
+        c = self._compiled(req)
+        st = self.streams[slot]
+        with torch.cuda.stream(st):
+            gen = torch.Generator(device=self.dev)
+            gen.manual_seed(req.seed)
+            ins = self._inputs(req, c, gen)
+            out = torch.empty(c.io_sizes[-1], device=self.dev)
+            sb = c.int_property("scratch_bytes")
+            scratch = torch.empty(max(sb // 4, 1), device=self.dev) if sb else None
+            c.run(ins + [out], sync=False, stream=st.cuda_stream,
+                  scratch=scratch.data_ptr() if scratch is not None else None)
+            ev = torch.cuda.Event()
+            ev.record(st)
+        req.event, req.hold, req.admitted = ev, (ins, out, scratch), now
+
+    def bytes_of(self, req):
+        c = self._compiled(req)
+        return 4 * sum(c.io_sizes) + c.int_property("scratch_bytes")
+
+    def serve(self, trace, time_scale=1.0, poll_sleep=0.0):
+        """Run a trace against the wall clock.  Returns per-request latencies
+        (seconds) and summary statistics."""
+        torch = self.torch
+        pending = deque()
+        inflight = {}
+        arrivals = deque(sorted(trace, key=lambda r: r.arrival))
+        done = []
+        self.peak_used = self.peak_inflight = 0
+        t0 = time.perf_counter()
+        while arrivals or pending or inflight:
+            now = time.perf_counter() - t0
+            while arrivals and arrivals[0].arrival * time_scale <= now:
+                r = arrivals.popleft()
+                r.bytes = self.bytes_of(r)
+                if r.bytes > self.budget:
+                    raise ValueError(f"request {r.rid} needs {r.bytes} B > budget {self.budget} B")
+                pending.append(r)
+            for slot, r in list(inflight.items()):
+                if r.event.query():
+                    r.done = time.perf_counter() - t0
+                    if self.keep:
+                        r.out = r.hold[1].cpu().numpy()
+                    r.hold = None
+                    self.used -= r.bytes
+                    self.free.append(slot)
+                    del inflight[slot]
+                    done.append(r)
+            while pending and self.free and self.used + pending[0].bytes <= self.budget:
+                r = pending.popleft()
+                slot = self.free.pop()
+                self.used += r.bytes
+                self._launch(r, slot, time.perf_counter() - t0)
+                inflight[slot] = r
+                self.peak_used = max(self.peak_used, self.used)
+                self.peak_inflight = max(self.peak_inflight, len(inflight))
+            if not pending and not inflight and arrivals:
+                wait = arrivals[0].arrival * time_scale - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.01))
+            elif poll_sleep:
+                time.sleep(poll_sleep)
+        torch.cuda.synchronize()
+        lat = np.array([r.done - r.arrival * time_scale for r in done])
+        span = max(r.done for r in done) - min(r.arrival * time_scale for r in done)
+        return {
+            "requests": len(done),
+            "req_per_s": len(done) / span if span > 0 else float("nan"),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3),
+            "span_s": span,
+            "compiles": self.compiles,
+            "peak_inflight": self.peak_inflight,
+            "peak_bytes": self.peak_used,
+            "slots": len(self.streams),
+            "precision": self.precision,
+        }, done
+
+
+def run_alone(req, precision="bf16x3", device=0):
+    """One request by itself on a fresh stream: the reference point for
+    "same result alone and in the mix"."""
+    s = Server(slots=1, precision=precision, device=device, keep_outputs=True)
+    r = Request(req.rid, req.kind, req.params, 0.0, req.seed)
+    s.serve([r])
+    return r.out
