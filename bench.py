@@ -1,23 +1,36 @@
 #!/usr/bin/env python
 """Benchmark of the B200 "cuda" backend for loop_tool.
 
-Workload (one step): the bandwidth-bound FP32 nests of the reference's
-headline configuration, each a loop tree built by the lazy frontend and run
-through the backend's Compiled::run entry point (the C ABI):
+Headline (one JSON line, `value`): the bandwidth-bound FP32 nests of the
+reference's headline configuration, each a loop tree built with the lazy
+frontend and run through the backend's Compiled::run entry point (C ABI):
   (i)   C = A + B over 2^28 elements
   (ii)  row softmax of x[8192, 4096] (max, subtract, exp, sum, divide)
   (iii) 2x2 stride-2 max-pool of X[64, 128, 112, 112]
-Metric: HBM GB/s of algorithmic traffic (every input element read once,
-every output element written once) for the whole step.
+one step = the three nests; value = HBM GB/s of algorithmic traffic (every
+input element read once, every output element written once) over the step.
+
+The same line carries the other configurations under "configs":
+  c1  (A.to(m,k) * B.to(k,n)).sum(k), 128^3, FP32, checked against the
+      reference CPU backend on the same IR
+  c3  conv [32,64,56,56] * [128,64,3,3], stride 1, pad 1: FP32 CUDA cores,
+      BF16 and split-BF16 tensor cores, error vs FP64 on sampled outputs
+  c4  512 uneven matmuls (M, N, K log-uniform in [64, 4096], multiples of 16)
+      in one graph-captured grouped launch (BF16, split-BF16, FP32), and a
+      single 8192^3 matmul (tensor-pipe share of the measured BF16 peak)
+  c5  serving: a seeded Poisson trace (50% matmul, 30% conv, 20% softmax) on
+      the continuous-batching server vs the plain FP32 one-stream path
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+      [--serve-requests R] [--no-extras]
 
 --impl reference times the reference's own CPU backend ("cpp": generated C
-compiled by cc -O3, single-threaded like the reference) on the host cores, on
-a bounded sample of the same workload.
+compiled by cc -O3, single-threaded as the reference is) on the host cores,
+on a bounded sample of the same workload.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -29,43 +42,32 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-
-NESTS = [
-    # name, IR fixture, input element counts, output element count
-    ("add_2p28", "add_2p28.txt"),
-    ("softmax_8192x4096", "softmax_8192x4096.txt"),
-    ("maxpool_64x128x112x112", "maxpool_64x128x112x112.txt"),
-]
-IR_DIR = os.path.join(ROOT, "tests", "golden", "ir")
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "lt_ref_harness")
+BF16_DENSE_NOMINAL = 2250.0
 
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get("hbm_gbs", 6650.0), "measured"
-    return 6650.0, "fallback"
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
 
 
 def read_traffic():
     p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        return json.load(open(p))
-    return {}
+    return json.load(open(p)) if os.path.exists(p) else {}
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.path = None
+        self.index, self.proc, self.path = index, None, None
 
     def start(self):
         try:
@@ -86,15 +88,13 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                rows.append(f)
+        rows = [[x.strip() for x in line.split(",")] for line in open(self.path)]
+        rows = [r for r in rows if len(r) >= 9]
         os.unlink(self.path)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        num = lambda x: x.replace(".", "", 1).isdigit()
+        sm = [float(r[1]) for r in rows if num(r[1])]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
@@ -102,30 +102,59 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "sm_max_mhz": float(rows[0][2]) if num(rows[0][2]) else None,
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def reference_time(nests, budget_s=20.0):
-    """Times the reference CPU backend on a bounded sample of each nest:
-    the same loop tree at reduced size, scaled by bytes."""
-    samples = {
-        "add_2p28": ("add", [1 << 24]),
-        "softmax_8192x4096": ("softmax", [512, 4096]),
-        "maxpool_64x128x112x112": ("maxpool", [4, 128, 112, 112, 2, 2]),
-    }
-    total_bytes = 0.0
-    total_s = 0.0
-    desc = []
-    for name in nests:
-        prog, params = samples[name]
+# ------------------------------------------------------------- workloads
+def nests():
+    """The three bandwidth nests, built with the lazy frontend."""
+    import loop_tool_b200.lazy as lt
+    import loop_tool_b200.nn as nn
+
+    A, B = lt.Tensor(1 << 28), lt.Tensor(1 << 28)
+    N = lt.Symbol("N")
+    add = A.to(N) + B.to(N)
+    X = lt.Tensor(8192, 4096)
+    r, n = lt.Symbol("r"), lt.Symbol("n")
+    x = X.to(r, n)
+    e = (x - x.max_reduce(n)).exp()
+    softmax = e / e.sum(n)
+    P = lt.Tensor(64, 128, 112, 112)
+    b, c, h, w = (lt.Symbol(s) for s in "nchw")
+    pool = nn.maxpool(P.to(b, c, h, w), [h, w], 2, 2)
+    return [("add_2p28", add.ir, 1.0), ("softmax_8192x4096", softmax.ir, 4.0),
+            ("maxpool_64x128x112x112", pool.ir, 1.0)]
+
+
+def mm_ir(M, K, N):
+    import loop_tool_b200.lazy as lt
+
+    A, B = lt.Tensor(M, K), lt.Tensor(K, N)
+    m, k, n = lt.Symbol("m"), lt.Symbol("k"), lt.Symbol("n")
+    return (A.to(m, k) * B.to(k, n)).sum(k).ir
+
+
+def conv_ir(b=32):
+    from loop_tool_b200.serve import _program
+
+    return _program("conv", (b,)).ir
+
+
+# --------------------------------------------------------- CPU reference
+def reference_time(samples=None):
+    """Times the reference CPU backend ("cpp", one pinned core) on a bounded
+    sample of each nest: the same loop trees at reduced size, scaled by
+    bytes."""
+    samples = samples or [("add", [1 << 24]), ("softmax", [512, 4096]),
+                          ("maxpool", [4, 128, 112, 112, 2, 2])]
+    total_bytes = total_s = 0.0
+    for prog, params in samples:
         with tempfile.TemporaryDirectory() as td:
             ir = subprocess.run([HARNESS, "ir", prog, *map(str, params)], capture_output=True,
                                 text=True, check=True).stdout
@@ -136,18 +165,15 @@ def reference_time(nests, budget_s=20.0):
             rng = np.random.default_rng(1)
             for i, n in enumerate(sizes["inputs"]):
                 rng.standard_normal(n, dtype=np.float32).tofile(os.path.join(td, f"in{i}.f32"))
-            r = subprocess.run(["taskset", "-c", "0", HARNESS, "run", irf, "cpp", td, td, "3"],
-                               capture_output=True, text=True)
+            cmd = [HARNESS, "run", irf, "cpp", td, td, "3"]
+            r = subprocess.run(["taskset", "-c", "0"] + cmd, capture_output=True, text=True)
             if r.returncode != 0:
-                r = subprocess.run([HARNESS, "run", irf, "cpp", td, td, "3"],
-                                   capture_output=True, text=True, check=True)
-            secs = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
-            t = min(secs)
-            b = 4 * (sum(sizes["inputs"]) + sum(sizes["outputs"]))
-            total_bytes += b
+                r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+            t = min(json.loads(r.stdout.strip().splitlines()[-1])["seconds"])
+            total_bytes += 4 * (sum(sizes["inputs"]) + sum(sizes["outputs"]))
             total_s += t
-            desc.append(f"{prog}{params}")
-    return total_bytes / total_s / 1e9, "; ".join(desc)
+    desc = "; ".join(f"{p}{q}" for p, q in samples)
+    return total_bytes / total_s / 1e9, desc
 
 
 def run_reference(args):
@@ -156,73 +182,50 @@ def run_reference(args):
         return
     if not os.path.exists(HARNESS):
         print(json.dumps({"impl": "reference",
-                          "unavailable": "oracle/_ref not built (make -C oracle)"}))
+                          "unavailable": "reference CPU build absent (make -C oracle)"}))
         return
+    for _ in range(args.warmup):
+        reference_time()
     vals = []
     desc = ""
-    for _ in range(args.warmup):
-        reference_time([n for n, _ in NESTS])
     for _ in range(args.steps):
-        v, desc = reference_time([n for n, _ in NESTS])
+        v, desc = reference_time()
         vals.append(v)
-    v = min(vals)
+    v = statistics.median(vals)
     print(json.dumps({
         "impl": "reference", "metric": "hbm_gbs_bandwidth_nests", "value": v, "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "bandwidth nests: add 2^28, softmax 8192x4096, maxpool 64x128x112x112",
-                   "parallelism": "cpu"},
+        "config": {"workload": "bandwidth nests: add 2^28, softmax 8192x4096, maxpool "
+                               "64x128x112x112 (FP32)", "parallelism": "cpu, 1 pinned core"},
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": 1, "kind": "reference",
                          "sample": desc},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    args = ap.parse_args()
-    if args.impl == "reference":
-        return run_reference(args)
-
+# ------------------------------------------------------------- headline
+def headline(args, world, rank, dev):
     import torch
 
-    import loop_tool_b200 as lt
-
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    torch.cuda.init()
+    import loop_tool_b200 as ltb
 
     comps, bufs, bytes_per = [], [], []
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
-    for name, fn in NESTS:
-        ir = open(os.path.join(IR_DIR, fn)).read()
-        c = lt.cuda(ir)
-        ins = [torch.randn(n, device=dev, generator=g) for n in c.io_sizes[:c.n_inputs]]
-        if name.startswith("softmax"):
-            ins = [4.0 * x for x in ins]
+    for name, ir, scale in nests():
+        c = ltb.Compiled(ir)
+        ins = [scale * torch.randn(n, device=dev, generator=g) for n in c.io_sizes[:c.n_inputs]]
         outs = [torch.empty(n, device=dev) for n in c.io_sizes[c.n_inputs:]]
-        comps.append(c)
+        comps.append((name, c))
         bufs.append(ins + outs)
         bytes_per.append(4 * sum(c.io_sizes))
     stream = torch.cuda.current_stream()
 
     def step(times=None):
-        for i, (c, b) in enumerate(zip(comps, bufs)):
+        for i, ((_, c), b) in enumerate(zip(comps, bufs)):
             if times is not None:
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
             c.run(b, sync=False)
             if times is not None:
@@ -234,12 +237,11 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
     time.sleep(0.3)
-    per = [[] for _ in NESTS]
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
+    per = [[] for _ in comps]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     t0.record(stream)
     for _ in range(args.steps):
@@ -256,21 +258,24 @@ def main():
     step_bytes = sum(bytes_per)
     value = world * step_bytes * args.steps / (ms / 1e3) / 1e9
 
-    # e2e: same step through the C ABI with pinned host buffers; host->device
-    # copies of the inputs and device->host copies of the outputs are inside
-    # the timed region (the backend stages host pointers through HBM).
+    # e2e: the same step through the C ABI with pinned host buffers; the
+    # host->device copies of the inputs and device->host copies of the
+    # outputs happen inside the timed region (the backend stages host
+    # pointers through HBM)
     hbufs = []
-    for c, b in zip(comps, bufs):
+    for (_, c), b in zip(comps, bufs):
         hb = [x.cpu().pin_memory() for x in b[:c.n_inputs]]
         hb += [torch.empty(n, pin_memory=True) for n in c.io_sizes[c.n_inputs:]]
         hbufs.append(hb)
-    e2e_steps = max(1, min(args.steps, 3))
-    for c, hb in zip(comps, hbufs):
+    for (_, c), hb in zip(comps, hbufs):
         c.run(hb, sync=True)
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e2e_steps = max(1, min(args.steps, 3))
     w0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for c, hb in zip(comps, hbufs):
+        for (_, c), hb in zip(comps, hbufs):
             c.run(hb, sync=True)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - w0) / e2e_steps
@@ -278,44 +283,262 @@ def main():
         tt = torch.tensor([e2e_s], device=dev)
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         e2e_s = tt.item()
-    h2d = sum(4 * sum(c.io_sizes[:c.n_inputs]) for c in comps)
-    d2h = sum(4 * sum(c.io_sizes[c.n_inputs:]) for c in comps)
-
-    peak, peak_kind = load_peaks()
+    h2d = sum(4 * sum(c.io_sizes[:c.n_inputs]) for _, c in comps)
+    d2h = sum(4 * sum(c.io_sizes[c.n_inputs:]) for _, c in comps)
+    hbm_peak, _, peak_kind = load_peaks()
     dom = int(np.argmax(nest_ms))
     achieved = bytes_per[dom] / (nest_ms[dom] / 1e3) / 1e9
-    traffic = read_traffic().get(NESTS[dom][0])
-    launches = sum(c.int_property("launches") for c in comps) * args.steps
+    return {
+        "metric": "hbm_gbs_bandwidth_nests", "value": value, "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "bandwidth nests: add 2^28, softmax 8192x4096, maxpool "
+                               "64x128x112x112 (FP32 lazy-frontend loop trees)",
+                   "l2": "inputs larger than L2 (126 MB), no flush needed",
+                   "parallelism": f"replicas{world}"},
+        "nests_ms": {n: t for (n, _), t in zip(comps, nest_ms)},
+        "nests_gbs": {n: b / (t / 1e3) / 1e9 for (n, _), b, t in zip(comps, bytes_per, nest_ms)},
+        "nests_frac_of_hbm": {n: b / (t / 1e3) / 1e9 / hbm_peak
+                              for (n, _), b, t in zip(comps, bytes_per, nest_ms)},
+        "roofline": {"bound": "hbm", "kernel": comps[dom][0], "achieved": achieved,
+                     "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": read_traffic().get(comps[dom][0])},
+        "e2e": {"value": world * step_bytes / e2e_s / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": sum(c.int_property("launches") for _, c in comps) * args.steps,
+        "clocks": clocks,
+    }
 
+
+def timed(fn, reps, stream=None):
+    import torch
+
+    stream = stream or torch.cuda.current_stream()
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+# ----------------------------------------------------------------- c1
+def extra_c1(dev):
+    import torch
+
+    import loop_tool_b200 as ltb
+
+    ir = mm_ir(128, 128, 128)
+    rng = np.random.default_rng(101)
+    a = rng.standard_normal(128 * 128).astype(np.float32)
+    b = np.random.default_rng(102).standard_normal(128 * 128).astype(np.float32)
+    out = {"workload": "(A.to(m,k) * B.to(k,n)).sum(k), 128^3 FP32, lazy frontend"}
+    A, B = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    for prec in ("fp32", "bf16x3"):
+        c = ltb.Compiled(ir, precision=prec)
+        C = torch.empty(128 * 128, device=dev)
+        us = timed(lambda: c.run([A, B, C], sync=False), 200) * 1e3
+        ch = np.empty(128 * 128, np.float32)
+        w0 = time.perf_counter()
+        for _ in range(50):
+            c([a, b, ch])
+        e2e_us = (time.perf_counter() - w0) / 50 * 1e6
+        res = {"device_us_per_call": us, "gflops": 2 * 128 ** 3 / (us * 1e-6) / 1e9,
+               "e2e_us_per_call_host_buffers": e2e_us}
+        # checked against the reference CPU backend on the same IR
+        if os.path.exists(HARNESS):
+            with tempfile.TemporaryDirectory() as td:
+                open(os.path.join(td, "ir.txt"), "w").write(ir)
+                a.tofile(os.path.join(td, "in0.f32"))
+                b.tofile(os.path.join(td, "in1.f32"))
+                subprocess.run([HARNESS, "run", os.path.join(td, "ir.txt"), "cpp", td, td],
+                               check=True, capture_output=True)
+                ref = np.fromfile(os.path.join(td, "out0.f32"), np.float32)
+            res["max_abs_diff_vs_reference_cpp"] = float(np.abs(ch - ref).max())
+        exact = a.reshape(128, 128).astype(np.float64) @ b.reshape(128, 128).astype(np.float64)
+        res["normwise_err_vs_fp64"] = float(np.linalg.norm(ch.reshape(128, 128) - exact) /
+                                            np.linalg.norm(exact))
+        out[prec] = res
+    return out
+
+
+# ----------------------------------------------------------------- c3
+def extra_c3(dev):
+    import torch
+
+    import loop_tool_b200 as ltb
+
+    ir = conv_ir(32)
+    flops = 2.0 * 32 * 128 * 56 * 56 * 64 * 9
+    x = torch.from_numpy(np.random.default_rng(301).standard_normal(32 * 64 * 56 * 56)
+                         .astype(np.float32)).to(dev)
+    bound = math.sqrt(6.0 / 576)
+    w = torch.from_numpy(np.random.default_rng(302).uniform(-bound, bound, 128 * 64 * 9)
+                         .astype(np.float32)).to(dev)
+    xs = x.cpu().numpy().reshape(32, 64, 56, 56).astype(np.float64)
+    ws = w.cpu().numpy().reshape(128, 64, 3, 3).astype(np.float64)
+    xp = np.pad(xs, ((0, 0), (0, 0), (1, 1), (1, 1)))
+    rng = np.random.default_rng(7)
+    pts = rng.integers(0, [32, 56, 56, 128], size=(512, 4))
+    exact = np.array([(xp[n, :, h:h + 3, wo:wo + 3] * ws[co]).sum() for n, h, wo, co in pts])
+    out = {"workload": "conv [32,64,56,56]*[128,64,3,3] s1 p1 (output [n,ho,wo,co])",
+           "gflop": flops / 1e9}
+    for prec in ("fp32", "bf16", "bf16x3"):
+        c = ltb.Compiled(ir, precision=prec)
+        y = torch.empty(c.io_sizes[-1], device=dev)
+        ms = timed(lambda: c.run([x, w, y], sync=False), 5)
+        got = y.cpu().numpy().reshape(32, 56, 56, 128)[pts[:, 0], pts[:, 1], pts[:, 2], pts[:, 3]]
+        out[prec] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+                     "normwise_err_vs_fp64_sampled": float(np.linalg.norm(got - exact) /
+                                                           np.linalg.norm(exact))}
+    return out
+
+
+# ----------------------------------------------------------------- c4
+def extra_c4(dev):
+    import torch
+
+    import loop_tool_b200 as ltb
+
+    _, bf16_peak, _ = load_peaks()
+    rng = np.random.default_rng(401)
+    v = np.exp(rng.uniform(math.log(64), math.log(4096), size=(512, 3)))
+    sizes = [tuple(int(max(16, 16 * round(x / 16))) for x in row) for row in v]
+    irs = [mm_ir(M, K, N) for M, N, K in sizes]
+    g = torch.Generator(device=dev).manual_seed(402)
+    bufs = []
+    for M, N, K in sizes:
+        bufs.append([torch.randn(M * K, device=dev, generator=g) / math.sqrt(K),
+                     torch.randn(K * N, device=dev, generator=g),
+                     torch.empty(M * N, device=dev)])
+    flops = sum(2.0 * M * N * K for M, N, K in sizes)
+    out = {"workload": "512 matmuls, M,N,K log-uniform [64,4096] x16, one grouped launch",
+           "tflop": flops / 1e12}
+    st = torch.cuda.Stream()
+    for prec in ("bf16", "bf16x3", "fp32"):
+        members = [(ltb.Compiled(ir, precision=prec), b) for ir, b in zip(irs, bufs)]
+        batch = ltb.Batch(members, capture_stream=st.cuda_stream)
+        with torch.cuda.stream(st):
+            ms = timed(lambda: batch.run(sync=False, stream=st.cuda_stream),
+                       3 if prec != "fp32" else 1, stream=st)
+            pack_ms, gemm_ms = batch.run_timed(stream=st.cuda_stream)
+        # sampled FP64 check of a few problems
+        errs = []
+        for i in (0, 100, 257, 511):
+            M, N, K = sizes[i]
+            a = bufs[i][0].cpu().numpy().reshape(M, K).astype(np.float64)
+            bb = bufs[i][1].cpu().numpy().reshape(K, N).astype(np.float64)
+            ex = a @ bb
+            errs.append(float(np.linalg.norm(bufs[i][2].cpu().numpy().reshape(M, N) - ex) /
+                              np.linalg.norm(ex)))
+        out[prec] = {"graph_replay_ms": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+                     "pack_ms": pack_ms, "gemm_ms": gemm_ms,
+                     "gemm_tflops": flops / (gemm_ms * 1e-3) / 1e12,
+                     "launches_per_replay": batch.int_property("launches"),
+                     "max_normwise_err_vs_fp64_sampled": max(errs)}
+        del batch, members
+    del bufs
+    torch.cuda.empty_cache()
+    n = 8192
+    A = torch.randn(n * n, device=dev, generator=g)
+    B = torch.randn(n * n, device=dev, generator=g)
+    C = torch.empty(n * n, device=dev)
+    ir = mm_ir(n, n, n)
+    big = {"workload": "8192^3 matmul"}
+    for prec in ("bf16", "bf16x3"):
+        b1 = ltb.Batch([(ltb.Compiled(ir, precision=prec), [A, B, C])])
+        b1.run_timed()
+        pack_ms, gemm_ms = b1.run_timed()
+        products = {"bf16": 1, "bf16x3": 3}[prec]
+        big[prec] = {"total_ms": pack_ms + gemm_ms, "pack_ms": pack_ms, "gemm_ms": gemm_ms,
+                     "tflops_total": 2 * n ** 3 / ((pack_ms + gemm_ms) * 1e-3) / 1e12,
+                     "tensor_tflops_gemm": products * 2 * n ** 3 / (gemm_ms * 1e-3) / 1e12,
+                     "frac_of_measured_bf16_peak": products * 2 * n ** 3 / (gemm_ms * 1e-3) /
+                     1e12 / bf16_peak}
+        del b1
+    out["mm_8192"] = big
+    return out
+
+
+# ----------------------------------------------------------------- c5
+def extra_c5(dev, n_requests, rates):
+    from loop_tool_b200.serve import Server, make_trace
+
+    out = {"workload": f"{n_requests} requests, Poisson arrivals, 50% matmul (c4 shapes), "
+                       f"30% conv (batch U[1,64]), 20% softmax (rows U[1,8192] x 4096)",
+           "kernel_cache": "warm (one pass over the trace first)"}
+    configs = [("b200_bf16x3_8slots", dict(slots=8, precision="bf16x3")),
+               ("plain_fp32_1slot", dict(slots=1, precision="fp32"))]
+    for rate in rates:
+        trace = make_trace(n_requests, rate=rate, seed=501)
+        row = {}
+        for name, kw in configs:
+            srv = Server(hbm_budget=24 << 30, **kw)
+            warm = make_trace(n_requests, rate=1e9, seed=501)
+            for r in warm:  # populate the IR and kernel caches
+                srv.bytes_of(r)
+            stats, _ = srv.serve(make_trace(n_requests, rate=rate, seed=501))
+            row[name] = {k: stats[k] for k in ("req_per_s", "p50_ms", "p99_ms", "mean_ms",
+                                               "peak_inflight")}
+        out[f"rate_{int(rate)}"] = row
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-rates", default="1000,4000")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.init()
+    line = headline(args, world, rank, dev)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and os.path.exists(HARNESS):
         try:
-            v, desc = reference_time([n for n, _ in NESTS])
+            v, desc = reference_time()
             cpu = {"value": v, "unit": "GB/s", "cores": 1, "kind": "reference", "sample": desc}
         except Exception as e:  # reported, never fatal to the GPU number
             cpu = {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",
                    "sample": f"failed: {e}"}
+    line["cpu_baseline"] = cpu
+    if rank == 0 and world == 1 and not args.no_extras:
+        configs = {}
+        for key, fn in (("c1_mm128", lambda: extra_c1(dev)), ("c3_conv", lambda: extra_c3(dev)),
+                        ("c4_batched", lambda: extra_c4(dev)),
+                        ("c5_serving", lambda: extra_c5(
+                            dev, args.serve_requests,
+                            [float(r) for r in args.serve_rates.split(",")]))):
+            try:
+                configs[key] = fn()
+            except Exception as e:  # one failing extra must not hide the headline
+                configs[key] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
+        line["configs"] = configs
     if rank == 0:
-        print(json.dumps({
-            "metric": "hbm_gbs_bandwidth_nests", "value": value, "unit": "GB/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "bandwidth nests: add 2^28, softmax 8192x4096, "
-                                   "maxpool 64x128x112x112 (FP32, lazy-frontend loop trees)",
-                       "l2": "inputs larger than L2 (126 MB)",
-                       "parallelism": f"replicas{world}"},
-            "nests_ms": {n: t for (n, _), t in zip(NESTS, nest_ms)},
-            "nests_gbs": {n: b / (t / 1e3) / 1e9 for (n, _), b, t in zip(NESTS, bytes_per, nest_ms)},
-            "roofline": {"bound": "hbm", "kernel": NESTS[dom][0], "achieved": achieved,
-                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic},
-            "e2e": {"value": world * step_bytes / e2e_s / 1e9, "unit": "GB/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches,
-            "clocks": clocks,
-            "cpu_baseline": cpu,
-        }))
+        print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -114,6 +114,9 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
  * the legacy default stream); later ltb_batch_run calls replay it. */
 int ltb_batch_capture(ltb_batch* b, void* stream);
 int ltb_batch_run(ltb_batch* b, int sync, void* stream);
+/* One eager run with device timings of its two phases (operand packing and
+ * the grouped GEMM), measured with CUDA events on `stream`; synchronises. */
+int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_ms);
 /* "problems", "flops", "launches", "tiles", "graph". */
 int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value);
 int ltb_batch_release(ltb_batch* b);

@@ -49,6 +49,9 @@ SIGNATURES = {
     "ltb_batch_int_property": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p,
                                               ctypes.POINTER(ctypes.c_int64)]),
     "ltb_batch_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "ltb_batch_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_float),
+                                           ctypes.POINTER(ctypes.c_float)]),
 }
 
 

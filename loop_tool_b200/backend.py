@@ -209,6 +209,14 @@ class Batch:
         _lib.check(_lib.lib().ltb_batch_int_property(self._h, name.encode(), ctypes.byref(v)))
         return v.value
 
+    def run_timed(self, stream=None):
+        """(pack_ms, gemm_ms) of one eager run, CUDA-event timed."""
+        if stream is None:
+            stream = _current_stream()
+        a, b = ctypes.c_float(), ctypes.c_float()
+        _lib.check(_lib.lib().ltb_batch_run_timed(self._h, stream, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h and _lib._lib is not None:

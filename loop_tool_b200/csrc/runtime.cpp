@@ -715,6 +715,38 @@ int ltb_batch_capture(ltb_batch* b, void* stream) {
   return LTB_OK;
 }
 
+int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_ms) {
+  if (!b || !pack_ms || !gemm_ms) return fail(LTB_ERR_INVALID, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+  try {
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventCreate(&e2));
+    CUDA_TRY(cudaEventRecord(e0, st));
+    if (b->tc) CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st));
+    CUDA_TRY(cudaEventRecord(e1, st));
+    if (b->tc)
+      CUDA_TRY(ltb_launch_gemm_tc(b->d_tc, b->n, b->tc_tiles, nullptr, b->sms, b->d_err, st));
+    else
+      CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles, st));
+    CUDA_TRY(cudaEventRecord(e2, st));
+    CUDA_TRY(cudaEventSynchronize(e2));
+    CUDA_TRY(cudaEventElapsedTime(pack_ms, e0, e1));
+    CUDA_TRY(cudaEventElapsedTime(gemm_ms, e1, e2));
+  } catch (const std::exception& e) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e2) cudaEventDestroy(e2);
+    return fail(LTB_ERR_CUDA, e.what());
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  return batch_finish(b, 1, st);
+}
+
 int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   if (!b || !name || !value) return fail(LTB_ERR_INVALID, "null argument");
   std::string k = name;
