@@ -112,12 +112,12 @@ def dist_setup():
 
 
 # ------------------------------------------------------------- workloads
-def nests():
+def nests(add_log2=28):
     """The three bandwidth nests, built with the lazy frontend."""
     import loop_tool_b200.lazy as lt
     import loop_tool_b200.nn as nn
 
-    A, B = lt.Tensor(1 << 28), lt.Tensor(1 << 28)
+    A, B = lt.Tensor(1 << add_log2), lt.Tensor(1 << add_log2)
     N = lt.Symbol("N")
     add = A.to(N) + B.to(N)
     X = lt.Tensor(8192, 4096)
@@ -128,7 +128,7 @@ def nests():
     P = lt.Tensor(64, 128, 112, 112)
     b, c, h, w = (lt.Symbol(s) for s in "nchw")
     pool = nn.maxpool(P.to(b, c, h, w), [h, w], 2, 2)
-    return [("add_2p28", add.ir, 1.0), ("softmax_8192x4096", softmax.ir, 4.0),
+    return [(f"add_2p{add_log2}", add.ir, 1.0), ("softmax_8192x4096", softmax.ir, 4.0),
             ("maxpool_64x128x112x112", pool.ir, 1.0)]
 
 
@@ -210,7 +210,7 @@ def headline(args, world, rank, dev):
 
     import loop_tool_b200 as ltb
 
-    comps, bufs, bytes_per = [], [], []
+    comps, bufs, bytes_per, schedules = [], [], [], {}
     g = torch.Generator(device=dev)
     g.manual_seed(1234 + rank)
     for name, ir, scale in nests():
@@ -220,6 +220,9 @@ def headline(args, world, rank, dev):
         comps.append((name, c))
         bufs.append(ins + outs)
         bytes_per.append(4 * sum(c.io_sizes))
+        if args.tune:  # the autotuner picks each stage's schedule (untimed)
+            schedules[name] = [ln.strip() for ln in c.tune(ins + outs, reps=5).splitlines()
+                               if ln.startswith("  ")]
     stream = torch.cuda.current_stream()
 
     def step(times=None):
@@ -296,7 +299,9 @@ def headline(args, world, rank, dev):
         "config": {"workload": "bandwidth nests: add 2^28, softmax 8192x4096, maxpool "
                                "64x128x112x112 (FP32 lazy-frontend loop trees)",
                    "l2": "inputs larger than L2 (126 MB), no flush needed",
+                   "schedules": "autotuned before warm-up" if args.tune else "heuristic",
                    "parallelism": f"replicas{world}"},
+        "schedules": schedules,
         "nests_ms": {n: t for (n, _), t in zip(comps, nest_ms)},
         "nests_gbs": {n: b / (t / 1e3) / 1e9 for (n, _), b, t in zip(comps, bytes_per, nest_ms)},
         "nests_frac_of_hbm": {n: b / (t / 1e3) / 1e9 / hbm_peak
@@ -390,11 +395,18 @@ def extra_c3(dev):
     for prec in ("fp32", "bf16", "bf16x3"):
         c = ltb.Compiled(ir, precision=prec)
         y = torch.empty(c.io_sizes[-1], device=dev)
+        schedule = c.tune([x, w, y], reps=3).strip().splitlines()
         ms = timed(lambda: c.run([x, w, y], sync=False), 5)
         got = y.cpu().numpy().reshape(32, 56, 56, 128)[pts[:, 0], pts[:, 1], pts[:, 2], pts[:, 3]]
         out[prec] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12,
                      "normwise_err_vs_fp64_sampled": float(np.linalg.norm(got - exact) /
-                                                           np.linalg.norm(exact))}
+                                                           np.linalg.norm(exact)),
+                     "schedule": [ln.strip() for ln in schedule if ln.startswith("  ")]}
+        if prec != "fp32":  # im2col packing vs tensor-core time
+            b1 = ltb.Batch([(c, [x, w, y])])
+            b1.run_timed()
+            out[prec]["pack_ms"], out[prec]["gemm_ms"] = b1.run_timed()
+            del b1
     return out
 
 
@@ -421,7 +433,11 @@ def extra_c4(dev):
     st = torch.cuda.Stream()
     for prec in ("bf16", "bf16x3", "fp32"):
         members = [(ltb.Compiled(ir, precision=prec), b) for ir, b in zip(irs, bufs)]
-        batch = ltb.Batch(members, capture_stream=st.cuda_stream)
+        tiles = "cuda cores (128 x 128)"
+        if prec == "fp32":
+            batch = ltb.Batch(members, capture_stream=st.cuda_stream)
+        else:  # tile widths chosen by the autotuner on the grouped launch
+            batch, best, tiles = ltb.tune_batch(members, capture_stream=st.cuda_stream)
         with torch.cuda.stream(st):
             ms = timed(lambda: batch.run(sync=False, stream=st.cuda_stream),
                        3 if prec != "fp32" else 1, stream=st)
@@ -439,6 +455,9 @@ def extra_c4(dev):
                      "pack_ms": pack_ms, "gemm_ms": gemm_ms,
                      "gemm_tflops": flops / (gemm_ms * 1e-3) / 1e12,
                      "launches_per_replay": batch.int_property("launches"),
+                     "tiles": tiles,
+                     "tiles_128_256": [batch.int_property("tiles_128"),
+                                       batch.int_property("tiles_256")],
                      "max_normwise_err_vs_fp64_sampled": max(errs)}
         del batch, members
     del bufs
@@ -450,11 +469,14 @@ def extra_c4(dev):
     ir = mm_ir(n, n, n)
     big = {"workload": "8192^3 matmul"}
     for prec in ("bf16", "bf16x3"):
-        b1 = ltb.Batch([(ltb.Compiled(ir, precision=prec), [A, B, C])])
+        c1 = ltb.Compiled(ir, precision=prec)
+        c1.tune([A, B, C], reps=2)
+        b1 = ltb.Batch([(c1, [A, B, C])])
         b1.run_timed()
         pack_ms, gemm_ms = b1.run_timed()
         products = {"bf16": 1, "bf16x3": 3}[prec]
         big[prec] = {"total_ms": pack_ms + gemm_ms, "pack_ms": pack_ms, "gemm_ms": gemm_ms,
+                     "tile_n": c1.schedule(0)[2],
                      "tflops_total": 2 * n ** 3 / ((pack_ms + gemm_ms) * 1e-3) / 1e12,
                      "tensor_tflops_gemm": products * 2 * n ** 3 / (gemm_ms * 1e-3) / 1e12,
                      "frac_of_measured_bf16_peak": products * 2 * n ** 3 / (gemm_ms * 1e-3) /
@@ -488,6 +510,49 @@ def extra_c5(dev, n_requests, rates):
     return out
 
 
+# ------------------------------------------------------- profiling cases
+NCU_CASES = ("add", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "conv_bf16", "batch_bf16")
+
+
+def ncu_case(name, reps):
+    """One workload at a profiling size (inputs above L2, about 1 GB on the
+    device), run `reps` times: the command ncu captures."""
+    import torch
+
+    import loop_tool_b200 as ltb
+
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(9)
+    opts = {}
+    if name in ("add", "softmax", "maxpool"):
+        ir = {n.split("_")[0]: t for n, t, _ in nests(add_log2=26)}[name]
+    elif name.startswith("mm_"):
+        ir, opts = mm_ir(8192, 8192, 8192), {"precision": name[3:]}
+    elif name == "conv_bf16":
+        ir, opts = conv_ir(32), {"precision": "bf16"}
+    else:
+        rng = np.random.default_rng(401)
+        v = np.exp(rng.uniform(math.log(64), math.log(4096), size=(128, 3)))
+        members = []
+        for row in v:
+            M, N, K = (int(max(16, 16 * round(x / 16))) for x in row)
+            c = ltb.Compiled(mm_ir(M, K, N), precision="bf16")
+            members.append((c, [torch.randn(M * K, device=dev, generator=g),
+                                torch.randn(K * N, device=dev, generator=g),
+                                torch.empty(M * N, device=dev)]))
+        b = ltb.Batch(members)
+        for _ in range(reps):
+            b.run(sync=False)
+        torch.cuda.synchronize()
+        return
+    c = ltb.Compiled(ir, **opts)
+    bufs = [torch.randn(n, device=dev, generator=g) for n in c.io_sizes[:c.n_inputs]]
+    bufs += [torch.empty(n, device=dev) for n in c.io_sizes[c.n_inputs:]]
+    for _ in range(reps):
+        c.run(bufs, sync=False)
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -496,11 +561,18 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="keep the heuristic schedules (no autotuning before warm-up)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rates", default="1000,4000")
+    ap.add_argument("--ncu-case", choices=NCU_CASES,
+                    help="run one workload at a profiling size and exit")
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.ncu_case:
+        return ncu_case(args.ncu_case, args.reps)
 
     import torch
 

@@ -117,7 +117,8 @@ int ltb_batch_run(ltb_batch* b, int sync, void* stream);
 /* One eager run with device timings of its two phases (operand packing and
  * the grouped GEMM), measured with CUDA events on `stream`; synchronises. */
 int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_ms);
-/* "problems", "flops", "launches", "tiles", "graph". */
+/* "problems", "flops", "launches", "tiles", "tiles_128", "tiles_256",
+ * "graph". */
 int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value);
 int ltb_batch_release(ltb_batch* b);
 
@@ -134,6 +135,40 @@ int ltb_batch_release(ltb_batch* b);
  * array's address; make it before any stream capture on that device. */
 int ltb_row_sum_noalloc(const float* x, int64_t rows, int64_t cols, float* out,
                         void* stream);
+
+/* ---------------------------------------------------------- autotuner
+ * Replaces the reference's manual schedule search: python/ui.py:34-45
+ * (benchmark a tensor's loop tree) driving the LoopTree mutations of
+ * include/loop_tool/mutate.h:13-60 (split, annotate, unroll).  Here the
+ * schedule space is the B200 kernels' own: per stage the grid (CTAs per SM,
+ * the "parallel" annotation), the CTA size ("threaded"), the row-softmax
+ * elements/threads pair and the tensor-core tile width (128 or 256).
+ *
+ * ltb_tune times every candidate schedule of every stage on `memory`
+ * (device or managed buffers, as ltb_run), keeps the fastest, leaves the
+ * outputs computed with it, records it in the process-wide schedule cache
+ * and writes a report (one line per stage, in annotation vocabulary) into
+ * report[len] if report is not NULL.  The cache key is a hash of the IR text
+ * (which carries every size) and the compile options; ltb_compile applies a
+ * cached schedule (int property "tuned" = 1).  reps: timed runs per
+ * candidate. */
+int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps,
+             char* report, size_t len);
+/* Read or set one stage's schedule (zeros = the built-in heuristic;
+ * threads in {0, 64, 128, 256, 512}; variant: family-specific). */
+int ltb_get_schedule(ltb_compiled* c, int stage, int* cta_per_sm, int* threads,
+                     int* variant);
+int ltb_set_schedule(ltb_compiled* c, int stage, int cta_per_sm, int threads,
+                     int variant);
+/* Store the compiled object's current schedules in the cache. */
+int ltb_tune_record(ltb_compiled* c);
+/* Cache persistence: a text file holding, per entry, the serialized IR
+ * (src/core/serialization.cpp:175-237 format), the options and one
+ * schedule line per stage.  Loading merges into the cache. */
+int ltb_tune_save(const char* path);
+int ltb_tune_load(const char* path);
+int ltb_tune_clear(void);
+int64_t ltb_tune_entries(void);
 
 /* Stream synchronisation helper (cuCtxSynchronize in the reference,
  * src/backends/cuda/cuda.cpp:847-849, when stream is NULL). */

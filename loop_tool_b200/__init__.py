@@ -5,6 +5,8 @@ Drop-in for the reference's deprecated NVRTC backend
 Compiled.run(memory, sync)), with loop trees passed as serialized IR.
 """
 from ._lib import LoopToolError  # noqa: F401
-from .backend import Batch, Compiled, RawTensor, cuda, device_count, plan  # noqa: F401
+from .backend import (Batch, Compiled, RawTensor, cuda, device_count, plan,  # noqa: F401
+                      tune_batch, tune_clear, tune_entries, tune_load, tune_save)
 
-__all__ = ["Batch", "Compiled", "RawTensor", "cuda", "device_count", "plan", "LoopToolError"]
+__all__ = ["Batch", "Compiled", "RawTensor", "cuda", "device_count", "plan", "LoopToolError",
+           "tune_save", "tune_load", "tune_clear", "tune_entries", "tune_batch"]

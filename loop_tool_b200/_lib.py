@@ -52,6 +52,18 @@ SIGNATURES = {
     "ltb_batch_run_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(ctypes.c_float),
                                            ctypes.POINTER(ctypes.c_float)]),
+    "ltb_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
+    "ltb_get_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]),
+    "ltb_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int]),
+    "ltb_tune_record": (ctypes.c_int, [ctypes.c_void_p]),
+    "ltb_tune_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "ltb_tune_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "ltb_tune_clear": (ctypes.c_int, []),
+    "ltb_tune_entries": (ctypes.c_int64, []),
 }
 
 

@@ -119,8 +119,37 @@ class Compiled:
     @property
     def int_properties(self):
         keys = ("bandwidth", "stages", "launches", "scratch_bytes", "inputs", "outputs",
-                "algorithmic_bytes", "flops")
+                "algorithmic_bytes", "flops", "tuned")
         return {k: self.int_property(k) for k in keys}
+
+    # ------------------------------------------------------------ autotuner
+    def tune(self, memory, reps=10, stream=None):
+        """Time every candidate schedule of every stage on `memory` (device
+        buffers in run order), keep the fastest, record it in the schedule
+        cache; returns the per-stage report.  The outputs in `memory` are
+        left computed with the chosen schedules."""
+        ptrs = [_ptr_and_keep(t)[0] for t in memory]
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        if stream is None:
+            stream = _current_stream()
+        buf = ctypes.create_string_buffer(1 << 16)
+        _lib.check(_lib.lib().ltb_tune(self._h, arr, len(ptrs), stream, int(reps), buf, len(buf)))
+        return buf.value.decode()
+
+    def schedule(self, stage):
+        """(cta_per_sm, threads, variant) of a stage; zeros = heuristic."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.lib().ltb_get_schedule(self._h, int(stage), ctypes.byref(a),
+                                                ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def set_schedule(self, stage, cta_per_sm=0, threads=0, variant=0):
+        _lib.check(_lib.lib().ltb_set_schedule(self._h, int(stage), int(cta_per_sm),
+                                                int(threads), int(variant)))
+
+    def record_schedule(self):
+        """Store the current schedules in the cache (keyed by IR + options)."""
+        _lib.check(_lib.lib().ltb_tune_record(self._h))
 
     @property
     def string_properties(self):
@@ -153,6 +182,57 @@ def _current_stream():
     except Exception:
         pass
     return None
+
+
+def tune_batch(members, capture_stream=None, reps=3):
+    """Tile widths for a batch of contractions, chosen by timing the grouped
+    launch (operand packing + persistent GEMMs) under each policy: the
+    members' current schedules, every problem at 128 or at 256 columns, and
+    each member's own tuned width.  The best policy is left on the members,
+    recorded in the schedule cache, and returned with its Batch and a
+    report."""
+    policies = {"current": [c.schedule(0) for c, _ in members]}
+    policies["all_128"] = [(0, 0, 128)] * len(members)
+    policies["all_256"] = [(0, 0, 256)] * len(members)
+    tuned = []
+    for c, bufs in members:
+        c.tune(bufs, reps=2)
+        tuned.append(c.schedule(0))
+    policies["member_tuned"] = tuned
+    times = {}
+    for name, sched in policies.items():
+        for (c, _), sc in zip(members, sched):
+            c.set_schedule(0, *sc)
+        b = Batch(members)
+        b.run_timed()
+        ms = min(sum(b.run_timed()) for _ in range(reps))
+        times[name] = ms
+        del b
+    best = min(times, key=times.get)
+    for (c, _), sc in zip(members, policies[best]):
+        c.set_schedule(0, *sc)
+        c.record_schedule()
+    report = "; ".join(f"{k} {v:.3f} ms" for k, v in times.items()) + f" -> {best}"
+    return Batch(members, capture_stream=capture_stream), best, report
+
+
+def tune_save(path):
+    """Write the schedule cache (IR text + options + per-stage schedule)."""
+    _lib.check(_lib.lib().ltb_tune_save(str(path).encode()))
+
+
+def tune_load(path):
+    """Merge a schedule file into the cache; later compiles of the same IR
+    and options start from the stored schedules."""
+    _lib.check(_lib.lib().ltb_tune_load(str(path).encode()))
+
+
+def tune_clear():
+    _lib.check(_lib.lib().ltb_tune_clear())
+
+
+def tune_entries():
+    return int(_lib.lib().ltb_tune_entries())
 
 
 def cuda(loop_tree, **opts):

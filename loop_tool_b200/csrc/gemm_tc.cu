@@ -35,13 +35,26 @@
 
 namespace {
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int BM = 128, BK = 64;
 constexpr int NT = 320;
 constexpr int kChunkBlocks = 8;  // 8 x 64 = 512 K elements per accumulator
-constexpr uint32_t TMEM_COLS = 512;
 constexpr int A_BYTES = BM * BK * 2;
-constexpr int B_BYTES = BN * BK * 2;
-constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+
+// Tile shapes: BM x BN output tiles, BN = 256 (4-stage ring of 48 KB) or
+// BN = 128 (6-stage ring of 32 KB; narrow outputs and small problems).
+template <int BN_>
+struct Tile {
+  static constexpr int B_BYTES = BN_ * BK * 2;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int STAGES = BN_ == 256 ? 4 : 6;
+  static constexpr uint32_t TMEM_COLS = 2 * BN_;  // two accumulator buffers
+  static constexpr int HALF = BN_ / 2;            // columns per drain thread
+  // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+  // K-major, M = 128, N = BN
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
+                                    ((uint32_t)(BN_ >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+  static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 256;
+};
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -102,17 +115,12 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
          (uint64_t)1 << 46 | (uint64_t)2 << 61;
 }
 
-// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
-// K-major, M = 128, N = 256.
-constexpr uint32_t kIdesc =
-    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b,
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
                                          uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -155,6 +163,7 @@ __device__ __forceinline__ int find_problem(const LtbTcProblem* __restrict__ P, 
 // the ~148 tiles in flight cover a compact 16 x 9 block region whose A and
 // B panels stay resident in L2.
 constexpr int kGroupM = 16;
+template <int BN>
 __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, int* m0, int* n0) {
   const int64_t per_group = (int64_t)kGroupM * p.tiles_n;
   const int g = (int)(lt / per_group);
@@ -164,6 +173,7 @@ __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, i
   *n0 = (idx / gm) * BN;
 }
 
+template <int BN>
 __global__ void __launch_bounds__(NT, 1)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
               float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
@@ -171,6 +181,8 @@ __global__ void __launch_bounds__(NT, 1)
               const __grid_constant__ CUtensorMap single_b) {
   // probs == nullptr: one problem passed by value with its tensor maps as
   // kernel parameters (encoded at launch over per-run scratch)
+  using T = Tile<BN>;
+  constexpr int STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -196,7 +208,7 @@ __global__ void __launch_bounds__(NT, 1)
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS));
+                 "r"(T::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -215,7 +227,7 @@ __global__ void __launch_bounds__(NT, 1)
       const CUtensorMap* mb =
           probs ? static_cast<const CUtensorMap*>(p.map_b) : &single_b;
       int m0, n0;
-      tile_coords(p, t - p.tile_start, &m0, &n0);
+      tile_coords<BN>(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % STAGES;
@@ -258,7 +270,7 @@ __global__ void __launch_bounds__(NT, 1)
           const uint64_t ad = sw128_desc(a0), bd = sw128_desc(a0 + A_BYTES);
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk)  // +32 bytes per K=16 step
-            mma_bf16(acc, ad + 2 * kk, bd + 2 * kk, (kb != c0) || (kk != 0));
+            mma_bf16(acc, ad + 2 * kk, bd + 2 * kk, T::IDESC, (kb != c0) || (kk != 0));
           mma_commit(smem_u32(&empty[s]));  // stage reusable once these finish
         }
         mma_commit(smem_u32(&chunk_full[buf]));  // chunk complete in TMEM
@@ -267,17 +279,17 @@ __global__ void __launch_bounds__(NT, 1)
   } else if (warp >= 2) {
     // ------------------------------------------------------ drain/epilogue
     const int quad = warp & 3;            // TMEM lanes 32*quad .. +31
-    const int half = (warp - 2) >> 2;     // columns 128*half .. +127
+    const int half = (warp - 2) >> 2;     // columns HALF*half .. +HALF-1
     uint32_t q = 0;
     bool alive = true;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       int m0, n0;
-      tile_coords(p, t - p.tile_start, &m0, &n0);
+      tile_coords<BN>(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
-      float run[128];
+      float run[T::HALF];
 #pragma unroll
-      for (int i = 0; i < 128; ++i) run[i] = 0.f;
+      for (int i = 0; i < T::HALF; ++i) run[i] = 0.f;
       for (int c0 = 0; c0 < nk; c0 += kChunkBlocks, ++q) {
         const int buf = q & 1;
         const bool ok = mbar_wait(smem_u32(&chunk_full[buf]), (q >> 1) & 1u, err);
@@ -287,9 +299,9 @@ __global__ void __launch_bounds__(NT, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t base =
-            tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * BN + half * 128);
+            tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * BN + half * T::HALF);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < T::HALF / 32; ++c) {
           uint32_t r[32];
           tmem_ld32(base + (uint32_t)(c * 32), r);
           tmem_wait_ld();
@@ -300,14 +312,14 @@ __global__ void __launch_bounds__(NT, 1)
         mbar_arrive(smem_u32(&chunk_empty[buf]));  // buffer free for the MMA
       }
       if (!alive) break;
-      // epilogue: this thread owns row m0 + 32*quad + lane, 128 columns
+      // epilogue: this thread owns row m0 + 32*quad + lane, HALF columns
       const int row = m0 + quad * 32 + lane;
       if (row < p.M) {
         const int64_t rbase = p.crow[row];
         float* dst = (c_override ? c_override : p.c) + rbase;
-        const int cbase = n0 + half * 128;
+        const int cbase = n0 + half * T::HALF;
 #pragma unroll
-        for (int c = 0; c < 128; c += 4) {
+        for (int c = 0; c < T::HALF; c += 4) {
           const int j = cbase + c;
           if (p.unit_cols && j + 4 <= p.N && ((rbase + j) & 3) == 0) {
             *reinterpret_cast<float4*>(dst + j) =
@@ -326,142 +338,220 @@ __global__ void __launch_bounds__(NT, 1)
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(TMEM_COLS));
+                 "r"(T::TMEM_COLS));
 }
 
 // ------------------------------------------------------------ packing
 // Gathers an operand through its separable description and writes the BF16
 // split of every element into nseg K-segments of a K-major matrix: bit s of
 // seg_mask selects the hi part (1) or the lo part (0, x - hi rounded to
-// BF16) for segment s.
-__device__ __forceinline__ float pack_fetch(const LtbGemmOperand& op, int64_t rows, int64_t K,
-                                            int64_t r, int64_t k) {
-  if (r >= rows || k >= K) return 0.f;
-  if (op.dense) return __ldg(op.base + r * op.ld_row + k * op.ld_k);
-  for (int g = 0; g < op.nguard; ++g) {
-    const int32_t v = op.grow[(int64_t)g * rows + r] + op.gk[(int64_t)g * K + k];
-    if (v < 0 || v >= op.gub[g]) return 0.f;
+// BF16) for segment s.  Columns [nseg*K, Kp) of every row are zeroed (the
+// packed buffers live in reused scratch).
+//
+// Work unit: a 64-row x 64-k tile.  Each CTA takes a contiguous range of
+// tiles (one job search per CTA, sequential addresses).  Four load modes:
+//   kPackDenseK   dense, k-contiguous: float4 loads, 16-byte BF16 stores,
+//                 no shared memory
+//   kPackDenseR   dense, row-contiguous (B[k, n] feeding B'[n, k]): float4
+//                 loads along rows into a shared tile, transposed on the
+//                 way out
+//   kPackGatherK / kPackGatherR  guarded gathers (padding, views), lanes
+//                 along k or along rows, through the shared tile
+constexpr int PR = 64, PKT = 64, PACK_THREADS = 256;
+
+// 8 consecutive k of row r (k < K) split and stored into every segment.
+__device__ __forceinline__ void pack_store8(const LtbPackJob& J, int64_t r, int64_t k,
+                                            const float (&x)[8]) {
+  uint32_t hi[4], lo[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * e], x[2 * e + 1]);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(x[2 * e] - hf.x, x[2 * e + 1] - hf.y);
+    hi[e] = *reinterpret_cast<const uint32_t*>(&h);
+    lo[e] = *reinterpret_cast<const uint32_t*>(&l);
   }
-  return __ldg(op.base + op.rowoff[r] + op.koff[k]);
-}
-
-__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __float2bfloat16_rn(x);
-  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-}
-
-// Operands contiguous along k: 4 consecutive k per thread, 128-bit loads and
-// 64-bit stores when the dense layout allows.
-__global__ void __launch_bounds__(256)
-    k_pack_k(LtbGemmOperand op, int64_t rows, int64_t K, __nv_bfloat16* __restrict__ out,
-             int64_t Kp, int nseg, int seg_mask) {
-  const int64_t k4n = (K + 3) / 4;
-  const bool vec = op.dense && op.ld_k == 1 && (op.ld_row & 3) == 0 &&
-                   ((reinterpret_cast<uintptr_t>(op.base) & 15) == 0) && (K & 3) == 0;
-  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < rows * k4n;
-       w += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = w / k4n, k = (w - r * k4n) * 4;
-    float x[4];
-    if (vec) {
-      const float4 t = __ldg(reinterpret_cast<const float4*>(op.base + r * op.ld_row + k));
-      x[0] = t.x; x[1] = t.y; x[2] = t.z; x[3] = t.w;
+  __nv_bfloat16* out = static_cast<__nv_bfloat16*>(J.out);
+  const int nv = J.K - k < 8 ? (int)(J.K - k) : 8;
+  const uint4 H = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+  const uint4 L = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  for (int s = 0; s < J.nseg; ++s) {
+    const uint4 v = (J.seg_mask >> s) & 1 ? H : L;
+    const int64_t off = r * J.Kp + s * J.K + k;
+    if (nv == 8 && (off & 7) == 0) {
+      *reinterpret_cast<uint4*>(out + off) = v;
     } else {
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-      for (int e = 0; e < 4; ++e) x[e] = pack_fetch(op, rows, K, r, k + e);
+      for (int e = 0; e < 8; ++e)
+        if (e < nv) {
+          const unsigned short b = (unsigned short)(w[e >> 1] >> (16 * (e & 1)));
+          out[off + e] = __ushort_as_bfloat16(b);
+        }
     }
-    __nv_bfloat16 hi[4], lo[4];
+  }
+}
+
+static_assert(sizeof(LtbPackJob) % 8 == 0, "job copied as 8-byte words");
+
+struct PackTables {
+  int64_t roff[PR], koff[PKT];
+  int32_t grow[LTB_MAXG][PR], gk[LTB_MAXG][PKT], gub[LTB_MAXG];
+};
+
+__device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
+                                          float (*sm)[PR + 1], PackTables* tabs) {
+  const int tid = threadIdx.x;
+  const int64_t r0 = (lt / J.tiles_k) * PR, k0 = (lt % J.tiles_k) * PKT;
+  if (J.mode == kPackDenseK) {
+    float x[2][8];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) split_bf16(x[e], hi[e], lo[e]);
-    __nv_bfloat16* dst = out + r * Kp + k;
-    if (k == 0)  // K padding of this row: scratch is reused, keep it zero
-      for (int64_t c = nseg * K; c < Kp; ++c) out[r * Kp + c] = __float2bfloat16_rn(0.f);
-    for (int s = 0; s < nseg; ++s) {
-      const __nv_bfloat16* v = (seg_mask >> s) & 1 ? hi : lo;
-      __nv_bfloat16* d = dst + s * K;
-      if (vec && ((r * Kp + s * K + k) & 3) == 0) {
-        __nv_bfloat162 a, b;
-        a.x = v[0]; a.y = v[1]; b.x = v[2]; b.y = v[3];
-        uint2 u;
-        u.x = *reinterpret_cast<uint32_t*>(&a);
-        u.y = *reinterpret_cast<uint32_t*>(&b);
-        *reinterpret_cast<uint2*>(d) = u;
-      } else {
+    for (int i = 0; i < 2; ++i) {
+      const int64_t r = r0 + (tid >> 3) + 32 * i, k = k0 + (tid & 7) * 8;
+      const bool rok = r < J.rows;
+      const float* p = J.op.base + r * J.op.ld_row + k;
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 u = rok && k < J.K ? __ldg(reinterpret_cast<const float4*>(p)) : z;
+      const float4 v = rok && k + 4 < J.K ? __ldg(reinterpret_cast<const float4*>(p + 4)) : z;
+      x[i][0] = u.x; x[i][1] = u.y; x[i][2] = u.z; x[i][3] = u.w;
+      x[i][4] = v.x; x[i][5] = v.y; x[i][6] = v.z; x[i][7] = v.w;
+    }
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (k + e < K) d[e] = v[e];
+    for (int i = 0; i < 2; ++i) {
+      const int64_t r = r0 + (tid >> 3) + 32 * i, k = k0 + (tid & 7) * 8;
+      if (r < J.rows && k < J.K) pack_store8(J, r, k, x[i]);
+    }
+  } else {
+    // shared tile sm[k][r], row pitch 65 floats
+    if (J.mode == kPackDenseR) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int idx = tid + PACK_THREADS * q;
+        const int kl = idx >> 4, rl = (idx & 15) * 4;
+        const int64_t k = k0 + kl, r = r0 + rl;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k < J.K && r < J.rows)  // rows % 4 == 0 in this mode
+          v = __ldg(reinterpret_cast<const float4*>(J.op.base + k * J.op.ld_k + r));
+        sm[kl][rl] = v.x; sm[kl][rl + 1] = v.y; sm[kl][rl + 2] = v.z; sm[kl][rl + 3] = v.w;
       }
-    }
-  }
-}
-
-// Operands contiguous along rows (e.g. B[k, n] feeding B'[n, k]): a 32 x 32
-// tile transposed through shared memory, reads coalesced along rows, writes
-// coalesced along k.
-__global__ void __launch_bounds__(256)
-    k_pack_r(LtbGemmOperand op, int64_t rows, int64_t K, __nv_bfloat16* __restrict__ out,
-             int64_t Kp, int nseg, int seg_mask) {
-  __shared__ float tile[32][33];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  const int64_t r0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 32;
+    } else {
+      // guarded gather: the tile's row and k tables staged in shared memory
+      // (offsets and guard partials), so each element costs one global load
+      PackTables& tb = *tabs;
+      const int ng = J.op.dense ? 0 : J.op.nguard;
+      if (tid < 64) {
+        const int64_t k = k0 + tid;
+        const bool ok = k < J.K;
+        tb.koff[tid] = !ok ? 0 : J.op.dense ? k * J.op.ld_k : J.op.koff[k];
+        for (int g = 0; g < ng; ++g) tb.gk[g][tid] = ok ? J.op.gk[(int64_t)g * J.K + k] : 0;
+      } else if (tid < 128) {
+        const int rl = tid - 64;
+        const int64_t r = r0 + rl;
+        const bool ok = r < J.rows;
+        tb.roff[rl] = !ok ? 0 : J.op.dense ? r * J.op.ld_row : J.op.rowoff[r];
+        for (int g = 0; g < ng; ++g) tb.grow[g][rl] = ok ? J.op.grow[(int64_t)g * J.rows + r] : 0;
+      } else if (tid < 128 + LTB_MAXG) {
+        if (tid - 128 < ng) tb.gub[tid - 128] = J.op.gub[tid - 128];
+      }
+      __syncthreads();
+      const int64_t rlim = J.rows - r0, klim = J.K - k0;
+      // one side of the element grid is fixed per thread (64 divides the
+      // block), so its offset and guard partials stay in registers
+      const bool along_r = J.mode == kPackGatherR;
+      const int fixed = tid & 63;
+      const bool fok = fixed < (along_r ? rlim : klim);
+      const int64_t fo = along_r ? tb.roff[fixed] : tb.koff[fixed];
+      int32_t fg[LTB_MAXG], ub[LTB_MAXG];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int a = ty + 8 * q;
-    tile[tx][a] = pack_fetch(op, rows, K, r0 + tx, k0 + a);
-  }
-  __syncthreads();
+      for (int g = 0; g < LTB_MAXG; ++g) {
+        fg[g] = g < ng ? (along_r ? tb.grow[g][fixed] : tb.gk[g][fixed]) : 0;
+        ub[g] = g < ng ? tb.gub[g] : 1;
+      }
+#pragma unroll 4
+      for (int q = 0; q < 16; ++q) {
+        const int v_ = (tid >> 6) + 4 * q;  // the varying side (warp-uniform)
+        float v = 0.f;
+        if (fok && v_ < (along_r ? klim : rlim)) {
+          bool ok = true;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int a = ty + 8 * q;
-    const int64_t r = r0 + a, k = k0 + tx;
-    if (r >= rows || k >= K) continue;
-    __nv_bfloat16 hi, lo;
-    split_bf16(tile[a][tx], hi, lo);
-    __nv_bfloat16* dst = out + r * Kp + k;
-    if (k == 0)  // K padding of this row: scratch is reused, keep it zero
-      for (int64_t c = nseg * K; c < Kp; ++c) out[r * Kp + c] = __float2bfloat16_rn(0.f);
-    for (int s = 0; s < nseg; ++s) dst[s * K] = (seg_mask >> s) & 1 ? hi : lo;
-  }
-}
-
-// Every operand of a batch in one launch: CTAs stride over the 32 x 32
-// tiles of all jobs (job found by binary search on tile_start).
-__global__ void __launch_bounds__(256)
-    k_pack_grouped(const LtbPackJob* __restrict__ jobs, int njobs, int64_t total_tiles) {
-  __shared__ float tile[32][33];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int64_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (jobs[mid].tile_start <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    const LtbPackJob& J = jobs[lo];
-    const int64_t lt = t - J.tile_start;
-    const int64_t r0 = (lt / J.tiles_k) * 32, k0 = (lt % J.tiles_k) * 32;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int a = ty + 8 * q;
-      if (J.k_contig)
-        tile[a][tx] = pack_fetch(J.op, J.rows, J.K, r0 + a, k0 + tx);
-      else
-        tile[tx][a] = pack_fetch(J.op, J.rows, J.K, r0 + tx, k0 + a);
+          for (int g = 0; g < LTB_MAXG; ++g) {
+            if (g < ng) {
+              const int32_t w = fg[g] + (along_r ? tb.gk[g][v_] : tb.grow[g][v_]);
+              ok = ok && w >= 0 && w < ub[g];
+            }
+          }
+          if (ok) v = __ldg(J.op.base + fo + (along_r ? tb.koff[v_] : tb.roff[v_]));
+        }
+        if (along_r) sm[v_][fixed] = v;
+        else sm[fixed][v_] = v;
+      }
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int a = ty + 8 * q;
-      const int64_t r = r0 + a, k = k0 + tx;
+    for (int i = 0; i < 2; ++i) {
+      const int c = tid + PACK_THREADS * i;
+      const int rl = c >> 3, kc = c & 7;
+      const int64_t r = r0 + rl, k = k0 + kc * 8;
       if (r < J.rows && k < J.K) {
-        __nv_bfloat16 hi, lo;
-        split_bf16(tile[a][tx], hi, lo);
-        __nv_bfloat16* row = static_cast<__nv_bfloat16*>(J.out) + r * J.Kp;
-        if (k == 0)
-          for (int64_t c = J.nseg * J.K; c < J.Kp; ++c) row[c] = __float2bfloat16_rn(0.f);
-        for (int s = 0; s < J.nseg; ++s) row[k + s * J.K] = (J.seg_mask >> s) & 1 ? hi : lo;
+        float x[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) x[e] = sm[kc * 8 + e][rl];
+        pack_store8(J, r, k, x);
       }
     }
-    __syncthreads();
+    __syncthreads();  // the next tile overwrites sm
+  }
+  if (k0 == 0) {  // K padding [nseg*K, Kp) of this tile's rows
+    const int pad = (int)(J.Kp - J.nseg * J.K);
+    __nv_bfloat16* out = static_cast<__nv_bfloat16*>(J.out);
+    for (int c = tid; c < PR * pad; c += PACK_THREADS) {
+      const int64_t r = r0 + c / pad;
+      if (r < J.rows) out[r * J.Kp + J.nseg * J.K + c % pad] = __float2bfloat16_rn(0.f);
+    }
+  }
+}
+
+__device__ __forceinline__ void tile_range(int64_t total, int64_t& t0, int64_t& t1) {
+  t0 = total * blockIdx.x / gridDim.x;
+  t1 = total * (blockIdx.x + 1) / gridDim.x;
+}
+
+__global__ void __launch_bounds__(PACK_THREADS, 4)
+    k_pack_one(const __grid_constant__ LtbPackJob J, int64_t total_tiles) {
+  __shared__ float sm[PKT][PR + 1];
+  __shared__ PackTables tabs;
+  int64_t t0, t1;
+  tile_range(total_tiles, t0, t1);
+  for (int64_t t = t0; t < t1; ++t) pack_tile(J, t, sm, &tabs);
+}
+
+// Every operand of a batch in one launch; the job of a tile is found by
+// binary search on tile_start once per CTA, then by stepping forward.
+__global__ void __launch_bounds__(PACK_THREADS, 4)
+    k_pack_grouped(const LtbPackJob* __restrict__ jobs, int njobs, int64_t total_tiles) {
+  __shared__ float sm[PKT][PR + 1];
+  __shared__ PackTables tabs;
+  int64_t t0, t1;
+  tile_range(total_tiles, t0, t1);
+  if (t0 >= t1) return;
+  __shared__ LtbPackJob sj;  // the current job, read from shared memory
+  int j = 0, hi = njobs - 1, cur = -1;
+  while (j < hi) {
+    const int mid = (j + hi + 1) >> 1;
+    if (jobs[mid].tile_start <= t0) j = mid;
+    else hi = mid - 1;
+  }
+  for (int64_t t = t0; t < t1; ++t) {
+    while (j + 1 < njobs && jobs[j + 1].tile_start <= t) ++j;
+    if (j != cur) {  // uniform across the block
+      __syncthreads();
+      const uint64_t* src = reinterpret_cast<const uint64_t*>(jobs + j);
+      for (int i = threadIdx.x; i < (int)(sizeof(LtbPackJob) / 8); i += PACK_THREADS)
+        reinterpret_cast<uint64_t*>(&sj)[i] = src[i];
+      __syncthreads();
+      cur = j;
+    }
+    pack_tile(sj, t - sj.tile_start, sm, &tabs);
   }
 }
 
@@ -495,41 +585,61 @@ cudaError_t ltb_make_tmap(void* map, const void* base, int64_t rows, int64_t Kp,
 }
 
 int ltb_tc_tile_m() { return BM; }
-int ltb_tc_tile_n() { return BN; }
+
+int ltb_pack_mode(const LtbGemmOperand& op, int64_t rows, int64_t K, int k_contig) {
+  const bool aligned = (reinterpret_cast<uintptr_t>(op.base) & 15) == 0;
+  if (op.dense && aligned && op.ld_k == 1 && (op.ld_row & 3) == 0 && (K & 3) == 0)
+    return kPackDenseK;
+  if (op.dense && aligned && op.ld_row == 1 && (op.ld_k & 3) == 0 && (rows & 3) == 0)
+    return kPackDenseR;
+  return k_contig ? kPackGatherK : kPackGatherR;
+}
+
+int64_t ltb_pack_tiles(int64_t rows, int64_t K) {
+  return ((rows + PR - 1) / PR) * ((K + PKT - 1) / PKT);
+}
+
+static int64_t pack_grid(int64_t tiles, int sms) {
+  const int64_t g = (int64_t)sms * 4;
+  return tiles < g ? tiles : g;
+}
 
 cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
-                            int64_t Kp, int nseg, int seg_mask, int k_contig, cudaStream_t st) {
-  __nv_bfloat16* o = static_cast<__nv_bfloat16*>(out);
-  if (k_contig) {
-    const int64_t work = rows * ((K + 3) / 4);
-    int64_t blocks = (work + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    k_pack_k<<<(unsigned)blocks, 256, 0, st>>>(op, rows, K, o, Kp, nseg, seg_mask);
-  } else {
-    dim3 grid((unsigned)((K + 31) / 32), (unsigned)((rows + 31) / 32));
-    if (grid.y > 65535) return cudaErrorInvalidConfiguration;
-    k_pack_r<<<grid, 256, 0, st>>>(op, rows, K, o, Kp, nseg, seg_mask);
-  }
+                            int64_t Kp, int nseg, int seg_mask, int k_contig, int sms,
+                            cudaStream_t st) {
+  LtbPackJob J{};
+  J.op = op;
+  J.out = out;
+  J.rows = rows;
+  J.K = K;
+  J.Kp = Kp;
+  J.tiles_k = (int)((K + PKT - 1) / PKT);
+  J.nseg = nseg;
+  J.seg_mask = seg_mask;
+  J.mode = ltb_pack_mode(op, rows, K, k_contig);
+  const int64_t tiles = ltb_pack_tiles(rows, K);
+  if (tiles == 0) return cudaSuccess;
+  k_pack_one<<<(unsigned)pack_grid(tiles, sms), PACK_THREADS, 0, st>>>(J, tiles);
   return cudaGetLastError();
 }
 
 cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t total_tiles,
                                     int sms, cudaStream_t st) {
-  const int64_t grid = total_tiles < (int64_t)sms * 8 ? total_tiles : (int64_t)sms * 8;
-  k_pack_grouped<<<(unsigned)grid, 256, 0, st>>>(d_jobs, njobs, total_tiles);
+  if (total_tiles == 0) return cudaSuccess;
+  k_pack_grouped<<<(unsigned)pack_grid(total_tiles, sms), PACK_THREADS, 0, st>>>(
+      d_jobs, njobs, total_tiles);
   return cudaGetLastError();
 }
 
-size_t ltb_tc_smem_bytes() { return (size_t)STAGES * STAGE_BYTES + 1024 + 256; }
-
-cudaError_t ltb_launch_gemm_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
-                               float* c_override, int sms, int* err, cudaStream_t st,
-                               const LtbTcProblem* single, const void* map_a, const void* map_b) {
+template <int BN>
+static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
+                             float* c_override, int sms, int* err, cudaStream_t st,
+                             const LtbTcProblem* single, const void* map_a, const void* map_b) {
   static bool attr = false;
-  const size_t smem = ltb_tc_smem_bytes();
+  const size_t smem = Tile<BN>::SMEM;
   if (!attr) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -542,6 +652,20 @@ cudaError_t ltb_launch_gemm_tc(const LtbTcProblem* d_probs, int nprob, int64_t t
     ma = *static_cast<const CUtensorMap*>(map_a);
     mb = *static_cast<const CUtensorMap*>(map_b);
   }
-  k_gemm_tc<<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err, one, ma, mb);
+  k_gemm_tc<BN><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err, one, ma, mb);
   return cudaGetLastError();
+}
+
+cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
+                               int64_t total_tiles, float* c_override, int sms, int* err,
+                               cudaStream_t st, const LtbTcProblem* single, const void* map_a,
+                               const void* map_b) {
+  if (total_tiles == 0) return cudaSuccess;
+  if (bn == 128)
+    return launch_tc<128>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a,
+                          map_b);
+  if (bn == 256)
+    return launch_tc<256>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a,
+                          map_b);
+  return cudaErrorInvalidValue;
 }

@@ -8,20 +8,37 @@
 // Records `msg` as the calling thread's ltb_last_error() and returns code.
 int ltb_set_last_error(int code, const char* msg);
 
+// Launch schedule of one stage, chosen by the autotuner (zero fields keep
+// the built-in heuristic).  cta_per_sm: grid = SMs x cta_per_sm CTAs
+// (grid-stride kernels); threads: CTA size; variant: family-specific
+// (row softmax: elements/threads pair; contraction: tile width 128/256).
+struct LtbCfg {
+  int cta_per_sm;
+  int threads;
+  int variant;
+};
+
+
 // (a) elementwise nests and (b) serial reductions
 cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
-                            const LtbBufTable& bt, int sms, cudaStream_t st);
+                            const LtbBufTable& bt, int sms, cudaStream_t st,
+                            const LtbCfg& cfg);
 // (b) block-parallel reductions; splits > 1 writes split-K partials to the
 // stage's partial buffer and combines them in order
 cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,
                               const LtbBufTable& bt, int splits, int sms,
-                              cudaStream_t st);
+                              cudaStream_t st, const LtbCfg& cfg);
 // (b) fused per-row chain of stages (d_stages contiguous, final one
-// elementwise)
-cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, int nsteps,
-                                 const LtbStage& final_stage,
-                                 const LtbBufTable& bt, int sms,
-                                 cudaStream_t st);
+// elementwise; h_stages the host copies of the same stages)
+cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, const LtbStage* const* h_stages,
+                                 int nsteps, const LtbBufTable& bt, int sms,
+                                 cudaStream_t st, const LtbCfg& cfg);
+// Candidate schedules the autotuner tries for a stage of a family (fills up
+// to cap entries, returns the count).  The row-softmax variants depend on
+// the row length.
+int ltb_row_chain_candidates(const LtbStage* const* h_stages, int nsteps, LtbCfg* out, int cap);
+int ltb_nest_candidates(const LtbStage& h, LtbCfg* out, int cap);
+int ltb_reduce_candidates(const LtbStage& h, LtbCfg* out, int cap);
 
 // (c) contractions.  Operand element (i, k) of A lives at
 // a_rowoff[i] + a_koff[k] (B: b_rowoff[j] + b_koff[k]); guards are kept as

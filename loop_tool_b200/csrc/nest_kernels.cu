@@ -3,6 +3,8 @@
 // design points are coalescing, 128-bit accesses along the innermost output
 // dim, and grids sized in multiples of the 148 SMs.
 #include <cfloat>
+#include <mutex>
+#include <unordered_map>
 
 #include "kernels.h"
 #include "vm.cuh"
@@ -770,7 +772,8 @@ __global__ void __launch_bounds__(256)
     float acc[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[j] = S.red_init;
-    for (int64_t rc = 0; rc < RC; ++rc) {
+#pragma unroll 4
+    for (int64_t rc = 0; rc < RC; ++rc) {  // unrolled: the spans' loads issue together
       const float* p = src + base + roff[rc];
       float span[N];
       if (nv == 4 && ((base + roff[rc]) & 3) == 0) {
@@ -801,74 +804,90 @@ __global__ void __launch_bounds__(256)
 }
 
 // ----------------------------------------------------------- row softmax
-// Fused pattern m = max_n x, s = sum_n exp(x - m), y = exp(x - m) / s.
-// One CTA per row, the row held in registers (EPT floats per thread, loaded
-// and stored as float4), so HBM sees one read and one write per element.
+// Fused pattern m = max_n x, s = sum_n exp(x - m), y = exp(x - m) / s, the
+// row held in registers (EPT floats per thread, loaded and stored as
+// float4), so HBM sees one read and one write per element.  One full wave
+// of CTAs strides over the rows; while a row is reduced the next row's loads
+// are already in flight (register double buffer).  The addressing of the
+// chain's three stages is flattened on the host into one parameter block.
 // The max is the reference's ternary fold from -FLT_MAX; its tie and NaN
 // order cannot change y (a NaN anywhere makes s, hence every y, NaN).
+struct SoftmaxRows {
+  const float* x;
+  float *y, *m, *s;
+  int64_t xoff, yoff, moff, soff, n, rows;
+  int nd;  // row dims
+  int64_t size[LTB_MAXD], xc[LTB_MAXD], yc[LTB_MAXD], mc[LTB_MAXD], sc[LTB_MAXD];
+};
+
+struct RowOffs {
+  int64_t x, y, m, s;
+};
+
+__device__ __forceinline__ RowOffs row_offs(const SoftmaxRows& P, int64_t row) {
+  RowOffs o{P.xoff, P.yoff, P.moff, P.soff};
+  for (int k = P.nd - 1; k >= 0; --k) {
+    const int64_t q = k ? row / P.size[k] : 0;
+    const int64_t c = row - q * P.size[k];
+    row = q;
+    o.x += P.xc[k] * c;
+    o.y += P.yc[k] * c;
+    o.m += P.mc[k] * c;
+    o.s += P.sc[k] * c;
+  }
+  return o;
+}
+
+template <int EPT, int NT>
+__device__ __forceinline__ void softmax_load(const SoftmaxRows& P, int64_t xoff, bool v4,
+                                             float (&v)[EPT]) {
+#pragma unroll
+  for (int q = 0; q < EPT / 4; ++q) {
+    const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
+    if (v4 && j < P.n) {
+      const float4 t = __ldcs(reinterpret_cast<const float4*>(P.x + xoff + j));
+      v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v[4 * q + e] = j + e < P.n ? P.x[xoff + j + e] : -INFINITY;
+    }
+  }
+}
+
 template <int EPT, int NT>
 __global__ void __launch_bounds__(NT)
-    k_row_softmax(const LtbStage* __restrict__ gst, LtbBufTable bt, int64_t nrows) {
-  __shared__ __align__(16) LtbStage S[3];
-  __shared__ float red[NT / 32];
-  {
-    const int4* src = reinterpret_cast<const int4*>(gst);
-    int4* dst = reinterpret_cast<int4*>(S);
-    for (int i = threadIdx.x; i < 3 * (int)(sizeof(LtbStage) / 16); i += NT) dst[i] = src[i];
-    __syncthreads();
-  }
-  const LtbStage& A = S[0];  // max over n
-  const LtbStage& B = S[1];  // sum over n
-  const LtbStage& C = S[2];  // elementwise output
-  const LtbLoad& X = A.loads[A.code[0].arg];
-  const int nrd = C.nout - 1;
-  const int64_t n = C.size[nrd];
-  const float* __restrict__ xb = bt.p[X.buf];
-  float* __restrict__ yb = bt.p[C.out_buf];
+    k_softmax_rows(const __grid_constant__ SoftmaxRows P) {
+  __shared__ float red[2][NT / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const bool vec_ok = (n & 3) == 0;
-  for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x) {
-    int64_t xoff = X.off, yoff = C.out_off, moff = A.out_off, soff = B.out_off;
-    {
-      int64_t r = row;
-      for (int k = nrd - 1; k >= 0; --k) {
-        const int64_t q = r / C.size[k];
-        const int64_t c = r - q * C.size[k];
-        r = q;
-        xoff += X.coef[k] * c;
-        yoff += C.out_coef[k] * c;
-        moff += A.out_coef[k] * c;
-        soff += B.out_coef[k] * c;
-      }
+  int64_t row = blockIdx.x;
+  if (row >= P.rows) return;
+  const bool vec_ok = (P.n & 3) == 0;
+  float v[EPT], nx[EPT];
+  RowOffs o = row_offs(P, row);
+  bool v4 = vec_ok && ((o.x | o.y) & 3) == 0;
+  softmax_load<EPT, NT>(P, o.x, v4, v);
+  for (; row < P.rows; row += gridDim.x) {
+    const int64_t nrow = row + gridDim.x;
+    RowOffs no = o;
+    bool nv4 = v4;
+    if (nrow < P.rows) {  // next row's loads go out before this row's reductions
+      no = row_offs(P, nrow);
+      nv4 = vec_ok && ((no.x | no.y) & 3) == 0;
+      softmax_load<EPT, NT>(P, no.x, nv4, nx);
     }
-    const bool v4 = vec_ok && ((xoff | yoff) & 3) == 0;
-    float v[EPT];
-#pragma unroll
-    for (int q = 0; q < EPT / 4; ++q) {
-      const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
-      if (v4 && j < n) {
-        const float4 t = __ldcs(reinterpret_cast<const float4*>(xb + xoff + j));
-        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
-      } else {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) v[4 * q + e] = j + e < n ? xb[xoff + j + e] : -INFINITY;
-      }
-    }
-    // max (ternary fold; padding lanes hold -inf, which never wins)
     float m = -FLT_MAX;
 #pragma unroll
     for (int e = 0; e < EPT; ++e) m = m > v[e] ? m : v[e];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-      const float o = __shfl_xor_sync(0xffffffffu, m, off);
-      m = m > o ? m : o;
+      const float t = __shfl_xor_sync(0xffffffffu, m, off);
+      m = m > t ? m : t;
     }
-    if (lane == 0) red[wid] = m;
+    if (lane == 0) red[0][wid] = m;
     __syncthreads();
-    m = red[0];
+    m = red[0][0];
 #pragma unroll
-    for (int w = 1; w < NT / 32; ++w) m = m > red[w] ? m : red[w];
-    __syncthreads();
+    for (int w = 1; w < NT / 32; ++w) m = m > red[0][w] ? m : red[0][w];
     float sum = 0.f;
 #pragma unroll
     for (int e = 0; e < EPT; ++e) {
@@ -877,53 +896,104 @@ __global__ void __launch_bounds__(NT)
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-    if (lane == 0) red[wid] = sum;
+    if (lane == 0) red[1][wid] = sum;
     __syncthreads();
     sum = 0.f;
 #pragma unroll
-    for (int w = 0; w < NT / 32; ++w) sum += red[w];
-    __syncthreads();
+    for (int w = 0; w < NT / 32; ++w) sum += red[1][w];
     if (threadIdx.x == 0) {  // per-row results stay visible to later stages
-      bt.p[A.out_buf][moff] = m;
-      bt.p[B.out_buf][soff] = sum;
+      P.m[o.m] = m;
+      P.s[o.s] = sum;
     }
 #pragma unroll
     for (int q = 0; q < EPT / 4; ++q) {
       const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
-      if (v4 && j < n) {
-        __stcs(reinterpret_cast<float4*>(yb + yoff + j),
+      if (v4 && j < P.n) {
+        __stcs(reinterpret_cast<float4*>(P.y + o.y + j),
                make_float4(v[4 * q] / sum, v[4 * q + 1] / sum, v[4 * q + 2] / sum,
                            v[4 * q + 3] / sum));
       } else {
 #pragma unroll
         for (int e = 0; e < 4; ++e)
-          if (j + e < n) yb[yoff + j + e] = v[4 * q + e] / sum;
+          if (j + e < P.n) P.y[o.y + j + e] = v[4 * q + e] / sum;
       }
     }
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) v[e] = nx[e];
+    o = no;
+    v4 = nv4;
   }
 }
 
 }  // namespace
 
 // ------------------------------------------------------------ launchers
-static int grid_for(int64_t work, int threads, int sms) {
+// Resident CTAs per SM of a kernel at a block size (occupancy calculator,
+// cached per kernel and block size).  By default grid-stride kernels launch
+// exactly one full wave (SMs x resident CTAs); a schedule's cta_per_sm
+// overrides that (more CTAs than resident = several waves).
+static int resident(const void* kernel, int threads) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache[3];  // 128 / 256 / 512 threads
+  const int slot = threads <= 128 ? 0 : threads <= 256 ? 1 : 2;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = cache[slot].find(kernel);
+  if (it != cache[slot].end()) return it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess ||
+      n < 1) {
+    cudaGetLastError();
+    n = 1;
+  }
+  cache[slot][kernel] = n;
+  return n;
+}
+
+template <typename K>
+static int grid_of(K kernel, int64_t work, int threads, int sms, const LtbCfg& cfg) {
   int64_t blocks = (work + threads - 1) / threads;
-  const int64_t cap = (int64_t)sms * 16;  // 16 resident 256-thread CTAs/SM
+  const int per_sm = cfg.cta_per_sm > 0 ? cfg.cta_per_sm
+                                        : resident(reinterpret_cast<const void*>(kernel), threads);
+  const int64_t cap = (int64_t)sms * per_sm;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   return (int)blocks;
 }
 
+static int pick_threads(const LtbCfg& cfg, int dflt, int maxt) {
+  const int t = cfg.threads > 0 ? cfg.threads : dflt;
+  return t > maxt ? maxt : t;
+}
+
+static const int kWaves[] = {0, 1, 2, 4, 8, 16, 32};
+
+int ltb_nest_candidates(const LtbStage& h, LtbCfg* out, int cap) {
+  int n = 0;
+  for (int w : kWaves)
+    for (int t : {128, 256})
+      if (n < cap) out[n++] = LtbCfg{w, t, 0};
+  return n;
+}
+
+int ltb_reduce_candidates(const LtbStage& h, LtbCfg* out, int cap) {
+  int n = 0;
+  for (int w : {0, 2, 4, 8, 16, 64})
+    for (int t : {64, 128, 256})
+      if (n < cap && (t <= 128 || h.red_total >= 256)) out[n++] = LtbCfg{w, t, 0};
+  return n;
+}
+
 cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
-                            const LtbBufTable& bt, int sms, cudaStream_t st) {
+                            const LtbBufTable& bt, int sms, cudaStream_t st,
+                            const LtbCfg& cfg) {
   const int no = h.nout;
   const int64_t inner = no ? h.size[no - 1] : 1;
   int64_t outer = 1;
   for (int k = 0; k < no - 1; ++k) outer *= h.size[k];
-  const int threads = 256;
+  const int threads = pick_threads(cfg, 256, 256);
   if (h.linear) {
     int64_t total = outer * inner;
-    const int grid = grid_for((total + 7) / 8, threads, sms);
+    const int64_t work8 = (total + 7) / 8;
     // [LOAD a, LOAD b, op] / [LOAD a, op] over linear, 16B-aligned operands
     auto lin = [&](int i) {
       const LtbLoad& L = h.loads[h.code[i].arg];
@@ -936,8 +1006,11 @@ cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
       const float* a = bt.p[h.loads[h.code[0].arg].buf] + h.loads[h.code[0].arg].off;
       const float* b = bt.p[h.loads[h.code[1].arg].buf] + h.loads[h.code[1].arg].off;
       switch (h.code[2].op) {
-#define LTB_BIN(O) \
-  case O: k_lin_bin<O><<<grid, threads, 0, st>>>(a, b, out, total); break;
+#define LTB_BIN(O)                                                                  \
+  case O:                                                                           \
+    k_lin_bin<O><<<grid_of(k_lin_bin<O>, work8, threads, sms, cfg), threads, 0, st>>>( \
+        a, b, out, total);                                                          \
+    break;
         LTB_BIN(LTB_V_ADD) LTB_BIN(LTB_V_SUB) LTB_BIN(LTB_V_MUL) LTB_BIN(LTB_V_DIV)
         LTB_BIN(LTB_V_MIN) LTB_BIN(LTB_V_MAX)
 #undef LTB_BIN
@@ -948,15 +1021,19 @@ cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
         lin(0) && h.code[1].op >= LTB_V_EXP && h.code[1].op <= LTB_V_RECIP) {
       const float* a = bt.p[h.loads[h.code[0].arg].buf] + h.loads[h.code[0].arg].off;
       switch (h.code[1].op) {
-#define LTB_UN(O) \
-  case O: k_lin_un<O><<<grid, threads, 0, st>>>(a, out, total); break;
+#define LTB_UN(O)                                                                 \
+  case O:                                                                         \
+    k_lin_un<O><<<grid_of(k_lin_un<O>, work8, threads, sms, cfg), threads, 0, st>>>( \
+        a, out, total);                                                           \
+    break;
         LTB_UN(LTB_V_EXP) LTB_UN(LTB_V_LOG) LTB_UN(LTB_V_SQRT) LTB_UN(LTB_V_ABS)
         LTB_UN(LTB_V_NEG) LTB_UN(LTB_V_RECIP)
 #undef LTB_UN
       }
       return cudaGetLastError();
     }
-    k_linear<4><<<grid_for((total + 3) / 4, threads, sms), threads, 0, st>>>(d_stage, bt, total);
+    k_linear<4><<<grid_of(k_linear<4>, (total + 3) / 4, threads, sms, cfg), threads, 0, st>>>(
+        d_stage, bt, total);
     return cudaGetLastError();
   }
   const bool vec = inner >= 4;
@@ -966,7 +1043,6 @@ cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
   while (l < 32 && (int64_t(1) << l) < nvec) ++l;
   const uint32_t mul =
       (uint32_t)((((uint64_t(1) << 32) * ((uint64_t(1) << l) - (uint64_t)nvec)) / (uint64_t)nvec) + 1);
-  const int grid = grid_for(work, threads, sms);
   // pooling-shaped reductions: one operand, unit-stride innermost window
   const LtbLoad& L0 = h.loads[0];
   if (vec && h.small && h.nout >= 1 && h.ndim > h.nout && h.nload == 1 && h.ninstr == 2 &&
@@ -975,63 +1051,139 @@ cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
       h.red_total / h.size[h.ndim - 1] <= 64 && h.red_op != LTB_R_SUB && h.red_op != LTB_R_DIV &&
       !h.kahan) {
     const int64_t s = L0.coef[h.nout - 1], k = h.size[h.ndim - 1];
-#define LTB_WIN(SS, KK)                                                      \
-  if (s == SS && k == KK) {                                                  \
-    k_window<SS, KK><<<grid, threads, 0, st>>>(d_stage, bt, mul, l);         \
-    return cudaGetLastError();                                               \
+#define LTB_WIN(SS, KK)                                                             \
+  if (s == SS && k == KK) {                                                         \
+    k_window<SS, KK><<<grid_of(k_window<SS, KK>, work, threads, sms, cfg), threads, 0, \
+                       st>>>(d_stage, bt, mul, l);                                  \
+    return cudaGetLastError();                                                      \
   }
     LTB_WIN(2, 2) LTB_WIN(1, 2) LTB_WIN(1, 3) LTB_WIN(2, 3) LTB_WIN(3, 3) LTB_WIN(1, 1)
     LTB_WIN(2, 1)
 #undef LTB_WIN
   }
   if (vec)
-    k_nest<4><<<grid, threads, 0, st>>>(d_stage, bt, mul, l);
+    k_nest<4><<<grid_of(k_nest<4>, work, threads, sms, cfg), threads, 0, st>>>(d_stage, bt, mul,
+                                                                                l);
   else
-    k_nest<1><<<grid, threads, 0, st>>>(d_stage, bt, mul, l);
+    k_nest<1><<<grid_of(k_nest<1>, work, threads, sms, cfg), threads, 0, st>>>(d_stage, bt, mul,
+                                                                                l);
   return cudaGetLastError();
 }
 
 cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,
                               const LtbBufTable& bt, int splits, int sms,
-                              cudaStream_t st) {
+                              cudaStream_t st, const LtbCfg& cfg) {
   int64_t outs = 1;
   for (int k = 0; k < h.nout; ++k) outs *= h.size[k];
-  const int threads = h.red_total >= 256 ? 256 : 128;
-  int64_t gx = outs < (int64_t)sms * 64 ? outs : (int64_t)sms * 64;
+  const int threads = pick_threads(cfg, h.red_total >= 256 ? 256 : 128, 256);
+  // one CTA per output, up to a cap of CTAs per SM (block-stride over outputs)
+  const int64_t per_sm = cfg.cta_per_sm > 0 ? cfg.cta_per_sm : 64;
+  int64_t gx = outs < (int64_t)sms * per_sm ? outs : (int64_t)sms * per_sm;
   if (gx < 1) gx = 1;
   dim3 grid((unsigned)gx, (unsigned)splits);
   k_reduce_par<<<grid, threads, 0, st>>>(d_stage, bt, outs);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || splits == 1) return e;
-  k_reduce_combine<<<grid_for(outs, 256, sms), 256, 0, st>>>(d_stage, bt, outs,
-                                                             splits);
+  k_reduce_combine<<<grid_of(k_reduce_combine, outs, 256, sms, LtbCfg{0, 0, 0}), 256, 0, st>>>(
+      d_stage, bt, outs, splits);
   return cudaGetLastError();
 }
 
-cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, int nsteps,
-                                 const LtbStage& final_stage,
-                                 const LtbBufTable& bt, int sms,
-                                 cudaStream_t st) {
+// Row-softmax schedules: (elements per thread, threads) pairs covering the
+// row; variant v (1-based) indexes this table.
+static const int kSmxVariants[][2] = {{4, 128},  {4, 256},  {8, 256},  {16, 256},
+                                      {32, 256}, {8, 128},  {16, 128}, {32, 128},
+                                      {4, 512},  {8, 512},  {16, 512}};
+constexpr int kNumSmx = sizeof(kSmxVariants) / sizeof(kSmxVariants[0]);
+
+static bool softmax_chain(const LtbStage* const* h_stages, int nsteps) {
+  const LtbStage& f = *h_stages[nsteps - 1];
+  return f.pattern == LTB_P_SOFTMAX && nsteps == 3 && f.size[f.nout - 1] <= 256 * 32;
+}
+
+// heuristic variant: the smallest EPT x 256 that covers the row
+static int softmax_default(int64_t inner) {
+  if (inner <= 128 * 4) return 1;
+  if (inner <= 256 * 4) return 2;
+  if (inner <= 256 * 8) return 3;
+  if (inner <= 256 * 16) return 4;
+  return 5;
+}
+
+static bool softmax_fits(int v, int64_t inner) {
+  const int e = kSmxVariants[v - 1][0], t = kSmxVariants[v - 1][1];
+  return (int64_t)e * t >= inner && ((int64_t)e * t <= 2 * inner || e == 4);
+}
+
+int ltb_row_chain_candidates(const LtbStage* const* h_stages, int nsteps, LtbCfg* out, int cap) {
+  int n = 0;
+  if (softmax_chain(h_stages, nsteps)) {
+    const LtbStage& f = *h_stages[nsteps - 1];
+    const int64_t inner = f.size[f.nout - 1];
+    for (int v = 1; v <= kNumSmx; ++v)
+      if (softmax_fits(v, inner))
+        for (int w : {0, 2, 4, 8})
+          if (n < cap) out[n++] = LtbCfg{w, 0, v};
+    return n;
+  }
+  for (int w : {0, 2, 4, 8, 16})
+    for (int t : {128, 256, 512})
+      if (n < cap) out[n++] = LtbCfg{w, t, 0};
+  return n;
+}
+
+cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, const LtbStage* const* h_stages,
+                                 int nsteps, const LtbBufTable& bt, int sms,
+                                 cudaStream_t st, const LtbCfg& cfg) {
   if (nsteps > kMaxChain) return cudaErrorInvalidValue;
+  const LtbStage& final_stage = *h_stages[nsteps - 1];
   int64_t rows = 1;
   for (int k = 0; k < final_stage.nout - 1; ++k) rows *= final_stage.size[k];
   const int64_t inner = final_stage.size[final_stage.nout - 1];
-  if (final_stage.pattern == LTB_P_SOFTMAX && nsteps == 3 && inner <= 256 * 32) {
-    const unsigned grid = (unsigned)(rows < (int64_t)sms * 64 ? rows : (int64_t)sms * 64);
-    if (inner <= 128 * 4)
-      k_row_softmax<4, 128><<<grid, 128, 0, st>>>(d_stages, bt, rows);
-    else if (inner <= 256 * 4)
-      k_row_softmax<4, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
-    else if (inner <= 256 * 8)
-      k_row_softmax<8, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
-    else if (inner <= 256 * 16)
-      k_row_softmax<16, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
-    else
-      k_row_softmax<32, 256><<<grid, 256, 0, st>>>(d_stages, bt, rows);
-    return cudaGetLastError();
+  if (softmax_chain(h_stages, nsteps)) {
+    const LtbStage& A = *h_stages[0];  // max over n
+    const LtbStage& B = *h_stages[1];  // sum over n
+    const LtbStage& C = final_stage;   // elementwise output
+    const LtbLoad& X = A.loads[A.code[0].arg];
+    SoftmaxRows P{};
+    P.x = bt.p[X.buf];
+    P.y = bt.p[C.out_buf];
+    P.m = bt.p[A.out_buf];
+    P.s = bt.p[B.out_buf];
+    P.xoff = X.off;
+    P.yoff = C.out_off;
+    P.moff = A.out_off;
+    P.soff = B.out_off;
+    P.n = inner;
+    P.rows = rows;
+    P.nd = C.nout - 1;
+    for (int k = 0; k < P.nd; ++k) {
+      P.size[k] = C.size[k];
+      P.xc[k] = X.coef[k];
+      P.yc[k] = C.out_coef[k];
+      P.mc[k] = A.out_coef[k];
+      P.sc[k] = B.out_coef[k];
+    }
+    int v = cfg.variant;
+    if (v < 1 || v > kNumSmx || !softmax_fits(v, inner)) v = softmax_default(inner);
+    switch (v) {
+#define LTB_SMX(V, EPT, NT)                                                            \
+  case V: {                                                                            \
+    const int g = grid_of(k_softmax_rows<EPT, NT>, rows * NT, NT, sms, cfg);           \
+    k_softmax_rows<EPT, NT><<<g, NT, 0, st>>>(P);                                      \
+    return cudaGetLastError();                                                         \
   }
-  const int threads = inner >= 4096 ? 512 : (inner >= 1024 ? 256 : 128);
-  int64_t grid = rows < (int64_t)sms * 8 ? rows : (int64_t)sms * 8;
+      LTB_SMX(1, 4, 128) LTB_SMX(2, 4, 256) LTB_SMX(3, 8, 256) LTB_SMX(4, 16, 256)
+      LTB_SMX(5, 32, 256) LTB_SMX(6, 8, 128) LTB_SMX(7, 16, 128) LTB_SMX(8, 32, 128)
+      LTB_SMX(9, 4, 512) LTB_SMX(10, 8, 512) LTB_SMX(11, 16, 512)
+#undef LTB_SMX
+    }
+    return cudaErrorInvalidValue;
+  }
+  const int threads =
+      pick_threads(cfg, inner >= 4096 ? 512 : (inner >= 1024 ? 256 : 128), 512);
+  const int64_t per_sm = cfg.cta_per_sm > 0 ? cfg.cta_per_sm : 8;
+  int64_t grid = rows < (int64_t)sms * per_sm ? rows : (int64_t)sms * per_sm;
   if (grid < 1) grid = 1;
   k_row_chain<<<(unsigned)grid, threads, 0, st>>>(d_stages, nsteps, bt, rows);
   return cudaGetLastError();

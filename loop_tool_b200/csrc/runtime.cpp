@@ -4,6 +4,9 @@
 
 #include <algorithm>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <sstream>
@@ -82,7 +85,16 @@ struct GemmTables {
   int a_slot = -1, b_slot = -1;       // scratch slots of the packed operands
   LtbTcProblem prob{};                // launch template (maps/c bound per run)
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
+  int bn = 256;                       // tensor-core tile width (128 or 256)
 };
+
+// Tile width of a tensor-core contraction: output tiles are 128 x bn.
+void set_tile_n(GemmTables& t, int bn) {
+  t.bn = bn;
+  const int64_t tn = (t.prob.N + bn - 1) / bn;
+  t.prob.tiles_n = (int)tn;
+  t.tiles = (int64_t)t.prob.tiles_m * tn;
+}
 
 // All of a compiled object's constant device data (stage descriptors,
 // contraction offset tables, the timeout flag) in one allocation and one
@@ -142,6 +154,9 @@ struct ltb_compiled {
   int* d_err = nullptr;               // device-side timeout flag
   int64_t bandwidth_gbs = 0;
   int launches = 0;
+  std::vector<LtbCfg> cfg;            // per stage launch schedule (autotuner)
+  uint64_t key = 0;                   // IR-text + options hash (schedule cache key)
+  bool tuned = false;                 // schedules came from the tuner / cache
 };
 
 namespace {
@@ -224,13 +239,22 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
       if (v[i] - v[i - 1] != *step) return false;
     return true;
   };
+  // packing orientation: the direction (k or rows) whose neighbouring
+  // offsets are most often adjacent in memory gets the warp's lanes, e.g.
+  // rows (output pixels) for an im2col operand, k for a row-major A
+  auto unit_frac = [](const std::vector<int64_t>& v) {
+    if (v.size() < 2) return 1.0;
+    size_t u = 0;
+    for (size_t i = 1; i < v.size(); ++i) u += v[i] - v[i - 1] == 1;
+    return (double)u / (double)(v.size() - 1);
+  };
   {
     auto ra = table(md, A.coef, A.off), rb = table(nd, B.coef, B.off);
     t.a_dense = A.ng == 0 && ra[0] == 0 && arith(ra, &t.a_ldr) && arith(ktab_a, &t.a_ldk);
     t.b_dense = B.ng == 0 && rb[0] == 0 && arith(rb, &t.b_ldr) && arith(ktab_b, &t.b_ldk);
+    t.a_kcontig = unit_frac(ktab_a) >= unit_frac(ra);
+    t.b_kcontig = unit_frac(ktab_b) >= unit_frac(rb);
   }
-  t.a_kcontig = ktab_a.size() < 2 || ktab_a[1] - ktab_a[0] == 1;
-  t.b_kcontig = ktab_b.size() < 2 || ktab_b[1] - ktab_b[0] == 1;
   auto ctab = table(nd, d.out_coef, 0);
   t.unit_cols = true;
   for (size_t j = 0; j < ctab.size(); ++j) t.unit_cols = t.unit_cols && ctab[j] == (int64_t)j;
@@ -253,8 +277,6 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     t.b_slot = P.num_slots();
     P.scratch_elems.push_back((con.N * t.Kp + 1) / 2);
     const int tm = (int)((con.M + ltb_tc_tile_m() - 1) / ltb_tc_tile_m());
-    const int64_t tn = (con.N + ltb_tc_tile_n() - 1) / ltb_tc_tile_n();
-    t.tiles = tm * tn;
     LtbTcProblem& e = t.prob;
     e.map_a = e.map_b = nullptr;
     e.c = nullptr;
@@ -266,8 +288,9 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     e.M = (int)con.M;
     e.N = (int)con.N;
     e.tiles_m = tm;
-    e.tiles_n = (int)tn;
     e.unit_cols = t.unit_cols ? 1 : 0;
+    // narrow outputs take 128-wide tiles (no half-empty MMA), the rest 256
+    set_tile_n(t, con.N <= 128 ? 128 : 256);
   }
 }
 
@@ -342,6 +365,10 @@ void compile_device(ltb_compiled* c) {
     }
   }
   c->launches = launches;
+  c->cfg.assign(ns, LtbCfg{0, 0, 0});
+  for (int i = 0; i < ns; ++i)
+    if (c->gemm_of[i] >= 0 && c->gemms[c->gemm_of[i]].tc)
+      c->cfg[i].variant = c->gemms[c->gemm_of[i]].bn;
 }
 
 bool is_device_accessible(const void* p) {
@@ -353,74 +380,97 @@ bool is_device_accessible(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
+// Launches of stage i (nothing for a row-chain member that is not the
+// chain's first stage: the chain launches as one kernel).
+cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStream_t st) {
   auto& P = c->plan;
   const int ns = (int)P.stages.size();
-  for (int i = 0; i < ns; ++i) {
-    const auto& s = P.stages[i];
-    const LtbStage* d = c->d_stages + i;
-    cudaError_t e = cudaSuccess;
-    switch (s.family) {
-      case ltb::Family::elementwise:
-      case ltb::Family::reduce_serial:
-        e = ltb_launch_nest(d, s.dev, bt, c->sms, st);
-        break;
-      case ltb::Family::reduce_parallel:
-      case ltb::Family::reduce_split:
-        e = ltb_launch_reduce(d, s.dev, bt, c->split_of[i], c->sms, st);
-        break;
-      case ltb::Family::row_chain: {
-        if (s.rows_from != i) break;
-        int n = 0;
-        while (i + n < ns && P.stages[i + n].family == ltb::Family::row_chain &&
-               P.stages[i + n].rows_from == i)
-          n++;
-        e = ltb_launch_row_chain(d, n, P.stages[i + n - 1].dev, bt, c->sms, st);
-        break;
-      }
-      case ltb::Family::contraction: {
-        const GemmTables& t = c->gemms[c->gemm_of[i]];
-        for (int64_t b = 0; b < t.nbatch && e == cudaSuccess; ++b) {
-          LtbGemmProblem p{};
-          const LtbLoad& A = s.dev.loads[s.con.a_load];
-          const LtbLoad& B = s.dev.loads[s.con.b_load];
-          p.a = {bt.p[A.buf] + t.a_boff[b], t.a_row, t.a_k, t.a_dense ? 1 : 0, t.a_ldr, t.a_ldk,
-                 t.a_ng, t.ag_row, t.ag_k, t.ag_ub};
-          p.b = {bt.p[B.buf] + t.b_boff[b], t.b_row, t.b_k, t.b_dense ? 1 : 0, t.b_ldr, t.b_ldk,
-                 t.b_ng, t.bg_row, t.bg_k, t.bg_ub};
-          p.c = bt.p[s.dev.out_buf] + t.c_boff[b];
-          p.crow = t.c_row;
-          p.ccol = t.c_col;
-          p.M = s.con.M;
-          p.N = s.con.N;
-          p.K = s.con.K;
-          if (!t.tc) {
-            e = ltb_launch_gemm_simt(p, c->sms, st);
-            continue;
-          }
-          void* ap = bt.p[t.a_slot];
-          void* bp = bt.p[t.b_slot];
-          e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, st);
-          if (e == cudaSuccess)
-            e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, st);
-          alignas(64) unsigned char maps[256];
-          if (e == cudaSuccess) e = ltb_make_tmap(maps, ap, p.M, t.Kp, ltb_tc_tile_m());
-          if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, ltb_tc_tile_n());
-          if (e == cudaSuccess) {
-            LtbTcProblem one = t.prob;
-            one.c = p.c;
-            one.crow = t.c_row;
-            one.ccol = t.c_col;
-            e = ltb_launch_gemm_tc(nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st, &one,
-                                   maps, maps + 128);
-          }
-        }
-        break;
-      }
+  const auto& s = P.stages[i];
+  const LtbStage* d = c->d_stages + i;
+  const LtbCfg& cfg = c->cfg[i];
+  cudaError_t e = cudaSuccess;
+  switch (s.family) {
+    case ltb::Family::elementwise:
+    case ltb::Family::reduce_serial:
+      e = ltb_launch_nest(d, s.dev, bt, c->sms, st, cfg);
+      break;
+    case ltb::Family::reduce_parallel:
+    case ltb::Family::reduce_split:
+      e = ltb_launch_reduce(d, s.dev, bt, c->split_of[i], c->sms, st, cfg);
+      break;
+    case ltb::Family::row_chain: {
+      if (s.rows_from != i) break;
+      int n = 0;
+      while (i + n < ns && P.stages[i + n].family == ltb::Family::row_chain &&
+             P.stages[i + n].rows_from == i)
+        n++;
+      const LtbStage* hs[16];
+      for (int k = 0; k < n && k < 16; ++k) hs[k] = &P.stages[i + k].dev;
+      e = n <= 16 ? ltb_launch_row_chain(d, hs, n, bt, c->sms, st, cfg) : cudaErrorInvalidValue;
+      break;
     }
+    case ltb::Family::contraction: {
+      const GemmTables& t = c->gemms[c->gemm_of[i]];
+      for (int64_t b = 0; b < t.nbatch && e == cudaSuccess; ++b) {
+        LtbGemmProblem p{};
+        const LtbLoad& A = s.dev.loads[s.con.a_load];
+        const LtbLoad& B = s.dev.loads[s.con.b_load];
+        p.a = {bt.p[A.buf] + t.a_boff[b], t.a_row, t.a_k, t.a_dense ? 1 : 0, t.a_ldr, t.a_ldk,
+               t.a_ng, t.ag_row, t.ag_k, t.ag_ub};
+        p.b = {bt.p[B.buf] + t.b_boff[b], t.b_row, t.b_k, t.b_dense ? 1 : 0, t.b_ldr, t.b_ldk,
+               t.b_ng, t.bg_row, t.bg_k, t.bg_ub};
+        p.c = bt.p[s.dev.out_buf] + t.c_boff[b];
+        p.crow = t.c_row;
+        p.ccol = t.c_col;
+        p.M = s.con.M;
+        p.N = s.con.N;
+        p.K = s.con.K;
+        if (!t.tc) {
+          e = ltb_launch_gemm_simt(p, c->sms, st);
+          continue;
+        }
+        void* ap = bt.p[t.a_slot];
+        void* bp = bt.p[t.b_slot];
+        e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, c->sms, st);
+        if (e == cudaSuccess)
+          e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, c->sms, st);
+        alignas(64) unsigned char maps[256];
+        if (e == cudaSuccess) e = ltb_make_tmap(maps, ap, p.M, t.Kp, ltb_tc_tile_m());
+        if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, t.bn);
+        if (e == cudaSuccess) {
+          LtbTcProblem one = t.prob;
+          one.c = p.c;
+          one.crow = t.c_row;
+          one.ccol = t.c_col;
+          e = ltb_launch_gemm_tc(t.bn, nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st, &one,
+                                 maps, maps + 128);
+        }
+      }
+      break;
+    }
+  }
+  return e;
+}
+
+void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
+  const int ns = (int)c->plan.stages.size();
+  for (int i = 0; i < ns; ++i) {
+    const cudaError_t e = launch_stage(c, i, bt, st);
     if (e != cudaSuccess)
-      throw CudaFailure(std::string("launch of stage ") + std::to_string(i) +
-                        " (" + s.text + "): " + cudaGetErrorString(e));
+      throw CudaFailure(std::string("launch of stage ") + std::to_string(i) + " (" +
+                        c->plan.stages[i].text + "): " + cudaGetErrorString(e));
+  }
+}
+
+// Apply a schedule to stage i (the tile width of a tensor-core contraction
+// changes its tile count).
+void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
+  c->cfg[i] = cfg;
+  const int g = c->gemm_of[i];
+  if (g >= 0 && c->gemms[g].tc) {
+    const int bn = cfg.variant == 128 ? 128 : 256;
+    set_tile_n(c->gemms[g], bn);
+    c->cfg[i].variant = bn;
   }
 }
 
@@ -501,6 +551,143 @@ int copy_out(const std::string& s, char* buf, size_t len) {
   return LTB_OK;
 }
 
+// ------------------------------------------------------------- schedules
+// Autotuned launch schedules, cached per process by a hash of the IR text
+// (which carries every size, so structure and shape together) and the
+// compile options, and persisted as text that keeps the IR itself (a
+// portable record: the serialized loop tree plus its schedule).
+struct TuneEntry {
+  std::string ir, opts;
+  int sms = 0;
+  std::vector<LtbCfg> cfg;
+  std::vector<double> us;
+};
+std::mutex g_tune_mu;
+std::map<uint64_t, TuneEntry> g_tune;
+
+std::string canon_options(const ltb::LowerOptions& o) {
+  return "precision=" + std::to_string((int)o.precision) + ";fuse_rows=" +
+         std::to_string((int)o.fuse_rows) + ";tensor_cores=" +
+         std::to_string((int)o.use_tensor_cores) + ";kahan_threshold=" +
+         std::to_string(o.kahan_threshold);
+}
+
+uint64_t fnv1a(const std::string& a, const std::string& b) {
+  uint64_t h = 1469598103934665603ULL;
+  auto mix = [&](const std::string& x) {
+    for (unsigned char ch : x) {
+      h ^= ch;
+      h *= 1099511628211ULL;
+    }
+    h ^= 0x1f;
+    h *= 1099511628211ULL;
+  };
+  mix(a);
+  mix(b);
+  return h;
+}
+
+// The schedule in the vocabulary of LoopTree annotations.
+std::string describe(ltb_compiled* c, int i) {
+  const auto& s = c->plan.stages[i];
+  const LtbCfg& f = c->cfg[i];
+  std::ostringstream o;
+  if (s.family == ltb::Family::contraction) {
+    const auto& t = c->gemms[c->gemm_of[i]];
+    if (t.tc)
+      o << "tile(128x" << t.bn << "x64) tensor_cores(tcgen05) parallel(persistent, "
+        << t.tiles << " tiles)";
+    else
+      o << "tile(128x128) cuda_cores";
+    return o.str();
+  }
+  o << "parallel(grid=SMs x " << (f.cta_per_sm ? std::to_string(f.cta_per_sm) : "resident")
+    << ") threaded(" << (f.threads ? std::to_string(f.threads) : "default") << ")";
+  if (f.variant) o << " variant(" << f.variant << ")";
+  return o.str();
+}
+
+std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
+  auto& P = c->plan;
+  const auto& s = P.stages[i];
+  LtbCfg buf[128];
+  int n = 0;
+  switch (s.family) {
+    case ltb::Family::elementwise:
+    case ltb::Family::reduce_serial:
+      n = ltb_nest_candidates(s.dev, buf, 128);
+      break;
+    case ltb::Family::reduce_parallel:
+    case ltb::Family::reduce_split:
+      n = ltb_reduce_candidates(s.dev, buf, 128);
+      break;
+    case ltb::Family::row_chain: {
+      int m = 0;
+      const LtbStage* hs[16];
+      while (i + m < (int)P.stages.size() && m < 16 &&
+             P.stages[i + m].family == ltb::Family::row_chain && P.stages[i + m].rows_from == i) {
+        hs[m] = &P.stages[i + m].dev;
+        m++;
+      }
+      n = ltb_row_chain_candidates(hs, m, buf, 128);
+      break;
+    }
+    case ltb::Family::contraction:
+      if (c->gemms[c->gemm_of[i]].tc) {
+        buf[n++] = LtbCfg{0, 0, 128};
+        buf[n++] = LtbCfg{0, 0, 256};
+      }
+      break;
+  }
+  return std::vector<LtbCfg>(buf, buf + n);
+}
+
+// Mean device time (microseconds) of stage i's launches over reps runs;
+// infinity if a launch is rejected.
+double time_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStream_t st, int reps,
+                  cudaEvent_t e0, cudaEvent_t e1) {
+  if (launch_stage(c, i, bt, st) != cudaSuccess) {
+    cudaGetLastError();
+    return std::numeric_limits<double>::infinity();
+  }
+  CUDA_TRY(cudaEventRecord(e0, st));
+  for (int r = 0; r < reps; ++r)
+    if (launch_stage(c, i, bt, st) != cudaSuccess) {
+      cudaGetLastError();
+      CUDA_TRY(cudaStreamSynchronize(st));
+      return std::numeric_limits<double>::infinity();
+    }
+  CUDA_TRY(cudaEventRecord(e1, st));
+  CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  return 1e3 * ms / reps;
+}
+
+void record_schedule(ltb_compiled* c, const std::vector<double>& us) {
+  TuneEntry e;
+  e.ir = c->ir_text;
+  e.opts = canon_options(c->opt);
+  e.sms = c->sms;
+  e.cfg = c->cfg;
+  e.us = us;
+  e.us.resize(e.cfg.size(), 0.0);
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune[c->key] = std::move(e);
+}
+
+// Schedules from the cache, if this IR + options were tuned before.
+void lookup_schedule(ltb_compiled* c) {
+  c->key = fnv1a(c->ir_text, canon_options(c->opt));
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  auto it = g_tune.find(c->key);
+  if (it == g_tune.end()) return;
+  const TuneEntry& e = it->second;
+  if (e.ir != c->ir_text || e.sms != c->sms || e.cfg.size() != c->cfg.size()) return;
+  for (size_t i = 0; i < e.cfg.size(); ++i) apply_cfg(c, (int)i, e.cfg[i]);
+  c->tuned = true;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ batch
@@ -515,8 +702,11 @@ struct ltb_batch {
   LtbPackJob* d_jobs = nullptr;
   int njobs = 0;
   int64_t pack_tiles = 0;
-  LtbTcProblem* d_tc = nullptr;
-  int64_t tc_tiles = 0;
+  // tensor-core problems grouped by tile width (group 0: 128, group 1: 256),
+  // one persistent launch per non-empty group
+  LtbTcProblem* d_tc[2] = {nullptr, nullptr};
+  int ntc[2] = {0, 0};
+  int64_t tc_tiles[2] = {0, 0};
   LtbGemmProblem* d_simt = nullptr;
   int64_t* d_simt_start = nullptr;
   int64_t simt_tiles = 0;
@@ -529,10 +719,17 @@ struct ltb_batch {
 
 namespace {
 
+void batch_gemms(ltb_batch* b, cudaStream_t st) {
+  for (int g = 0; g < 2; ++g)
+    if (b->ntc[g])
+      CUDA_TRY(ltb_launch_gemm_tc(g ? 256 : 128, b->d_tc[g], b->ntc[g], b->tc_tiles[g], nullptr,
+                                  b->sms, b->d_err, st));
+}
+
 void batch_launch(ltb_batch* b, cudaStream_t st) {
   if (b->tc) {
     CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st));
-    CUDA_TRY(ltb_launch_gemm_tc(b->d_tc, b->n, b->tc_tiles, nullptr, b->sms, b->d_err, st));
+    batch_gemms(b, st);
   } else {
     CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles, st));
   }
@@ -566,8 +763,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->device = cs[0]->device;
     b->sms = cs[0]->sms;
     std::vector<LtbPackJob> jobs;
-    std::vector<LtbTcProblem> tcp;
-    std::vector<unsigned char> maps;  // two 128-byte CUtensorMaps per problem
+    std::vector<LtbTcProblem> tcp[2];
+    std::vector<unsigned char> maps[2];  // two 128-byte CUtensorMaps per problem
     std::vector<LtbGemmProblem> sp;
     std::vector<int64_t> sstart;
     for (int i = 0; i < n; ++i) {
@@ -609,12 +806,12 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
           j.rows = rows;
           j.K = p.K;
           j.Kp = t.Kp;
-          j.tiles_k = (int)((p.K + 31) / 32);
+          j.tiles_k = (int)((p.K + 63) / 64);
           j.tile_start = b->pack_tiles;
           j.nseg = t.nseg;
           j.seg_mask = mask;
-          j.k_contig = kc ? 1 : 0;
-          b->pack_tiles += ((rows + 31) / 32) * j.tiles_k;
+          j.mode = ltb_pack_mode(op, rows, p.K, kc ? 1 : 0);
+          b->pack_tiles += ltb_pack_tiles(rows, p.K);
           jobs.push_back(j);
         };
         void *ap = nullptr, *bp = nullptr;
@@ -624,17 +821,19 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         b->owned.push_back(bp);
         job(p.a, p.M, ap, t.a_mask, t.a_kcontig);
         job(p.b, p.N, bp, t.b_mask, t.b_kcontig);
-        maps.resize(maps.size() + 256);
-        unsigned char* m = maps.data() + maps.size() - 256;
+        const int grp = t.bn == 128 ? 0 : 1;
+        auto& mv = maps[grp];
+        mv.resize(mv.size() + 256);
+        unsigned char* m = mv.data() + mv.size() - 256;
         CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
-        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, ltb_tc_tile_n()));
+        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, t.bn));
         LtbTcProblem q = t.prob;
         q.c = p.c;
         q.crow = t.c_row;
         q.ccol = t.c_col;
-        q.tile_start = b->tc_tiles;
-        b->tc_tiles += t.tiles;
-        tcp.push_back(q);
+        q.tile_start = b->tc_tiles[grp];
+        b->tc_tiles[grp] += t.tiles;
+        tcp[grp].push_back(q);
       } else {
         sstart.push_back(b->simt_tiles);
         b->simt_tiles += ((p.M + 127) / 128) * ((p.N + 127) / 128);
@@ -644,13 +843,16 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->njobs = (int)jobs.size();
     if (b->tc) {
       b->d_jobs = upload(jobs, b->owned);
-      // tensor maps in device memory (cudaMalloc is 256-byte aligned)
-      unsigned char* d_maps = upload(maps, b->owned);
-      for (size_t i = 0; i < tcp.size(); ++i) {
-        tcp[i].map_a = d_maps + 256 * i;
-        tcp[i].map_b = d_maps + 256 * i + 128;
+      for (int g = 0; g < 2; ++g) {
+        // tensor maps in device memory (cudaMalloc is 256-byte aligned)
+        unsigned char* d_maps = upload(maps[g], b->owned);
+        for (size_t i = 0; i < tcp[g].size(); ++i) {
+          tcp[g][i].map_a = d_maps + 256 * i;
+          tcp[g][i].map_b = d_maps + 256 * i + 128;
+        }
+        b->ntc[g] = (int)tcp[g].size();
+        b->d_tc[g] = upload(tcp[g], b->owned);
       }
-      b->d_tc = upload(tcp, b->owned);
     } else {
       b->d_simt = upload(sp, b->owned);
       b->d_simt_start = upload(sstart, b->owned);
@@ -728,7 +930,7 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
     if (b->tc) CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st));
     CUDA_TRY(cudaEventRecord(e1, st));
     if (b->tc)
-      CUDA_TRY(ltb_launch_gemm_tc(b->d_tc, b->n, b->tc_tiles, nullptr, b->sms, b->d_err, st));
+      batch_gemms(b, st);
     else
       CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles, st));
     CUDA_TRY(cudaEventRecord(e2, st));
@@ -752,8 +954,10 @@ int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   std::string k = name;
   if (k == "problems") *value = b->n;
   else if (k == "flops") *value = (int64_t)b->flops;
-  else if (k == "launches") *value = b->tc ? 2 : 1;
-  else if (k == "tiles") *value = b->tc ? b->tc_tiles : b->simt_tiles;
+  else if (k == "launches") *value = b->tc ? 1 + (b->ntc[0] > 0) + (b->ntc[1] > 0) : 1;
+  else if (k == "tiles") *value = b->tc ? b->tc_tiles[0] + b->tc_tiles[1] : b->simt_tiles;
+  else if (k == "tiles_128") *value = b->tc_tiles[0];
+  else if (k == "tiles_256") *value = b->tc_tiles[1];
   else if (k == "graph") *value = b->exec ? 1 : 0;
   else return fail(LTB_ERR_INVALID, "unknown property " + k);
   return LTB_OK;
@@ -817,6 +1021,7 @@ int ltb_compile(const char* ir_text, const char* options, ltb_compiled** out) {
   }
   try {
     compile_device(c);
+    lookup_schedule(c);
   } catch (const std::exception& e) {
     for (void* p : c->owned) cudaFree(p);
     delete c;
@@ -860,6 +1065,7 @@ int ltb_int_property(ltb_compiled* c, const char* name, int64_t* value) {
   else if (k == "outputs") *value = c->plan.n_out;
   else if (k == "algorithmic_bytes") *value = c->plan.algorithmic_bytes;
   else if (k == "flops") *value = (int64_t)c->plan.flops;
+  else if (k == "tuned") *value = c->tuned ? 1 : 0;
   else return fail(LTB_ERR_INVALID, "unknown property " + k);
   return LTB_OK;
 }
@@ -889,6 +1095,192 @@ int ltb_free(void* ptr) {
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(LTB_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return LTB_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps, char* report,
+             size_t len) {
+  if (!c || !memory) return fail(LTB_ERR_INVALID, "null argument");
+  auto& P = c->plan;
+  if (n != P.n_in + P.n_out)
+    return fail(LTB_ERR_INVALID, "expected " + std::to_string(P.n_in + P.n_out) +
+                                     " buffers, got " + std::to_string(n));
+  if (reps < 1) reps = 1;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::ostringstream rep;
+  try {
+    CUDA_TRY(cudaSetDevice(c->device));
+    LtbBufTable bt{};
+    for (int i = 0; i < n; ++i) {
+      if (!memory[i] || !is_device_accessible(memory[i]))
+        return fail(LTB_ERR_INVALID, "tuning needs device or managed buffers");
+      bt.p[i] = static_cast<float*>(memory[i]);
+    }
+    {
+      std::lock_guard<std::mutex> lock(c->mu);
+      if (!c->scratch && c->scratch_bytes) {
+        CUDA_TRY(cudaMalloc(&c->scratch, c->scratch_bytes));
+        c->owned.push_back(c->scratch);
+      }
+    }
+    for (size_t k = 0; k < P.scratch_elems.size(); ++k)
+      bt.p[P.n_in + P.n_out + k] =
+          reinterpret_cast<float*>(static_cast<char*>(c->scratch) + c->scratch_off[k]);
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    launch_plan(c, bt, st);  // every stage's inputs in place
+    CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<double> best_us(P.stages.size(), 0.0);
+    for (int i = 0; i < (int)P.stages.size(); ++i) {
+      const auto& s = P.stages[i];
+      if (s.family == ltb::Family::row_chain && s.rows_from != i) continue;
+      auto cands = candidates(c, i);
+      const LtbCfg start = c->cfg[i];
+      const double t0 = time_stage(c, i, bt, st, reps, e0, e1);
+      LtbCfg best = start;
+      double bt_us = t0;
+      for (const auto& cand : cands) {
+        apply_cfg(c, i, cand);
+        const double t = time_stage(c, i, bt, st, reps, e0, e1);
+        if (t < bt_us) {
+          bt_us = t;
+          best = c->cfg[i];
+        }
+      }
+      apply_cfg(c, i, best);
+      best_us[i] = bt_us;
+      rep << "stage " << i << " " << s.text << "\n  " << describe(c, i) << "  "
+          << std::fixed << std::setprecision(2) << bt_us << " us (default " << t0 << " us, "
+          << cands.size() << " candidates)\n";
+    }
+    launch_plan(c, bt, st);  // outputs from the chosen schedules
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int flag = 0;
+    CUDA_TRY(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
+      throw ltb::Error("a bounded wait in a tensor-core kernel gave up while tuning");
+    }
+    c->tuned = true;
+    record_schedule(c, best_us);
+  } catch (const CudaFailure& e) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return fail(LTB_ERR_CUDA, e.what());
+  } catch (const std::exception& e) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return fail(LTB_ERR_INVALID, e.what());
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (report && len) return copy_out(rep.str(), report, len);
+  return LTB_OK;
+}
+
+int ltb_set_schedule(ltb_compiled* c, int stage, int cta_per_sm, int threads, int variant) {
+  if (!c || stage < 0 || stage >= (int)c->cfg.size())
+    return fail(LTB_ERR_INVALID, "bad compiled object or stage index");
+  if (cta_per_sm < 0 || cta_per_sm > 1024 || !(threads == 0 || threads == 64 ||
+                                                threads == 128 || threads == 256 ||
+                                                threads == 512))
+    return fail(LTB_ERR_INVALID, "bad schedule");
+  apply_cfg(c, stage, LtbCfg{cta_per_sm, threads, variant});
+  return LTB_OK;
+}
+
+int ltb_get_schedule(ltb_compiled* c, int stage, int* cta_per_sm, int* threads, int* variant) {
+  if (!c || stage < 0 || stage >= (int)c->cfg.size())
+    return fail(LTB_ERR_INVALID, "bad compiled object or stage index");
+  if (cta_per_sm) *cta_per_sm = c->cfg[stage].cta_per_sm;
+  if (threads) *threads = c->cfg[stage].threads;
+  if (variant) *variant = c->cfg[stage].variant;
+  return LTB_OK;
+}
+
+int ltb_tune_record(ltb_compiled* c) {
+  if (!c) return fail(LTB_ERR_INVALID, "null compiled object");
+  record_schedule(c, {});
+  c->tuned = true;
+  return LTB_OK;
+}
+
+int64_t ltb_tune_entries(void) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  return (int64_t)g_tune.size();
+}
+
+int ltb_tune_clear(void) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune.clear();
+  return LTB_OK;
+}
+
+// Text file: a header line, then per entry
+//   entry <sms> <stages> <ir bytes> <options bytes>\n<ir><options>\n
+//   <cta_per_sm> <threads> <variant> <us>\n   (one line per stage)
+int ltb_tune_save(const char* path) {
+  if (!path) return fail(LTB_ERR_INVALID, "null path");
+  std::ofstream f(path, std::ios::binary | std::ios::trunc);
+  if (!f) return fail(LTB_ERR_INVALID, std::string("cannot write ") + path);
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  f << "loop_tool_b200 schedules 1\n";
+  for (const auto& kv : g_tune) {
+    const TuneEntry& e = kv.second;
+    f << "entry " << e.sms << " " << e.cfg.size() << " " << e.ir.size() << " " << e.opts.size()
+      << "\n";
+    f.write(e.ir.data(), (std::streamsize)e.ir.size());
+    f.write(e.opts.data(), (std::streamsize)e.opts.size());
+    f << "\n";
+    for (size_t i = 0; i < e.cfg.size(); ++i)
+      f << e.cfg[i].cta_per_sm << " " << e.cfg[i].threads << " " << e.cfg[i].variant << " "
+        << (i < e.us.size() ? e.us[i] : 0.0) << "\n";
+  }
+  return f ? LTB_OK : fail(LTB_ERR_INVALID, std::string("write failed: ") + path);
+}
+
+int ltb_tune_load(const char* path) {
+  if (!path) return fail(LTB_ERR_INVALID, "null path");
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(LTB_ERR_INVALID, std::string("cannot read ") + path);
+  std::string line;
+  if (!std::getline(f, line) || line != "loop_tool_b200 schedules 1")
+    return fail(LTB_ERR_INVALID, "not a schedule file");
+  std::vector<TuneEntry> got;
+  while (std::getline(f, line)) {
+    if (line.empty()) continue;
+    std::istringstream h(line);
+    std::string tag;
+    size_t ns = 0, irb = 0, ob = 0;
+    TuneEntry e;
+    if (!(h >> tag >> e.sms >> ns >> irb >> ob) || tag != "entry" || ns > 4096 ||
+        irb > (64u << 20) || ob > 4096)
+      return fail(LTB_ERR_INVALID, "malformed schedule entry");
+    e.ir.resize(irb);
+    e.opts.resize(ob);
+    if (irb) f.read(&e.ir[0], (std::streamsize)irb);
+    if (ob) f.read(&e.opts[0], (std::streamsize)ob);
+    std::getline(f, line);
+    if (!f) return fail(LTB_ERR_INVALID, "truncated schedule entry");
+    for (size_t i = 0; i < ns; ++i) {
+      LtbCfg cfg{};
+      double us = 0;
+      if (!std::getline(f, line)) return fail(LTB_ERR_INVALID, "truncated schedule entry");
+      std::istringstream r(line);
+      if (!(r >> cfg.cta_per_sm >> cfg.threads >> cfg.variant >> us))
+        return fail(LTB_ERR_INVALID, "malformed schedule line");
+      e.cfg.push_back(cfg);
+      e.us.push_back(us);
+    }
+    got.push_back(std::move(e));
+  }
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (auto& e : got) {
+    const uint64_t k = fnv1a(e.ir, e.opts);
+    g_tune[k] = std::move(e);
   }
   return LTB_OK;
 }

@@ -20,15 +20,22 @@ struct LtbTcProblem {
   int unit_cols;         // ccol[j] == j
 };
 
-// One operand packing job of a grouped pack launch (32 x 32 tiles).
+// Load modes of the operand packer (ltb_pack_mode picks one per operand).
+enum { kPackDenseK = 0, kPackDenseR = 1, kPackGatherK = 2, kPackGatherR = 3 };
+
+// One operand packing job: FP32 operand -> BF16 K-major [rows, Kp] in
+// 64-row x 64-k tiles.
 struct LtbPackJob {
   LtbGemmOperand op;
   void* out;            // BF16 [rows, Kp]
   int64_t rows, K, Kp;
-  int64_t tile_start;   // first global tile index of this job
-  int tiles_k;          // ceil(K / 32)
-  int nseg, seg_mask, k_contig;
+  int64_t tile_start;   // first global tile index of this job (grouped launch)
+  int tiles_k;          // ceil(K / 64)
+  int nseg, seg_mask;
+  int mode;             // kPack*
 };
+int ltb_pack_mode(const LtbGemmOperand& op, int64_t rows, int64_t K, int k_contig);
+int64_t ltb_pack_tiles(int64_t rows, int64_t K);
 cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t total_tiles,
                                     int sms, cudaStream_t st);
 
@@ -39,17 +46,17 @@ cudaError_t ltb_make_tmap(void* map, const void* base, int64_t rows, int64_t Kp,
 
 // FP32 operand -> BF16 K-major segments (hi / lo split per segment).
 cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
-                            int64_t Kp, int nseg, int seg_mask, int k_contig, cudaStream_t st);
+                            int64_t Kp, int nseg, int seg_mask, int k_contig, int sms,
+                            cudaStream_t st);
 
 // Persistent grouped launch over every tile of every problem
-// (tiles_m * ceil(N / tile_n) tiles per problem).  c_override, if not null,
-// replaces every problem's output pointer (single-problem launches).
+// (tiles_m * ceil(N / bn) tiles per problem, bn = 128 or 256: the tile
+// width the problems' tiles_n and B tensor maps were made for).
+// c_override, if not null, replaces every problem's output pointer.
 // d_probs == nullptr: a single problem passed by value with its two tensor
 // maps (host copies, passed as kernel parameters).
-cudaError_t ltb_launch_gemm_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
-                               float* c_override, int sms, int* err, cudaStream_t st,
-                               const LtbTcProblem* single = nullptr,
+cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
+                               int64_t total_tiles, float* c_override, int sms, int* err,
+                               cudaStream_t st, const LtbTcProblem* single = nullptr,
                                const void* map_a = nullptr, const void* map_b = nullptr);
 int ltb_tc_tile_m();
-int ltb_tc_tile_n();
-size_t ltb_tc_smem_bytes();

@@ -695,7 +695,7 @@ def _resolve_sizes(t, sizes):
 
 # ------------------------------------------------------------ kernel cache
 _CACHE = OrderedDict()
-_CACHE_MAX = 512
+_CACHE_MAX = 4096
 
 
 def compiled(ir_text, **opts):
@@ -715,6 +715,14 @@ def compiled(ir_text, **opts):
 
 def cache_info():
     return {"entries": len(_CACHE), "max": _CACHE_MAX}
+
+
+def set_cache_limit(n):
+    """Most compiled loop trees kept (least recently used evicted first)."""
+    global _CACHE_MAX
+    _CACHE_MAX = max(1, int(n))
+    while len(_CACHE) > _CACHE_MAX:
+        _CACHE.popitem(last=False)
 
 
 def clear_cache():

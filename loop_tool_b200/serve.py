@@ -90,9 +90,21 @@ def _program(kind, params):
     return e / e.sum(n)
 
 
+_ALIGN = 64  # floats (256 bytes) between the regions of a slot workspace
+
+
+def _up(n):
+    return (n + _ALIGN - 1) // _ALIGN * _ALIGN
+
+
 class Server:
     """slots: concurrent requests (one CUDA stream each); hbm_budget: bytes of
-    request buffers admitted at once; precision: contraction mode."""
+    request buffers admitted at once; precision: contraction mode.
+
+    Each slot owns one device workspace (grown on demand, never per request)
+    that holds its request's inputs, output and run scratch, so the steady
+    state makes no allocator calls; a slot that must grow first releases the
+    workspaces of idle slots when the sum would pass the budget."""
 
     def __init__(self, slots=8, hbm_budget=16 << 30, precision="bf16x3", device=0,
                  keep_outputs=False):
@@ -101,6 +113,9 @@ class Server:
         self.torch = torch
         self.dev = torch.device("cuda", device)
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(slots)]
+        self.gens = [torch.Generator(device=self.dev) for _ in range(slots)]
+        self.events = [torch.cuda.Event() for _ in range(slots)]
+        self.ws = [None] * slots
         self.free = list(range(slots))
         self.budget = hbm_budget
         self.used = 0
@@ -120,36 +135,50 @@ class Server:
         self.compiles += lt.cache_info()["entries"] > before
         return c
 
-    def _inputs(self, req, c, gen):
+    def _workspace(self, slot, floats):
         torch = self.torch
-        ins = []
-        for i, n in enumerate(c.io_sizes[:c.n_inputs]):
-            x = torch.randn(n, device=self.dev, generator=gen)
-            if req.kind == "matmul":
-                x /= math.sqrt(req.params[1])  # N(0,1)/sqrt(K)
-            elif req.kind == "conv" and i == 1:
-                x *= math.sqrt(6.0 / 576) / math.sqrt(3.0)  # Kaiming-uniform scale
-            elif req.kind == "softmax":
-                x *= 4.0
-            ins.append(x)
-        return ins
+        ws = self.ws[slot]
+        if ws is not None and ws.numel() >= floats:
+            return ws
+        want = max(floats, int(1.25 * ws.numel()) if ws is not None else 0)
+        held = sum(w.numel() for w in self.ws if w is not None) - (ws.numel() if ws is not None else 0)
+        if 4 * (held + want) > self.budget:
+            for s in self.free:
+                if s != slot:
+                    self.ws[s] = None
+            want = floats
+        self.ws[slot] = None
+        self.ws[slot] = torch.empty(want, device=self.dev)
+        return self.ws[slot]
 
     def _launch(self, req, slot, now):
         torch = self.torch
         c = self._compiled(req)
         st = self.streams[slot]
+        sizes = c.io_sizes
+        sb = (c.int_property("scratch_bytes") + 3) // 4
+        offs, o = [], 0
+        for n in sizes:
+            offs.append(o)
+            o += _up(n)
         with torch.cuda.stream(st):
-            gen = torch.Generator(device=self.dev)
+            ws = self._workspace(slot, o + _up(sb))
+            gen = self.gens[slot]
             gen.manual_seed(req.seed)
-            ins = self._inputs(req, c, gen)
-            out = torch.empty(c.io_sizes[-1], device=self.dev)
-            sb = c.int_property("scratch_bytes")
-            scratch = torch.empty(max(sb // 4, 1), device=self.dev) if sb else None
-            c.run(ins + [out], sync=False, stream=st.cuda_stream,
-                  scratch=scratch.data_ptr() if scratch is not None else None)
-            ev = torch.cuda.Event()
+            views = [ws[a:a + n] for a, n in zip(offs, sizes)]
+            for i, x in enumerate(views[:c.n_inputs]):
+                torch.randn(x.numel(), generator=gen, device=self.dev, out=x)
+                if req.kind == "matmul":
+                    x /= math.sqrt(req.params[1])  # N(0,1)/sqrt(K)
+                elif req.kind == "conv" and i == 1:
+                    x *= math.sqrt(6.0 / 576) / math.sqrt(3.0)  # Kaiming-uniform scale
+                elif req.kind == "softmax":
+                    x *= 4.0
+            c.run(views, sync=False, stream=st.cuda_stream,
+                  scratch=ws[o:].data_ptr() if sb else None)
+            ev = self.events[slot]
             ev.record(st)
-        req.event, req.hold, req.admitted = ev, (ins, out, scratch), now
+        req.event, req.hold, req.admitted = ev, views[-1], now
 
     def bytes_of(self, req):
         c = self._compiled(req)
@@ -177,7 +206,7 @@ class Server:
                 if r.event.query():
                     r.done = time.perf_counter() - t0
                     if self.keep:
-                        r.out = r.hold[1].cpu().numpy()
+                        r.out = r.hold.cpu().numpy()
                     r.hold = None
                     self.used -= r.bytes
                     self.free.append(slot)

@@ -70,3 +70,38 @@ def test_mm_2048_sampled(precision, cuda_dev):
     err = normwise(got[rows, cols], exact)
     tol = dict(TOL, fp32=1e-6)[precision]
     assert err <= tol, f"{precision}: sampled normwise error {err:.3g}"
+
+
+# Operand-packing layouts: k-contiguous A with K % 8 == 4 (half-vector tail),
+# row-contiguous B with rows % 4 == 0 (float4 transpose path) and % 4 != 0
+# (gather path), split-BF16 segments starting at offsets that are not
+# multiples of 8 (scalar stores), tiles straddling the 64 x 64 edges.
+PACK_SHAPES = [(100, 68, 20), (64, 132, 36), (130, 256, 84), (65, 66, 67), (1, 300, 8),
+               (300, 1, 12)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
+@pytest.mark.parametrize("shape", PACK_SHAPES)
+def test_pack_layouts(shape, precision, cuda_dev):
+    import torch
+
+    import loop_tool_b200 as lt
+    from programs import mm
+
+    M, N, K = shape
+    T, _ = mm(M, K, N)
+    c = lt.cuda(T.ir, precision=precision)
+    g = torch.Generator(device=cuda_dev).manual_seed(M * 7 + N * 3 + K)
+    A = torch.randn(M * K, device=cuda_dev, generator=g)
+    B = torch.randn(K * N, device=cuda_dev, generator=g)
+    C = torch.full((M * N,), float("nan"), device=cuda_dev)
+    for _ in range(2):  # the second run reuses scratch: padding must stay zero
+        c([A, B, C])
+    torch.cuda.synchronize()
+    exact = (A.cpu().numpy().reshape(M, K).astype(np.float64) @
+             B.cpu().numpy().reshape(K, N).astype(np.float64))
+    got = C.cpu().numpy().reshape(M, N)
+    assert np.isfinite(got).all()
+    err = normwise(got, exact)
+    assert err <= TOL[precision], f"{shape} {precision}: normwise error {err:.3g}"
