@@ -246,11 +246,13 @@ def headline(args, world, rank, dev):
     per = [[] for _ in comps]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")  # ncu --nvtx --nvtx-include timed/
     t0.record(stream)
     for _ in range(args.steps):
         step(per)
     t1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     clocks = sampler.stop()
     ms = t0.elapsed_time(t1)
     nest_ms = [statistics.mean(a.elapsed_time(b) for a, b in lst) for lst in per]
@@ -476,7 +478,7 @@ def extra_c4(dev):
         pack_ms, gemm_ms = b1.run_timed()
         products = {"bf16": 1, "bf16x3": 3}[prec]
         big[prec] = {"total_ms": pack_ms + gemm_ms, "pack_ms": pack_ms, "gemm_ms": gemm_ms,
-                     "tile_n": c1.schedule(0)[2],
+                     "tile_variant": c1.schedule(0)[2],
                      "tflops_total": 2 * n ** 3 / ((pack_ms + gemm_ms) * 1e-3) / 1e12,
                      "tensor_tflops_gemm": products * 2 * n ** 3 / (gemm_ms * 1e-3) / 1e12,
                      "frac_of_measured_bf16_peak": products * 2 * n ** 3 / (gemm_ms * 1e-3) /
@@ -492,7 +494,8 @@ def extra_c5(dev, n_requests, rates):
 
     out = {"workload": f"{n_requests} requests, Poisson arrivals, 50% matmul (c4 shapes), "
                        f"30% conv (batch U[1,64]), 20% softmax (rows U[1,8192] x 4096)",
-           "kernel_cache": "warm (one pass over the trace first)"}
+           "kernel_cache": "warm (one pass over the trace first)",
+           "workspaces": "reserved per slot before serving"}
     configs = [("b200_bf16x3_8slots", dict(slots=8, precision="bf16x3")),
                ("plain_fp32_1slot", dict(slots=1, precision="fp32"))]
     for rate in rates:
@@ -503,6 +506,7 @@ def extra_c5(dev, n_requests, rates):
             warm = make_trace(n_requests, rate=1e9, seed=501)
             for r in warm:  # populate the IR and kernel caches
                 srv.bytes_of(r)
+            srv.reserve(warm)  # slot workspaces sized before the clock starts
             stats, _ = srv.serve(make_trace(n_requests, rate=rate, seed=501))
             row[name] = {k: stats[k] for k in ("req_per_s", "p50_ms", "p99_ms", "mean_ms",
                                                "peak_inflight")}
@@ -514,9 +518,10 @@ def extra_c5(dev, n_requests, rates):
 NCU_CASES = ("add", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "conv_bf16", "batch_bf16")
 
 
-def ncu_case(name, reps):
+def ncu_case(name, reps, tune=True):
     """One workload at a profiling size (inputs above L2, about 1 GB on the
-    device), run `reps` times: the command ncu captures."""
+    device), autotuned as in the benchmark, then run `reps` times inside the
+    NVTX range "profile" (capture with ncu --nvtx --nvtx-include profile/)."""
     import torch
 
     import loop_tool_b200 as ltb
@@ -540,17 +545,28 @@ def ncu_case(name, reps):
             members.append((c, [torch.randn(M * K, device=dev, generator=g),
                                 torch.randn(K * N, device=dev, generator=g),
                                 torch.empty(M * N, device=dev)]))
-        b = ltb.Batch(members)
+        if tune:
+            b, _, _ = ltb.tune_batch(members)
+        else:
+            b = ltb.Batch(members)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("profile")
         for _ in range(reps):
             b.run(sync=False)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         return
     c = ltb.Compiled(ir, **opts)
     bufs = [torch.randn(n, device=dev, generator=g) for n in c.io_sizes[:c.n_inputs]]
     bufs += [torch.empty(n, device=dev) for n in c.io_sizes[c.n_inputs:]]
+    if tune:
+        print(c.tune(bufs, reps=3))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("profile")
     for _ in range(reps):
         c.run(bufs, sync=False)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
 
 
 def main():
@@ -572,7 +588,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.ncu_case:
-        return ncu_case(args.ncu_case, args.reps)
+        return ncu_case(args.ncu_case, args.reps, args.tune)
 
     import torch
 

@@ -187,13 +187,14 @@ def _current_stream():
 def tune_batch(members, capture_stream=None, reps=3):
     """Tile widths for a batch of contractions, chosen by timing the grouped
     launch (operand packing + persistent GEMMs) under each policy: the
-    members' current schedules, every problem at 128 or at 256 columns, and
-    each member's own tuned width.  The best policy is left on the members,
+    members' current schedules, every problem at one variant (128 or 256
+    columns, each with either epilogue), and each member's own tuned
+    variant.  The best policy is left on the members,
     recorded in the schedule cache, and returned with its Batch and a
     report."""
     policies = {"current": [c.schedule(0) for c, _ in members]}
-    policies["all_128"] = [(0, 0, 128)] * len(members)
-    policies["all_256"] = [(0, 0, 256)] * len(members)
+    for v in (128, 129, 256, 257):  # tile width, +1: transposed epilogue
+        policies[f"all_{v}"] = [(0, 0, v)] * len(members)
     tuned = []
     for c, bufs in members:
         c.tune(bufs, reps=2)

@@ -30,6 +30,7 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include "async.cuh"
 #include "kernels.h"
 #include "tc_api.h"
 
@@ -39,6 +40,10 @@ constexpr int BM = 128, BK = 64;
 constexpr int NT = 320;
 constexpr int kChunkBlocks = 8;  // 8 x 64 = 512 K elements per accumulator
 constexpr int A_BYTES = BM * BK * 2;
+// epilogue: each drain warp transposes 32 x 32 blocks through a padded
+// shared buffer so global stores are whole 128-byte row segments
+constexpr int kEpiPitch = 33;
+constexpr int kEpiBytes = 8 * 32 * kEpiPitch * 4;
 
 // Tile shapes: BM x BN output tiles, BN = 256 (4-stage ring of 48 KB) or
 // BN = 128 (6-stage ring of 32 KB; narrow outputs and small problems).
@@ -53,52 +58,10 @@ struct Tile {
   // K-major, M = 128, N = BN
   static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
                                     ((uint32_t)(BN_ >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+  // dynamic: ring + alignment slack + barriers (the epilogue buffers are
+  // static shared memory, kEpiBytes more per CTA)
   static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 256;
 };
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n"
-      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for the phase of parity `parity` to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err) {
-  if (mbar_try(bar, parity)) return true;
-  const long long t0 = clock64();
-  while (!mbar_try(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles || *(volatile int*)err) {
-      atomicExch(err, 1);
-      return false;
-    }
-  }
-  return true;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
                                             int x, int y) {
   asm volatile(
@@ -129,16 +92,14 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r) {
+// 16 consecutive 32-bit columns of the warp's 32 TMEM lanes (one per thread)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-      "%28, %29, %30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
 }
 
@@ -173,7 +134,9 @@ __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, i
   *n0 = (idx / gm) * BN;
 }
 
-template <int BN>
+// 10 warps per CTA: the SM's four register partitions (16K each) hold up to
+// three warps each, so at most 168 registers per thread.
+template <int BN, bool kTransposeEpi>
 __global__ void __launch_bounds__(NT, 1)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
               float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
@@ -191,6 +154,8 @@ __global__ void __launch_bounds__(NT, 1)
   uint64_t* chunk_full = empty + STAGES;     // [2] MMA -> drain
   uint64_t* chunk_empty = chunk_full + 2;    // [2] drain -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(chunk_empty + 2);
+  __shared__ float epi[kTransposeEpi ? 8 * 32 * kEpiPitch : 1];  // drain warps' transposes
+  static_assert(T::SMEM + kEpiBytes <= 227 * 1024, "shared memory per CTA");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -301,23 +266,44 @@ __global__ void __launch_bounds__(NT, 1)
         const uint32_t base =
             tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * BN + half * T::HALF);
 #pragma unroll
-        for (int c = 0; c < T::HALF / 32; ++c) {
-          uint32_t r[32];
-          tmem_ld32(base + (uint32_t)(c * 32), r);
+        for (int c = 0; c < T::HALF / 16; ++c) {  // 16 columns at a time: fewer live registers
+          uint32_t r[16];
+          tmem_ld16(base + (uint32_t)(c * 16), r);
           tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 32; ++i) run[c * 32 + i] += __uint_as_float(r[i]);
+          for (int i = 0; i < 16; ++i) run[c * 16 + i] += __uint_as_float(r[i]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive(smem_u32(&chunk_empty[buf]));  // buffer free for the MMA
       }
       if (!alive) break;
-      // epilogue: this thread owns row m0 + 32*quad + lane, HALF columns
+      // epilogue: this warp owns rows m0 + 32*quad .. +31 (row m0 + 32*quad
+      // + lane in this thread's registers) and HALF columns from cbase
+      float* cb = c_override ? c_override : p.c;
       const int row = m0 + quad * 32 + lane;
-      if (row < p.M) {
+      const int cbase = n0 + half * T::HALF;
+      if (kTransposeEpi && p.unit_cols) {
+        float* stage = epi + (warp - 2) * (32 * kEpiPitch);
+        const int r0 = m0 + quad * 32;
+        const int rows = p.M - r0 < 32 ? p.M - r0 : 32;
+        const int64_t rb = row < p.M ? p.crow[row] : 0;
+#pragma unroll
+        for (int c = 0; c < T::HALF; c += 32) {
+          __syncwarp();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) stage[lane * kEpiPitch + j] = run[c + j];
+          __syncwarp();
+          const int col = cbase + c + lane;
+          const bool cok = col < p.N;
+#pragma unroll 8
+          for (int i = 0; i < 32; ++i) {  // row i of the block: 32 consecutive columns
+            const int64_t rbi = __shfl_sync(0xffffffffu, rb, i);
+            if (i < rows && cok) cb[rbi + col] = stage[i * kEpiPitch + lane];
+          }
+        }
+      } else if (row < p.M) {  // this thread's row: 16-byte stores where aligned
         const int64_t rbase = p.crow[row];
-        float* dst = (c_override ? c_override : p.c) + rbase;
-        const int cbase = n0 + half * T::HALF;
+        float* dst = cb + rbase;
 #pragma unroll
         for (int c = 0; c < T::HALF; c += 4) {
           const int j = cbase + c;
@@ -399,6 +385,47 @@ struct PackTables {
   int32_t grow[LTB_MAXG][PR], gk[LTB_MAXG][PKT], gub[LTB_MAXG];
 };
 
+// Guarded gather of one 64 x 64 tile into sm[k][r].  One side of the
+// element grid is fixed per thread (64 divides the block), so its offset
+// and guard partials stay in registers; the other side is warp-uniform and
+// read from the staged tables (broadcast).  NG: guard count (-1: any, up to
+// LTB_MAXG, through a runtime loop).
+template <int NG, bool along_r>
+__device__ __forceinline__ void gather_fill(const LtbPackJob& J, const PackTables& tb,
+                                            float (*sm)[PR + 1], int64_t rlim, int64_t klim,
+                                            int ng) {
+  constexpr int G = NG < 0 ? LTB_MAXG : NG;
+  const int tid = threadIdx.x;
+  const int fixed = tid & 63;
+  const bool fok = fixed < (along_r ? rlim : klim);
+  const int64_t fo = along_r ? tb.roff[fixed] : tb.koff[fixed];
+  const int vlim = (int)(along_r ? klim : rlim);
+  int32_t fg[G > 0 ? G : 1], ub[G > 0 ? G : 1];
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    const bool on = NG >= 0 || g < ng;
+    fg[g] = on ? (along_r ? tb.grow[g][fixed] : tb.gk[g][fixed]) : 0;
+    ub[g] = on ? tb.gub[g] : 1;  // off: 0 <= 0 + 0 < 1 always holds
+  }
+#pragma unroll 4
+  for (int q = 0; q < 16; ++q) {
+    const int v_ = (tid >> 6) + 4 * q;  // the varying side (warp-uniform)
+    float v = 0.f;
+    if (fok && v_ < vlim) {
+      bool ok = true;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int32_t o = NG >= 0 || g < ng ? (along_r ? tb.gk[g][v_] : tb.grow[g][v_]) : 0;
+        const int32_t w = fg[g] + o;
+        ok = ok && w >= 0 && w < ub[g];
+      }
+      if (ok) v = __ldg(J.op.base + fo + (along_r ? tb.koff[v_] : tb.roff[v_]));
+    }
+    if (along_r) sm[v_][fixed] = v;
+    else sm[fixed][v_] = v;
+  }
+}
+
 __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
                                           float (*sm)[PR + 1], PackTables* tabs) {
   const int tid = threadIdx.x;
@@ -455,36 +482,22 @@ __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
       }
       __syncthreads();
       const int64_t rlim = J.rows - r0, klim = J.K - k0;
-      // one side of the element grid is fixed per thread (64 divides the
-      // block), so its offset and guard partials stay in registers
       const bool along_r = J.mode == kPackGatherR;
-      const int fixed = tid & 63;
-      const bool fok = fixed < (along_r ? rlim : klim);
-      const int64_t fo = along_r ? tb.roff[fixed] : tb.koff[fixed];
-      int32_t fg[LTB_MAXG], ub[LTB_MAXG];
-#pragma unroll
-      for (int g = 0; g < LTB_MAXG; ++g) {
-        fg[g] = g < ng ? (along_r ? tb.grow[g][fixed] : tb.gk[g][fixed]) : 0;
-        ub[g] = g < ng ? tb.gub[g] : 1;
+#define LTB_GATHER(AR)                                                    \
+  switch (ng) { /* guard count known at compile time: no predicated loop */ \
+    case 0: gather_fill<0, AR>(J, tb, sm, rlim, klim, ng); break;          \
+    case 1: gather_fill<1, AR>(J, tb, sm, rlim, klim, ng); break;          \
+    case 2: gather_fill<2, AR>(J, tb, sm, rlim, klim, ng); break;          \
+    case 3: gather_fill<3, AR>(J, tb, sm, rlim, klim, ng); break;          \
+    case 4: gather_fill<4, AR>(J, tb, sm, rlim, klim, ng); break;          \
+    default: gather_fill<-1, AR>(J, tb, sm, rlim, klim, ng); break;        \
+  }
+      if (along_r) {
+        LTB_GATHER(true)
+      } else {
+        LTB_GATHER(false)
       }
-#pragma unroll 4
-      for (int q = 0; q < 16; ++q) {
-        const int v_ = (tid >> 6) + 4 * q;  // the varying side (warp-uniform)
-        float v = 0.f;
-        if (fok && v_ < (along_r ? klim : rlim)) {
-          bool ok = true;
-#pragma unroll
-          for (int g = 0; g < LTB_MAXG; ++g) {
-            if (g < ng) {
-              const int32_t w = fg[g] + (along_r ? tb.gk[g][v_] : tb.grow[g][v_]);
-              ok = ok && w >= 0 && w < ub[g];
-            }
-          }
-          if (ok) v = __ldg(J.op.base + fo + (along_r ? tb.koff[v_] : tb.roff[v_]));
-        }
-        if (along_r) sm[v_][fixed] = v;
-        else sm[fixed][v_] = v;
-      }
+#undef LTB_GATHER
     }
     __syncthreads();
 #pragma unroll
@@ -631,15 +644,15 @@ cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t
   return cudaGetLastError();
 }
 
-template <int BN>
+template <int BN, bool TE>
 static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b) {
   static bool attr = false;
   const size_t smem = Tile<BN>::SMEM;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN, TE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -652,7 +665,8 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
     ma = *static_cast<const CUtensorMap*>(map_a);
     mb = *static_cast<const CUtensorMap*>(map_b);
   }
-  k_gemm_tc<BN><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err, one, ma, mb);
+  k_gemm_tc<BN, TE><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err, one, ma,
+                                            mb);
   return cudaGetLastError();
 }
 
@@ -661,11 +675,15 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                cudaStream_t st, const LtbTcProblem* single, const void* map_a,
                                const void* map_b) {
   if (total_tiles == 0) return cudaSuccess;
-  if (bn == 128)
-    return launch_tc<128>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a,
-                          map_b);
-  if (bn == 256)
-    return launch_tc<256>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a,
-                          map_b);
+#define LTB_TC(BN, TE)                                                                      \
+  return launch_tc<BN, TE>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a, \
+                           map_b)
+  switch (bn) {
+    case 128: LTB_TC(128, false);
+    case 129: LTB_TC(128, true);
+    case 256: LTB_TC(256, false);
+    case 257: LTB_TC(256, true);
+  }
+#undef LTB_TC
   return cudaErrorInvalidValue;
 }

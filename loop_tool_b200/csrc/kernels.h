@@ -32,7 +32,7 @@ cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,
 // elementwise; h_stages the host copies of the same stages)
 cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, const LtbStage* const* h_stages,
                                  int nsteps, const LtbBufTable& bt, int sms,
-                                 cudaStream_t st, const LtbCfg& cfg);
+                                 cudaStream_t st, const LtbCfg& cfg, int* err);
 // Candidate schedules the autotuner tries for a stage of a family (fills up
 // to cap entries, returns the count).  The row-softmax variants depend on
 // the row length.

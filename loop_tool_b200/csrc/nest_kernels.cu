@@ -3,9 +3,11 @@
 // design points are coalescing, 128-bit accesses along the innermost output
 // dim, and grids sized in multiples of the 148 SMs.
 #include <cfloat>
+#include <map>
 #include <mutex>
-#include <unordered_map>
+#include <tuple>
 
+#include "async.cuh"
 #include "kernels.h"
 #include "vm.cuh"
 
@@ -752,59 +754,86 @@ __global__ void __launch_bounds__(256)
   const uint32_t total = outer * nvec;
   const float* __restrict__ src = bt.p[L.buf];
   float* __restrict__ out = bt.p[S.out_buf];
-  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < total;
-       w += gridDim.x * blockDim.x) {
-    const uint32_t o32 = fdiv(w, nvec_mul, nvec_shr);
-    const uint32_t iv = w - o32 * nvec;
-    int64_t base = L.off, obase = S.out_off;
-    uint32_t r = o32;
-    for (int k = ki - 1; k >= 0; --k) {
-      const uint32_t q = fdiv(r, S.dm_mul[k], S.dm_shr[k]);
-      const int64_t c = r - q * (uint32_t)S.size[k];
-      base += L.coef[k] * c;
-      obase += S.out_coef[k] * c;
-      r = q;
+  // two work items per thread per step: their span loads are all issued
+  // before either fold, doubling the bytes in flight per thread
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t w0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w0 < total;
+       w0 += 2 * stride) {
+    int64_t base[2], obase[2];
+    int nv[2];
+    bool live[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const uint64_t w = w0 + u * stride;
+      live[u] = w < total;
+      const uint32_t ww = (uint32_t)(live[u] ? w : w0);  // < total < 2^32
+      const uint32_t o32 = fdiv(ww, nvec_mul, nvec_shr);
+      const uint32_t iv = ww - o32 * nvec;
+      int64_t b = L.off, ob = S.out_off;
+      uint32_t r = o32;
+      for (int k = ki - 1; k >= 0; --k) {
+        const uint32_t q = fdiv(r, S.dm_mul[k], S.dm_shr[k]);
+        const int64_t c = r - q * (uint32_t)S.size[k];
+        b += L.coef[k] * c;
+        ob += S.out_coef[k] * c;
+        r = q;
+      }
+      const int64_t o0 = (int64_t)iv * 4;
+      base[u] = b + L.coef[ki] * o0;
+      obase[u] = ob + o0;
+      nv[u] = (int)(inner - o0 < 4 ? inner - o0 : 4);
     }
-    const int64_t o0 = (int64_t)iv * 4;
-    base += L.coef[ki] * o0;
-    obase += o0;
-    const int nv = (int)(inner - o0 < 4 ? inner - o0 : 4);
-    float acc[4];
+    float acc[2][4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[j] = S.red_init;
-#pragma unroll 4
-    for (int64_t rc = 0; rc < RC; ++rc) {  // unrolled: the spans' loads issue together
-      const float* p = src + base + roff[rc];
-      float span[N];
-      if (nv == 4 && ((base + roff[rc]) & 3) == 0) {
+    for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int q = 0; q + 4 <= N; q += 4) {
-          const float4 t = __ldg(reinterpret_cast<const float4*>(p + q));
-          span[q] = t.x; span[q + 1] = t.y; span[q + 2] = t.z; span[q + 3] = t.w;
+      for (int j = 0; j < 4; ++j) acc[u][j] = S.red_init;
+#pragma unroll 2
+    for (int64_t rc = 0; rc < RC; ++rc) {
+      float span[2][N];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const float* p = src + base[u] + roff[rc];
+        if (nv[u] == 4 && ((base[u] + roff[rc]) & 3) == 0) {
+#pragma unroll
+          for (int q = 0; q + 4 <= N; q += 4) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(p + q));
+            span[u][q] = t.x; span[u][q + 1] = t.y; span[u][q + 2] = t.z; span[u][q + 3] = t.w;
+          }
+#pragma unroll
+          for (int q = N & ~3; q < N; ++q) span[u][q] = __ldg(p + q);
+        } else {
+#pragma unroll
+          for (int q = 0; q < N; ++q)
+            span[u][q] = q <= (nv[u] - 1) * S_ + K_ - 1 ? __ldg(p + q) : 0.f;
         }
-#pragma unroll
-        for (int q = N & ~3; q < N; ++q) span[q] = __ldg(p + q);
-      } else {
-#pragma unroll
-        for (int q = 0; q < N; ++q) span[q] = q <= (nv - 1) * S_ + K_ - 1 ? __ldg(p + q) : 0.f;
       }
 #pragma unroll
-      for (int q = 0; q < K_; ++q)
+      for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[j] = fold(S.red_op, acc[j], span[j * S_ + q]);
+        for (int q = 0; q < K_; ++q)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[u][j] = fold(S.red_op, acc[u][j], span[u][j * S_ + q]);
     }
-    if (nv == 4 && (obase & 3) == 0) {
-      *reinterpret_cast<float4*>(out + obase) = make_float4(acc[0], acc[1], acc[2], acc[3]);
-    } else {
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (j < nv) out[obase + j] = acc[j];
+    for (int u = 0; u < 2; ++u) {
+      if (!live[u]) continue;
+      float* o = out + obase[u];
+      if (nv[u] == 4 && (obase[u] & 3) == 0) {
+        *reinterpret_cast<float4*>(o) =
+            make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv[u]) o[j] = acc[u][j];
+      }
     }
   }
 }
 
 // ----------------------------------------------------------- row softmax
-// Fused pattern m = max_n x, s = sum_n exp(x - m), y = exp(x - m) / s, the
+// Fused pattern m = max_n x, s = sum_n exp(x - m), y = exp(x - m) / s
+// (computed as e * (1/s) with a correctly rounded reciprocal), the
 // row held in registers (EPT floats per thread, loaded and stored as
 // float4), so HBM sees one read and one write per element.  One full wave
 // of CTAs strides over the rows; while a row is reduced the next row's loads
@@ -905,17 +934,20 @@ __global__ void __launch_bounds__(NT)
       P.m[o.m] = m;
       P.s[o.s] = sum;
     }
+    // y = e * (1 / s): one correctly rounded reciprocal per row, within
+    // 1.5 ulp of e / s
+    const float inv = __frcp_rn(sum);
 #pragma unroll
     for (int q = 0; q < EPT / 4; ++q) {
       const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
       if (v4 && j < P.n) {
         __stcs(reinterpret_cast<float4*>(P.y + o.y + j),
-               make_float4(v[4 * q] / sum, v[4 * q + 1] / sum, v[4 * q + 2] / sum,
-                           v[4 * q + 3] / sum));
+               make_float4(v[4 * q] * inv, v[4 * q + 1] * inv, v[4 * q + 2] * inv,
+                           v[4 * q + 3] * inv));
       } else {
 #pragma unroll
         for (int e = 0; e < 4; ++e)
-          if (j + e < P.n) P.y[o.y + j + e] = v[4 * q + e] / sum;
+          if (j + e < P.n) P.y[o.y + j + e] = v[4 * q + e] * inv;
       }
     }
 #pragma unroll
@@ -925,6 +957,116 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// TMA-staged form: each CTA keeps kSmxRing of its rows in flight in a
+// shared-memory ring, one 1-D bulk copy (cp.async.bulk) per row completing
+// on the slot's mbarrier; a slot is refilled with the row kSmxRing ahead as
+// soon as every thread has read it.  Needs 16-byte aligned rows.  Same
+// arithmetic as k_softmax_rows.  A copy that does not land within the
+// bounded wait raises *err; the CTA then waits (bounded) for the copies it
+// still has in flight and exits.
+constexpr int kSmxRing = 4;
+
+template <int EPT, int NT>
+__global__ void __launch_bounds__(NT)
+    k_softmax_bulk(const __grid_constant__ SoftmaxRows P, int* err) {
+  extern __shared__ __align__(128) float ring[];  // kSmxRing x n floats
+  __shared__ __align__(8) uint64_t bars[kSmxRing];
+  __shared__ float red[2][NT / 32];
+  __shared__ int stop;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t first = blockIdx.x;
+  if (first >= P.rows) return;
+  const int64_t cnt = (P.rows - first + gridDim.x - 1) / gridDim.x;  // rows of this CTA
+  const uint32_t bytes = (uint32_t)(P.n * 4);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kSmxRing; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    fence_mbar_init();
+    stop = 0;
+  }
+  __syncthreads();
+  auto issue = [&](int64_t i) {  // row i of this CTA into slot i % kSmxRing
+    const int s = (int)(i % kSmxRing);
+    const RowOffs o = row_offs(P, first + i * gridDim.x);
+    const uint32_t bar = smem_u32(&bars[s]);
+    mbar_expect_tx(bar, bytes);
+    bulk_load(smem_u32(ring + (size_t)s * P.n), P.x + o.x, bytes, bar);
+  };
+  if (threadIdx.x == 0)
+    for (int64_t i = 0; i < cnt && i < kSmxRing; ++i) issue(i);
+  int64_t i = 0;
+  for (; i < cnt; ++i) {
+    const int s = (int)(i % kSmxRing);
+    if (!mbar_wait(smem_u32(&bars[s]), (uint32_t)((i / kSmxRing) & 1), err)) stop = 1;
+    __syncthreads();
+    if (stop) break;
+    const RowOffs o = row_offs(P, first + i * gridDim.x);
+    const float* xs = ring + (size_t)s * P.n;
+    float v[EPT];
+#pragma unroll
+    for (int q = 0; q < EPT / 4; ++q) {
+      const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
+      if (j < P.n) {
+        const float4 t = *reinterpret_cast<const float4*>(xs + j);
+        v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
+      } else {
+        v[4 * q] = v[4 * q + 1] = v[4 * q + 2] = v[4 * q + 3] = -INFINITY;
+      }
+    }
+    float m = -FLT_MAX;
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) m = m > v[e] ? m : v[e];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const float t = __shfl_xor_sync(0xffffffffu, m, off);
+      m = m > t ? m : t;
+    }
+    if (lane == 0) red[0][wid] = m;
+    __syncthreads();  // every thread has read slot s: refill it
+    if (threadIdx.x == 0 && i + kSmxRing < cnt) issue(i + kSmxRing);
+    m = red[0][0];
+#pragma unroll
+    for (int w = 1; w < NT / 32; ++w) m = m > red[0][w] ? m : red[0][w];
+    float sum = 0.f;
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      v[e] = expf(v[e] - m);
+      sum += v[e];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    if (lane == 0) red[1][wid] = sum;
+    __syncthreads();
+    sum = 0.f;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) sum += red[1][w];
+    if (threadIdx.x == 0) {
+      P.m[o.m] = m;
+      P.s[o.s] = sum;
+    }
+    // y = e * (1 / s): one correctly rounded reciprocal per row, within
+    // 1.5 ulp of e / s
+    const float inv = __frcp_rn(sum);
+    const bool v4 = (o.y & 3) == 0;
+#pragma unroll
+    for (int q = 0; q < EPT / 4; ++q) {
+      const int64_t j = (int64_t)(q * NT + threadIdx.x) * 4;
+      if (v4 && j < P.n) {
+        __stcs(reinterpret_cast<float4*>(P.y + o.y + j),
+               make_float4(v[4 * q] * inv, v[4 * q + 1] * inv, v[4 * q + 2] * inv,
+                           v[4 * q + 3] * inv));
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (j + e < P.n) P.y[o.y + j + e] = v[4 * q + e] * inv;
+      }
+    }
+  }
+  // stopped early: rows [i, i + kSmxRing) may still be landing
+  if (threadIdx.x == 0 && i < cnt)
+    for (int64_t k = i; k < cnt && k < i + kSmxRing; ++k)
+      mbar_drain(smem_u32(&bars[k % kSmxRing]), (uint32_t)((k / kSmxRing) & 1));
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ launchers
@@ -932,28 +1074,30 @@ __global__ void __launch_bounds__(NT)
 // cached per kernel and block size).  By default grid-stride kernels launch
 // exactly one full wave (SMs x resident CTAs); a schedule's cta_per_sm
 // overrides that (more CTAs than resident = several waves).
-static int resident(const void* kernel, int threads) {
+static int resident(const void* kernel, int threads, size_t smem = 0) {
   static std::mutex mu;
-  static std::unordered_map<const void*, int> cache[3];  // 128 / 256 / 512 threads
-  const int slot = threads <= 128 ? 0 : threads <= 256 ? 1 : 2;
+  static std::map<std::tuple<const void*, int, size_t>, int> cache;
+  const auto key = std::make_tuple(kernel, threads, smem);
   std::lock_guard<std::mutex> g(mu);
-  auto it = cache[slot].find(kernel);
-  if (it != cache[slot].end()) return it->second;
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess ||
       n < 1) {
     cudaGetLastError();
     n = 1;
   }
-  cache[slot][kernel] = n;
+  cache[key] = n;
   return n;
 }
 
 template <typename K>
-static int grid_of(K kernel, int64_t work, int threads, int sms, const LtbCfg& cfg) {
+static int grid_of(K kernel, int64_t work, int threads, int sms, const LtbCfg& cfg,
+                   size_t smem = 0) {
   int64_t blocks = (work + threads - 1) / threads;
-  const int per_sm = cfg.cta_per_sm > 0 ? cfg.cta_per_sm
-                                        : resident(reinterpret_cast<const void*>(kernel), threads);
+  const int per_sm = cfg.cta_per_sm > 0
+                         ? cfg.cta_per_sm
+                         : resident(reinterpret_cast<const void*>(kernel), threads, smem);
   const int64_t cap = (int64_t)sms * per_sm;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
@@ -1090,10 +1234,15 @@ cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,
 }
 
 // Row-softmax schedules: (elements per thread, threads) pairs covering the
-// row; variant v (1-based) indexes this table.
+// row; variant v (1-based) indexes this table.  Variants 1-11 hold the next
+// row in registers (k_softmax_rows), 12-17 stage rows through a shared
+// memory ring with bulk copies (k_softmax_bulk).
 static const int kSmxVariants[][2] = {{4, 128},  {4, 256},  {8, 256},  {16, 256},
                                       {32, 256}, {8, 128},  {16, 128}, {32, 128},
-                                      {4, 512},  {8, 512},  {16, 512}};
+                                      {4, 512},  {8, 512},  {16, 512}, {4, 256},
+                                      {8, 256},  {16, 256}, {32, 256}, {8, 512},
+                                      {16, 512}};
+constexpr int kFirstBulk = 12;
 constexpr int kNumSmx = sizeof(kSmxVariants) / sizeof(kSmxVariants[0]);
 
 static bool softmax_chain(const LtbStage* const* h_stages, int nsteps) {
@@ -1115,13 +1264,28 @@ static bool softmax_fits(int v, int64_t inner) {
   return (int64_t)e * t >= inner && ((int64_t)e * t <= 2 * inner || e == 4);
 }
 
+// Rows staged by bulk copies must start on 16-byte boundaries (x offsets
+// and row strides multiples of 4 floats) and a ring of kSmxRing rows must
+// fit in shared memory.
+static bool softmax_bulk_ok(const LtbStage* const* h_stages, int nsteps) {
+  const LtbStage& A = *h_stages[0];
+  const LtbStage& C = *h_stages[nsteps - 1];
+  const LtbLoad& X = A.loads[A.code[0].arg];
+  const int64_t n = C.size[C.nout - 1];
+  if ((n & 3) || (X.off & 3) || n * 4 * kSmxRing > 200 * 1024) return false;
+  for (int k = 0; k < C.nout - 1; ++k)
+    if (X.coef[k] & 3) return false;
+  return true;
+}
+
 int ltb_row_chain_candidates(const LtbStage* const* h_stages, int nsteps, LtbCfg* out, int cap) {
   int n = 0;
   if (softmax_chain(h_stages, nsteps)) {
     const LtbStage& f = *h_stages[nsteps - 1];
     const int64_t inner = f.size[f.nout - 1];
+    const bool bulk = softmax_bulk_ok(h_stages, nsteps);
     for (int v = 1; v <= kNumSmx; ++v)
-      if (softmax_fits(v, inner))
+      if (softmax_fits(v, inner) && (v < kFirstBulk || bulk))
         for (int w : {0, 2, 4, 8})
           if (n < cap) out[n++] = LtbCfg{w, 0, v};
     return n;
@@ -1132,9 +1296,25 @@ int ltb_row_chain_candidates(const LtbStage* const* h_stages, int nsteps, LtbCfg
   return n;
 }
 
+template <int EPT, int NT>
+static cudaError_t launch_softmax_bulk(const SoftmaxRows& P, int sms, const LtbCfg& cfg,
+                                       int* err, cudaStream_t st) {
+  static size_t attr = 0;  // largest dynamic shared memory opted into so far
+  const size_t smem = (size_t)kSmxRing * P.n * 4;
+  if (smem > attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_softmax_bulk<EPT, NT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = smem;
+  }
+  const int g = grid_of(k_softmax_bulk<EPT, NT>, P.rows * NT, NT, sms, cfg, smem);
+  k_softmax_bulk<EPT, NT><<<g, NT, smem, st>>>(P, err);
+  return cudaGetLastError();
+}
+
 cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, const LtbStage* const* h_stages,
                                  int nsteps, const LtbBufTable& bt, int sms,
-                                 cudaStream_t st, const LtbCfg& cfg) {
+                                 cudaStream_t st, const LtbCfg& cfg, int* err) {
   if (nsteps > kMaxChain) return cudaErrorInvalidValue;
   const LtbStage& final_stage = *h_stages[nsteps - 1];
   int64_t rows = 1;
@@ -1165,7 +1345,10 @@ cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, const LtbStage* const
       P.sc[k] = B.out_coef[k];
     }
     int v = cfg.variant;
-    if (v < 1 || v > kNumSmx || !softmax_fits(v, inner)) v = softmax_default(inner);
+    const bool bulk = softmax_bulk_ok(h_stages, nsteps) &&
+                      (reinterpret_cast<uintptr_t>(P.x) & 15) == 0;
+    if (v < 1 || v > kNumSmx || !softmax_fits(v, inner) || (v >= kFirstBulk && !bulk))
+      v = softmax_default(inner);
     switch (v) {
 #define LTB_SMX(V, EPT, NT)                                                            \
   case V: {                                                                            \
@@ -1177,6 +1360,12 @@ cudaError_t ltb_launch_row_chain(const LtbStage* d_stages, const LtbStage* const
       LTB_SMX(5, 32, 256) LTB_SMX(6, 8, 128) LTB_SMX(7, 16, 128) LTB_SMX(8, 32, 128)
       LTB_SMX(9, 4, 512) LTB_SMX(10, 8, 512) LTB_SMX(11, 16, 512)
 #undef LTB_SMX
+      case 12: return launch_softmax_bulk<4, 256>(P, sms, cfg, err, st);
+      case 13: return launch_softmax_bulk<8, 256>(P, sms, cfg, err, st);
+      case 14: return launch_softmax_bulk<16, 256>(P, sms, cfg, err, st);
+      case 15: return launch_softmax_bulk<32, 256>(P, sms, cfg, err, st);
+      case 16: return launch_softmax_bulk<8, 512>(P, sms, cfg, err, st);
+      case 17: return launch_softmax_bulk<16, 512>(P, sms, cfg, err, st);
     }
     return cudaErrorInvalidValue;
   }

@@ -86,11 +86,13 @@ struct GemmTables {
   LtbTcProblem prob{};                // launch template (maps/c bound per run)
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
   int bn = 256;                       // tensor-core tile width (128 or 256)
+  int epi = 0;                        // 1: shared-memory transposed epilogue
 };
 
 // Tile width of a tensor-core contraction: output tiles are 128 x bn.
-void set_tile_n(GemmTables& t, int bn) {
+void set_tile_n(GemmTables& t, int bn, int epi) {
   t.bn = bn;
+  t.epi = epi;
   const int64_t tn = (t.prob.N + bn - 1) / bn;
   t.prob.tiles_n = (int)tn;
   t.tiles = (int64_t)t.prob.tiles_m * tn;
@@ -290,7 +292,7 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     e.tiles_m = tm;
     e.unit_cols = t.unit_cols ? 1 : 0;
     // narrow outputs take 128-wide tiles (no half-empty MMA), the rest 256
-    set_tile_n(t, con.N <= 128 ? 128 : 256);
+    set_tile_n(t, con.N <= 128 ? 128 : 256, 0);
   }
 }
 
@@ -406,7 +408,7 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         n++;
       const LtbStage* hs[16];
       for (int k = 0; k < n && k < 16; ++k) hs[k] = &P.stages[i + k].dev;
-      e = n <= 16 ? ltb_launch_row_chain(d, hs, n, bt, c->sms, st, cfg) : cudaErrorInvalidValue;
+      e = n <= 16 ? ltb_launch_row_chain(d, hs, n, bt, c->sms, st, cfg, c->d_err) : cudaErrorInvalidValue;
       break;
     }
     case ltb::Family::contraction: {
@@ -442,8 +444,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           one.c = p.c;
           one.crow = t.c_row;
           one.ccol = t.c_col;
-          e = ltb_launch_gemm_tc(t.bn, nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st, &one,
-                                 maps, maps + 128);
+          e = ltb_launch_gemm_tc(t.bn | t.epi, nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st,
+                                 &one, maps, maps + 128);
         }
       }
       break;
@@ -467,10 +469,11 @@ void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
 void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
   c->cfg[i] = cfg;
   const int g = c->gemm_of[i];
-  if (g >= 0 && c->gemms[g].tc) {
-    const int bn = cfg.variant == 128 ? 128 : 256;
-    set_tile_n(c->gemms[g], bn);
-    c->cfg[i].variant = bn;
+  if (g >= 0 && c->gemms[g].tc) {  // variant: tile width, +1 for the transposed epilogue
+    const int bn = (cfg.variant & ~1) == 128 ? 128 : 256;
+    const int epi = cfg.variant & 1;
+    set_tile_n(c->gemms[g], bn, epi);
+    c->cfg[i].variant = bn | epi;
   }
 }
 
@@ -596,7 +599,7 @@ std::string describe(ltb_compiled* c, int i) {
     const auto& t = c->gemms[c->gemm_of[i]];
     if (t.tc)
       o << "tile(128x" << t.bn << "x64) tensor_cores(tcgen05) parallel(persistent, "
-        << t.tiles << " tiles)";
+        << t.tiles << " tiles) epilogue(" << (t.epi ? "smem transpose" : "row stores") << ")";
     else
       o << "tile(128x128) cuda_cores";
     return o.str();
@@ -633,10 +636,8 @@ std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
       break;
     }
     case ltb::Family::contraction:
-      if (c->gemms[c->gemm_of[i]].tc) {
-        buf[n++] = LtbCfg{0, 0, 128};
-        buf[n++] = LtbCfg{0, 0, 256};
-      }
+      if (c->gemms[c->gemm_of[i]].tc)
+        for (int v : {128, 129, 256, 257}) buf[n++] = LtbCfg{0, 0, v};
       break;
   }
   return std::vector<LtbCfg>(buf, buf + n);
@@ -702,11 +703,11 @@ struct ltb_batch {
   LtbPackJob* d_jobs = nullptr;
   int njobs = 0;
   int64_t pack_tiles = 0;
-  // tensor-core problems grouped by tile width (group 0: 128, group 1: 256),
-  // one persistent launch per non-empty group
-  LtbTcProblem* d_tc[2] = {nullptr, nullptr};
-  int ntc[2] = {0, 0};
-  int64_t tc_tiles[2] = {0, 0};
+  // tensor-core problems grouped by schedule variant (group 2 * (tile width
+  // == 256) + transposed epilogue), one persistent launch per non-empty group
+  LtbTcProblem* d_tc[4] = {nullptr, nullptr, nullptr, nullptr};
+  int ntc[4] = {0, 0, 0, 0};
+  int64_t tc_tiles[4] = {0, 0, 0, 0};
   LtbGemmProblem* d_simt = nullptr;
   int64_t* d_simt_start = nullptr;
   int64_t simt_tiles = 0;
@@ -720,9 +721,10 @@ struct ltb_batch {
 namespace {
 
 void batch_gemms(ltb_batch* b, cudaStream_t st) {
-  for (int g = 0; g < 2; ++g)
+  for (int g = 0; g < 4; ++g)
     if (b->ntc[g])
-      CUDA_TRY(ltb_launch_gemm_tc(g ? 256 : 128, b->d_tc[g], b->ntc[g], b->tc_tiles[g], nullptr,
+      CUDA_TRY(ltb_launch_gemm_tc((g >= 2 ? 256 : 128) | (g & 1), b->d_tc[g], b->ntc[g],
+                                  b->tc_tiles[g], nullptr,
                                   b->sms, b->d_err, st));
 }
 
@@ -763,8 +765,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->device = cs[0]->device;
     b->sms = cs[0]->sms;
     std::vector<LtbPackJob> jobs;
-    std::vector<LtbTcProblem> tcp[2];
-    std::vector<unsigned char> maps[2];  // two 128-byte CUtensorMaps per problem
+    std::vector<LtbTcProblem> tcp[4];
+    std::vector<unsigned char> maps[4];  // two 128-byte CUtensorMaps per problem
     std::vector<LtbGemmProblem> sp;
     std::vector<int64_t> sstart;
     for (int i = 0; i < n; ++i) {
@@ -821,7 +823,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         b->owned.push_back(bp);
         job(p.a, p.M, ap, t.a_mask, t.a_kcontig);
         job(p.b, p.N, bp, t.b_mask, t.b_kcontig);
-        const int grp = t.bn == 128 ? 0 : 1;
+        const int grp = (t.bn == 256 ? 2 : 0) + t.epi;
         auto& mv = maps[grp];
         mv.resize(mv.size() + 256);
         unsigned char* m = mv.data() + mv.size() - 256;
@@ -843,7 +845,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->njobs = (int)jobs.size();
     if (b->tc) {
       b->d_jobs = upload(jobs, b->owned);
-      for (int g = 0; g < 2; ++g) {
+      for (int g = 0; g < 4; ++g) {
         // tensor maps in device memory (cudaMalloc is 256-byte aligned)
         unsigned char* d_maps = upload(maps[g], b->owned);
         for (size_t i = 0; i < tcp[g].size(); ++i) {
@@ -954,10 +956,13 @@ int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   std::string k = name;
   if (k == "problems") *value = b->n;
   else if (k == "flops") *value = (int64_t)b->flops;
-  else if (k == "launches") *value = b->tc ? 1 + (b->ntc[0] > 0) + (b->ntc[1] > 0) : 1;
-  else if (k == "tiles") *value = b->tc ? b->tc_tiles[0] + b->tc_tiles[1] : b->simt_tiles;
-  else if (k == "tiles_128") *value = b->tc_tiles[0];
-  else if (k == "tiles_256") *value = b->tc_tiles[1];
+  else if (k == "launches")
+    *value = b->tc ? 1 + (b->ntc[0] > 0) + (b->ntc[1] > 0) + (b->ntc[2] > 0) + (b->ntc[3] > 0) : 1;
+  else if (k == "tiles")
+    *value = b->tc ? b->tc_tiles[0] + b->tc_tiles[1] + b->tc_tiles[2] + b->tc_tiles[3]
+                   : b->simt_tiles;
+  else if (k == "tiles_128") *value = b->tc_tiles[0] + b->tc_tiles[1];
+  else if (k == "tiles_256") *value = b->tc_tiles[2] + b->tc_tiles[3];
   else if (k == "graph") *value = b->exec ? 1 : 0;
   else return fail(LTB_ERR_INVALID, "unknown property " + k);
   return LTB_OK;

@@ -50,8 +50,10 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
                             cudaStream_t st);
 
 // Persistent grouped launch over every tile of every problem
-// (tiles_m * ceil(N / bn) tiles per problem, bn = 128 or 256: the tile
-// width the problems' tiles_n and B tensor maps were made for).
+// (tiles_m * ceil(N / tile) tiles per problem, tile = bn & ~1 = 128 or 256:
+// the tile width the problems' tiles_n and B tensor maps were made for;
+// odd bn selects the epilogue that transposes 32 x 32 blocks through shared
+// memory into whole-row stores instead of per-thread 16-byte row stores).
 // c_override, if not null, replaces every problem's output pointer.
 // d_probs == nullptr: a single problem passed by value with its two tensor
 // maps (host copies, passed as kernel parameters).

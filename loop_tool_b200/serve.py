@@ -151,6 +151,24 @@ class Server:
         self.ws[slot] = torch.empty(want, device=self.dev)
         return self.ws[slot]
 
+    def _need(self, req):
+        """Floats of a slot workspace for this request (regions 256-byte
+        aligned: inputs, output, run scratch)."""
+        c = self._compiled(req)
+        return sum(_up(n) for n in c.io_sizes) + _up((c.int_property("scratch_bytes") + 3) // 4)
+
+    def reserve(self, trace):
+        """Size every slot's workspace for the largest request of `trace`
+        (within the HBM budget) before serving, so no allocation, and no
+        allocator synchronisation, happens while requests are in flight."""
+        need = max((self._need(r) for r in trace), default=0)
+        per_slot = min(need, self.budget // (4 * len(self.streams)))
+        for slot in range(len(self.streams)):
+            with self.torch.cuda.stream(self.streams[slot]):
+                self._workspace(slot, per_slot)
+        self.torch.cuda.synchronize()
+        return 4 * per_slot * len(self.streams)
+
     def _launch(self, req, slot, now):
         torch = self.torch
         c = self._compiled(req)

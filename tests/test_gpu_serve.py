@@ -46,3 +46,23 @@ def test_admission_respects_hbm_budget(cuda_dev):
     assert stats["requests"] == len(trace)
     assert srv.peak_used <= int(need * 1.5)
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
+
+
+@pytest.mark.gpu
+def test_reserved_workspaces_serve_without_growth(cuda_dev):
+    """Workspaces sized up front: serving allocates nothing more, and every
+    result matches the unreserved server's."""
+    from loop_tool_b200.serve import Server
+
+    trace = small_trace(24, seed=13)
+    ref = Server(slots=4, keep_outputs=True)
+    _, base = ref.serve(small_trace(24, seed=13))
+    srv = Server(slots=4, keep_outputs=True)
+    reserved = srv.reserve(trace)
+    sizes = [w.numel() for w in srv.ws]
+    assert reserved == 4 * sum(sizes) and min(sizes) > 0
+    _, done = srv.serve(trace)
+    assert [w.numel() for w in srv.ws] == sizes, "a workspace grew while serving"
+    by_id = {r.rid: r.out for r in base}
+    for r in done:
+        assert same(r.out, by_id[r.rid]), f"request {r.rid} differs"
