@@ -515,7 +515,8 @@ def extra_c5(dev, n_requests, rates):
 
 
 # ------------------------------------------------------- profiling cases
-NCU_CASES = ("add", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "conv_bf16", "batch_bf16")
+NCU_CASES = ("add", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "conv_bf16", "batch_bf16",
+             "mm_bf16_batch")
 
 
 def ncu_case(name, reps, tune=True):
@@ -531,6 +532,21 @@ def ncu_case(name, reps, tune=True):
     opts = {}
     if name in ("add", "softmax", "maxpool"):
         ir = {n.split("_")[0]: t for n, t, _ in nests(add_log2=26)}[name]
+    elif name == "mm_bf16_batch":  # 8192^3 through the grouped (batch) launch path
+        n = 8192
+        c = ltb.Compiled(mm_ir(n, n, n), precision="bf16")
+        bufs = [torch.randn(n * n, device=dev, generator=g) for _ in range(2)]
+        bufs.append(torch.empty(n * n, device=dev))
+        if tune:
+            c.tune(bufs, reps=2)
+        b = ltb.Batch([(c, bufs)])
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("profile")
+        for _ in range(reps):
+            b.run(sync=False)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        return
     elif name.startswith("mm_"):
         ir, opts = mm_ir(8192, 8192, 8192), {"precision": name[3:]}
     elif name == "conv_bf16":

@@ -382,6 +382,7 @@ static_assert(sizeof(LtbPackJob) % 8 == 0, "job copied as 8-byte words");
 
 struct PackTables {
   int64_t roff[PR], koff[PKT];
+  int32_t roff32[PR], koff32[PKT];  // the same offsets when the job is off32
   int32_t grow[LTB_MAXG][PR], gk[LTB_MAXG][PKT], gub[LTB_MAXG];
 };
 
@@ -390,7 +391,7 @@ struct PackTables {
 // and guard partials stay in registers; the other side is warp-uniform and
 // read from the staged tables (broadcast).  NG: guard count (-1: any, up to
 // LTB_MAXG, through a runtime loop).
-template <int NG, bool along_r>
+template <int NG, bool along_r, bool off32>
 __device__ __forceinline__ void gather_fill(const LtbPackJob& J, const PackTables& tb,
                                             float (*sm)[PR + 1], int64_t rlim, int64_t klim,
                                             int ng) {
@@ -398,7 +399,9 @@ __device__ __forceinline__ void gather_fill(const LtbPackJob& J, const PackTable
   const int tid = threadIdx.x;
   const int fixed = tid & 63;
   const bool fok = fixed < (along_r ? rlim : klim);
-  const int64_t fo = along_r ? tb.roff[fixed] : tb.koff[fixed];
+  const int64_t fo = off32 ? (int64_t)(along_r ? tb.roff32[fixed] : tb.koff32[fixed])
+                           : (along_r ? tb.roff[fixed] : tb.koff[fixed]);
+  const int32_t fo32 = (int32_t)fo;
   const int vlim = (int)(along_r ? klim : rlim);
   int32_t fg[G > 0 ? G : 1], ub[G > 0 ? G : 1];
 #pragma unroll
@@ -407,22 +410,33 @@ __device__ __forceinline__ void gather_fill(const LtbPackJob& J, const PackTable
     fg[g] = on ? (along_r ? tb.grow[g][fixed] : tb.gk[g][fixed]) : 0;
     ub[g] = on ? tb.gub[g] : 1;  // off: 0 <= 0 + 0 < 1 always holds
   }
-#pragma unroll 4
+  // all 16 gathers issue before any shared-memory store (loads in flight)
+  float v[16];
+#pragma unroll
   for (int q = 0; q < 16; ++q) {
     const int v_ = (tid >> 6) + 4 * q;  // the varying side (warp-uniform)
-    float v = 0.f;
+    v[q] = 0.f;
     if (fok && v_ < vlim) {
       bool ok = true;
 #pragma unroll
-      for (int g = 0; g < G; ++g) {
+      for (int g = 0; g < G; ++g) {  // 0 <= w < ub as one unsigned compare
         const int32_t o = NG >= 0 || g < ng ? (along_r ? tb.gk[g][v_] : tb.grow[g][v_]) : 0;
-        const int32_t w = fg[g] + o;
-        ok = ok && w >= 0 && w < ub[g];
+        ok = ok && (uint32_t)(fg[g] + o) < (uint32_t)ub[g];
       }
-      if (ok) v = __ldg(J.op.base + fo + (along_r ? tb.koff[v_] : tb.roff[v_]));
+      if (ok) {
+        if (off32)
+          v[q] = __ldg(J.op.base +
+                       (uint32_t)(fo32 + (along_r ? tb.koff32[v_] : tb.roff32[v_])));
+        else
+          v[q] = __ldg(J.op.base + fo + (along_r ? tb.koff[v_] : tb.roff[v_]));
+      }
     }
-    if (along_r) sm[v_][fixed] = v;
-    else sm[fixed][v_] = v;
+  }
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int v_ = (tid >> 6) + 4 * q;
+    if (along_r) sm[v_][fixed] = v[q];
+    else sm[fixed][v_] = v[q];
   }
 }
 
@@ -470,12 +484,14 @@ __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
         const int64_t k = k0 + tid;
         const bool ok = k < J.K;
         tb.koff[tid] = !ok ? 0 : J.op.dense ? k * J.op.ld_k : J.op.koff[k];
+        tb.koff32[tid] = (int32_t)tb.koff[tid];
         for (int g = 0; g < ng; ++g) tb.gk[g][tid] = ok ? J.op.gk[(int64_t)g * J.K + k] : 0;
       } else if (tid < 128) {
         const int rl = tid - 64;
         const int64_t r = r0 + rl;
         const bool ok = r < J.rows;
         tb.roff[rl] = !ok ? 0 : J.op.dense ? r * J.op.ld_row : J.op.rowoff[r];
+        tb.roff32[rl] = (int32_t)tb.roff[rl];
         for (int g = 0; g < ng; ++g) tb.grow[g][rl] = ok ? J.op.grow[(int64_t)g * J.rows + r] : 0;
       } else if (tid < 128 + LTB_MAXG) {
         if (tid - 128 < ng) tb.gub[tid - 128] = J.op.gub[tid - 128];
@@ -483,19 +499,27 @@ __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
       __syncthreads();
       const int64_t rlim = J.rows - r0, klim = J.K - k0;
       const bool along_r = J.mode == kPackGatherR;
-#define LTB_GATHER(AR)                                                    \
-  switch (ng) { /* guard count known at compile time: no predicated loop */ \
-    case 0: gather_fill<0, AR>(J, tb, sm, rlim, klim, ng); break;          \
-    case 1: gather_fill<1, AR>(J, tb, sm, rlim, klim, ng); break;          \
-    case 2: gather_fill<2, AR>(J, tb, sm, rlim, klim, ng); break;          \
-    case 3: gather_fill<3, AR>(J, tb, sm, rlim, klim, ng); break;          \
-    case 4: gather_fill<4, AR>(J, tb, sm, rlim, klim, ng); break;          \
-    default: gather_fill<-1, AR>(J, tb, sm, rlim, klim, ng); break;        \
+#define LTB_GATHER(AR, O32)                                                    \
+  switch (ng) { /* guard count known at compile time: no predicated loop */      \
+    case 0: gather_fill<0, AR, O32>(J, tb, sm, rlim, klim, ng); break;          \
+    case 1: gather_fill<1, AR, O32>(J, tb, sm, rlim, klim, ng); break;          \
+    case 2: gather_fill<2, AR, O32>(J, tb, sm, rlim, klim, ng); break;          \
+    case 3: gather_fill<3, AR, O32>(J, tb, sm, rlim, klim, ng); break;          \
+    case 4: gather_fill<4, AR, O32>(J, tb, sm, rlim, klim, ng); break;          \
+    default: gather_fill<-1, AR, O32>(J, tb, sm, rlim, klim, ng); break;        \
   }
       if (along_r) {
-        LTB_GATHER(true)
+        if (J.off32) {
+          LTB_GATHER(true, true)
+        } else {
+          LTB_GATHER(true, false)
+        }
       } else {
-        LTB_GATHER(false)
+        if (J.off32) {
+          LTB_GATHER(false, true)
+        } else {
+          LTB_GATHER(false, false)
+        }
       }
 #undef LTB_GATHER
     }
@@ -544,27 +568,44 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
     k_pack_grouped(const LtbPackJob* __restrict__ jobs, int njobs, int64_t total_tiles) {
   __shared__ float sm[PKT][PR + 1];
   __shared__ PackTables tabs;
-  int64_t t0, t1;
-  tile_range(total_tiles, t0, t1);
-  if (t0 >= t1) return;
   __shared__ LtbPackJob sj;  // the current job, read from shared memory
+  // chunks of kGroupChunk consecutive tiles dealt round-robin to the CTAs:
+  // every CTA sees a mix of the jobs (fast and slow layouts alike), and its
+  // tile indices only grow, so the job index only moves forward
+  constexpr int kGroupChunk = 4;
+  const int64_t nchunks = (total_tiles + kGroupChunk - 1) / kGroupChunk;
+  int64_t ch = blockIdx.x;
+  if (ch >= nchunks) return;
   int j = 0, hi = njobs - 1, cur = -1;
+  const int64_t t_first = ch * kGroupChunk;
   while (j < hi) {
     const int mid = (j + hi + 1) >> 1;
-    if (jobs[mid].tile_start <= t0) j = mid;
+    if (jobs[mid].tile_start <= t_first) j = mid;
     else hi = mid - 1;
   }
-  for (int64_t t = t0; t < t1; ++t) {
-    while (j + 1 < njobs && jobs[j + 1].tile_start <= t) ++j;
-    if (j != cur) {  // uniform across the block
-      __syncthreads();
-      const uint64_t* src = reinterpret_cast<const uint64_t*>(jobs + j);
-      for (int i = threadIdx.x; i < (int)(sizeof(LtbPackJob) / 8); i += PACK_THREADS)
-        reinterpret_cast<uint64_t*>(&sj)[i] = src[i];
-      __syncthreads();
-      cur = j;
+  for (; ch < nchunks; ch += gridDim.x) {
+    const int64_t t1 = (ch + 1) * kGroupChunk < total_tiles ? (ch + 1) * kGroupChunk
+                                                             : total_tiles;
+    for (int64_t t = ch * kGroupChunk; t < t1; ++t) {
+      if (j + 1 < njobs && jobs[j + 1].tile_start <= t) {  // skip ahead (binary search)
+        int lo = j + 1, h2 = njobs - 1;
+        while (lo < h2) {
+          const int mid = (lo + h2 + 1) >> 1;
+          if (jobs[mid].tile_start <= t) lo = mid;
+          else h2 = mid - 1;
+        }
+        j = lo;
+      }
+      if (j != cur) {  // uniform across the block
+        __syncthreads();
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(jobs + j);
+        for (int i = threadIdx.x; i < (int)(sizeof(LtbPackJob) / 8); i += PACK_THREADS)
+          reinterpret_cast<uint64_t*>(&sj)[i] = src[i];
+        __syncthreads();
+        cur = j;
+      }
+      pack_tile(sj, t - sj.tile_start, sm, &tabs);
     }
-    pack_tile(sj, t - sj.tile_start, sm, &tabs);
   }
 }
 
@@ -618,7 +659,7 @@ static int64_t pack_grid(int64_t tiles, int sms) {
 }
 
 cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
-                            int64_t Kp, int nseg, int seg_mask, int k_contig, int sms,
+                            int64_t Kp, int nseg, int seg_mask, int k_contig, int off32, int sms,
                             cudaStream_t st) {
   LtbPackJob J{};
   J.op = op;
@@ -630,6 +671,7 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
   J.nseg = nseg;
   J.seg_mask = seg_mask;
   J.mode = ltb_pack_mode(op, rows, K, k_contig);
+  J.off32 = off32;
   const int64_t tiles = ltb_pack_tiles(rows, K);
   if (tiles == 0) return cudaSuccess;
   k_pack_one<<<(unsigned)pack_grid(tiles, sms), PACK_THREADS, 0, st>>>(J, tiles);

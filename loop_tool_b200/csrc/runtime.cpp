@@ -85,6 +85,7 @@ struct GemmTables {
   int a_slot = -1, b_slot = -1;       // scratch slots of the packed operands
   LtbTcProblem prob{};                // launch template (maps/c bound per run)
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
+  bool a_off32 = false, b_off32 = false;  // operand offsets fit in int32
   int bn = 256;                       // tensor-core tile width (128 or 256)
   int epi = 0;                        // 1: shared-memory transposed epilogue
 };
@@ -256,6 +257,14 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     t.b_dense = B.ng == 0 && rb[0] == 0 && arith(rb, &t.b_ldr) && arith(ktab_b, &t.b_ldk);
     t.a_kcontig = unit_frac(ktab_a) >= unit_frac(ra);
     t.b_kcontig = unit_frac(ktab_b) >= unit_frac(rb);
+    auto maxabs = [](const std::vector<int64_t>& v) {
+      int64_t m = 0;
+      for (auto x : v) m = std::max<int64_t>(m, x < 0 ? -x : x);
+      return m;
+    };
+    const int64_t lim = int64_t(1) << 31;
+    t.a_off32 = maxabs(ra) + maxabs(ktab_a) < lim;
+    t.b_off32 = maxabs(rb) + maxabs(ktab_b) < lim;
   }
   auto ctab = table(nd, d.out_coef, 0);
   t.unit_cols = true;
@@ -433,9 +442,11 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         }
         void* ap = bt.p[t.a_slot];
         void* bp = bt.p[t.b_slot];
-        e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, c->sms, st);
+        e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, t.a_off32,
+                            c->sms, st);
         if (e == cudaSuccess)
-          e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, c->sms, st);
+          e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, t.b_off32,
+                              c->sms, st);
         alignas(64) unsigned char maps[256];
         if (e == cudaSuccess) e = ltb_make_tmap(maps, ap, p.M, t.Kp, ltb_tc_tile_m());
         if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, t.bn);
@@ -801,7 +812,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
       p.K = s.con.K;
       b->flops += 2.0 * p.M * p.N * p.K;
       if (b->tc) {
-        auto job = [&](const LtbGemmOperand& op, int64_t rows, void* dst, int mask, bool kc) {
+        auto job = [&](const LtbGemmOperand& op, int64_t rows, void* dst, int mask, bool kc,
+                       bool off32) {
           LtbPackJob j{};
           j.op = op;
           j.out = dst;
@@ -813,6 +825,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
           j.nseg = t.nseg;
           j.seg_mask = mask;
           j.mode = ltb_pack_mode(op, rows, p.K, kc ? 1 : 0);
+          j.off32 = off32 ? 1 : 0;
           b->pack_tiles += ltb_pack_tiles(rows, p.K);
           jobs.push_back(j);
         };
@@ -821,8 +834,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         b->owned.push_back(ap);
         CUDA_TRY(cudaMalloc(&bp, (size_t)p.N * t.Kp * 2));
         b->owned.push_back(bp);
-        job(p.a, p.M, ap, t.a_mask, t.a_kcontig);
-        job(p.b, p.N, bp, t.b_mask, t.b_kcontig);
+        job(p.a, p.M, ap, t.a_mask, t.a_kcontig, t.a_off32);
+        job(p.b, p.N, bp, t.b_mask, t.b_kcontig, t.b_off32);
         const int grp = (t.bn == 256 ? 2 : 0) + t.epi;
         auto& mv = maps[grp];
         mv.resize(mv.size() + 256);

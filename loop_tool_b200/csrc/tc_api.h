@@ -33,6 +33,8 @@ struct LtbPackJob {
   int tiles_k;          // ceil(K / 64)
   int nseg, seg_mask;
   int mode;             // kPack*
+  int off32;            // every element offset of the operand fits in int32
+  int pad_;
 };
 int ltb_pack_mode(const LtbGemmOperand& op, int64_t rows, int64_t K, int k_contig);
 int64_t ltb_pack_tiles(int64_t rows, int64_t K);
@@ -45,8 +47,10 @@ cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t
 cudaError_t ltb_make_tmap(void* map, const void* base, int64_t rows, int64_t Kp, int box_rows);
 
 // FP32 operand -> BF16 K-major segments (hi / lo split per segment).
+// off32: every element offset (rowoff[r] + koff[k], both >= 0) is below 2^31,
+// so the gather adds 32-bit offsets.
 cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
-                            int64_t Kp, int nseg, int seg_mask, int k_contig, int sms,
+                            int64_t Kp, int nseg, int seg_mask, int k_contig, int off32, int sms,
                             cudaStream_t st);
 
 // Persistent grouped launch over every tile of every problem

@@ -11,6 +11,7 @@
 #include <loop_tool/hardware.h>
 #include <loop_tool/serialization.h>
 
+#include <cstdlib>
 #include <memory>
 #include <string>
 #include <vector>
@@ -23,6 +24,16 @@ const char* options() {
   // e.g. LOOP_TOOL_B200_OPTIONS="precision=bf16x3"
   const char* o = std::getenv("LOOP_TOOL_B200_OPTIONS");
   return o ? o : "";
+}
+
+// Schedule cache file (LOOP_TOOL_B200_SCHEDULES): loaded at registration so
+// compiles of loop trees tuned before start from their tuned schedules; with
+// LOOP_TOOL_B200_AUTOTUNE=1 the first run of every new loop tree is tuned
+// (on its own buffers) and the file rewritten.
+const char* schedule_file() { return std::getenv("LOOP_TOOL_B200_SCHEDULES"); }
+bool autotune() {
+  const char* a = std::getenv("LOOP_TOOL_B200_AUTOTUNE");
+  return a && std::string(a) == "1";
 }
 
 // CudaGPUHardware (cuda.cpp:800-816): managed memory, usable by the CPU too.
@@ -56,6 +67,17 @@ struct B200Compiled : public loop_tool::Compiled {
   }
   ~B200Compiled() override { ltb_release(h); }
   void run(const std::vector<void*>& memory, bool sync) const override {
+    int64_t tuned = 1;
+    ltb_int_property(h, "tuned", &tuned);
+    if (!tuned && autotune()) {
+      // tuning needs device-visible buffers (managed memory from the "cuda"
+      // hardware qualifies); it leaves the outputs computed
+      if (ltb_tune(h, memory.data(), (int)memory.size(), nullptr, 5, nullptr, 0) == LTB_OK) {
+        if (const char* f = schedule_file()) ltb_tune_save(f);
+        if (sync) ltb_synchronize(nullptr);
+        return;
+      }
+    }
     ASSERT(ltb_run(h, memory.data(), (int)memory.size(), sync ? 1 : 0, nullptr) == LTB_OK)
         << ltb_last_error();
   }
@@ -75,6 +97,7 @@ struct B200Backend : public loop_tool::Backend {
 struct Registration {
   Registration() {
     if (ltb_device_count() == 0) return;
+    if (const char* f = schedule_file()) ltb_tune_load(f);  // absent file: start empty
     auto hw = std::make_shared<B200Hardware>();
     loop_tool::registerHardware(hw);
     loop_tool::registerBackend(std::make_shared<B200Backend>(hw->id()));

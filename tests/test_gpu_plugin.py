@@ -44,3 +44,32 @@ def test_reference_frontend_drives_b200(name, cuda_dev):
         assert_parity(got, case["expected"], True, what=name)
     else:
         assert_accuracy(got, case["expected"], fp64_oracle(case), what=name)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["softmax_16x4096", "add_4099", "maxpool_specials"])
+def test_plugin_autotunes_and_persists_schedules(name, cuda_dev):
+    """LOOP_TOOL_B200_AUTOTUNE=1: the first run of a loop tree through the
+    reference frontend tunes it (outputs still exact / accurate) and writes
+    the schedule file; a second process loads the file at registration."""
+    if not (os.path.exists(HARNESS) and os.path.exists(PLUGIN)):
+        pytest.skip("reference CPU build (oracle/_ref) not present")
+    case = load(name)
+    with tempfile.TemporaryDirectory() as td:
+        for i, a in enumerate(case["inputs"]):
+            a.tofile(os.path.join(td, f"in{i}.f32"))
+        sched = os.path.join(td, "schedules.txt")
+        env = dict(os.environ, LT_PLUGIN=PLUGIN, LOOP_TOOL_B200_AUTOTUNE="1",
+                   LOOP_TOOL_B200_SCHEDULES=sched)
+        for _ in range(2):
+            r = subprocess.run([HARNESS, "lazyrun", td, td, case["program"],
+                                *map(str, case["params"])], env=env, capture_output=True,
+                               text=True)
+            assert r.returncode == 0, r.stderr
+            got = np.fromfile(os.path.join(td, "out0.f32"), dtype=np.float32)
+            if case["program"] in EXACT_PROGRAMS:
+                assert_parity(got, case["expected"], True, what=name)
+            else:
+                assert_accuracy(got, case["expected"], fp64_oracle(case), what=name)
+            text = open(sched, "rb").read()
+            assert text.startswith(b"loop_tool_b200 schedules 1\n") and b"\nentry " in text
