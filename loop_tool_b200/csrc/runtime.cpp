@@ -305,22 +305,43 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
   }
 }
 
-void compile_device(ltb_compiled* c) {
-  CUDA_TRY(cudaGetDevice(&c->device));
-  CUDA_TRY(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device));
+// Per-device facts, queried once per process and device (compiles are
+// frequent in a serving loop: every new size is a new loop tree).
+struct DeviceInfo {
+  bool ready = false;
+  int sms = 0;
+  int64_t bandwidth_gbs = 0;
+};
+
+const DeviceInfo& device_info(int dev) {
+  static std::mutex mu;
+  static std::map<int, DeviceInfo> info;
+  std::lock_guard<std::mutex> g(mu);
+  DeviceInfo& d = info[dev];
+  if (d.ready) return d;
+  CUDA_TRY(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
   int memclk_khz = 0, bus_bits = 0;
-  cudaDeviceGetAttribute(&memclk_khz, cudaDevAttrMemoryClockRate, c->device);
-  cudaDeviceGetAttribute(&bus_bits, cudaDevAttrGlobalMemoryBusWidth, c->device);
+  cudaDeviceGetAttribute(&memclk_khz, cudaDevAttrMemoryClockRate, dev);
+  cudaDeviceGetAttribute(&bus_bits, cudaDevAttrGlobalMemoryBusWidth, dev);
   cudaGetLastError();
-  c->bandwidth_gbs = (int64_t)(2.0 * memclk_khz * 1e3 * (bus_bits / 8) / 1e9);
+  d.bandwidth_gbs = (int64_t)(2.0 * memclk_khz * 1e3 * (bus_bits / 8) / 1e9);
   // host buffers are staged through the stream-ordered pool; keep what it
   // reserved across synchronisations instead of unmapping it every time
   cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) {
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   cudaGetLastError();
+  d.ready = true;
+  return d;
+}
+
+void compile_device(ltb_compiled* c) {
+  CUDA_TRY(cudaGetDevice(&c->device));
+  const DeviceInfo& di = device_info(c->device);
+  c->sms = di.sms;
+  c->bandwidth_gbs = di.bandwidth_gbs;
   auto& P = c->plan;
   const int ns = (int)P.stages.size();
   c->split_of.assign(ns, 1);
@@ -993,17 +1014,24 @@ int ltb_batch_release(ltb_batch* b) {
 const char* ltb_last_error(void) { return g_err.c_str(); }
 
 int ltb_device_count(void) {
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+  // the set of visible devices is fixed for the life of the process
+  static const int count = [] {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    int ok = 0;
+    for (int i = 0; i < n; ++i) {
+      int major = 0;
+      if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, i) == cudaSuccess &&
+          major == 10)
+        ok++;
+    }
     cudaGetLastError();
-    return 0;
-  }
-  int ok = 0;
-  for (int i = 0; i < n; ++i) {
-    cudaDeviceProp p{};
-    if (cudaGetDeviceProperties(&p, i) == cudaSuccess && p.major == 10) ok++;
-  }
-  return ok;
+    return ok;
+  }();
+  return count;
 }
 
 int ltb_plan(const char* ir_text, const char* options, char* buf, size_t len) {

@@ -6,9 +6,9 @@ symbolic sizes.  The loop:
     (inputs + output + scratch, from the compiled plan) fit the HBM budget;
     requests that arrive while others run are admitted in arrival order as
     slots and memory free up, so their kernels overlap on the device;
-  * reuses compiled loop trees through the IR-text kernel cache
-    (loop_tool_b200.lazy.compiled), one entry per distinct program + sizes
-    (the reference's lazy cache is keyed the same way, lazy.h:82-115);
+  * reuses compiled loop trees through its kernel cache, one entry per
+    distinct program + sizes (the reference's lazy cache is keyed the same
+    way, lazy.h:82-115), applying any autotuned schedule cached for the IR;
   * keeps every buffer device-resident: inputs are produced on the device,
     buffers come from torch's stream-ordered caching allocator, and each run
     gets its own scratch (ltb_run_with_scratch), so concurrent runs of one
@@ -26,6 +26,7 @@ import numpy as np
 
 from . import lazy as lt
 from . import nn
+from .backend import Compiled
 
 KINDS = ("matmul", "conv", "softmax")
 
@@ -121,18 +122,19 @@ class Server:
         self.used = 0
         self.precision = precision
         self.keep = keep_outputs
-        self._ir = {}
+        self._kernels = {}
         self.compiles = 0
 
     def _compiled(self, req):
+        """The request's compiled loop tree from the server's own kernel
+        cache: one entry per distinct program and sizes, never evicted (a
+        trace of 20,000 requests holds ~14,000 distinct programs)."""
         key = (req.kind, req.params)
-        text = self._ir.get(key)
-        if text is None:
-            text = _program(req.kind, req.params).ir
-            self._ir[key] = text
-        before = lt.cache_info()["entries"]
-        c = lt.compiled(text, precision=self.precision)
-        self.compiles += lt.cache_info()["entries"] > before
+        c = self._kernels.get(key)
+        if c is None:
+            c = Compiled(_program(req.kind, req.params).ir, precision=self.precision)
+            self._kernels[key] = c
+            self.compiles += 1
         return c
 
     def _workspace(self, slot, floats):
