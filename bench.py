@@ -472,13 +472,14 @@ def extra_c4(dev):
     big = {"workload": "8192^3 matmul"}
     for prec in ("bf16", "bf16x3"):
         c1 = ltb.Compiled(ir, precision=prec)
-        c1.tune([A, B, C], reps=2)
-        b1 = ltb.Batch([(c1, [A, B, C])])
+        b1, _, sched = ltb.tune_batch([(c1, [A, B, C])], reps=2)
         b1.run_timed()
         pack_ms, gemm_ms = b1.run_timed()
         products = {"bf16": 1, "bf16x3": 3}[prec]
         big[prec] = {"total_ms": pack_ms + gemm_ms, "pack_ms": pack_ms, "gemm_ms": gemm_ms,
                      "tile_variant": c1.schedule(0)[2],
+                     "pack_schedule": [b1.int_property("pack_chunk"),
+                                       b1.int_property("pack_cta_per_sm")],
                      "tflops_total": 2 * n ** 3 / ((pack_ms + gemm_ms) * 1e-3) / 1e12,
                      "tensor_tflops_gemm": products * 2 * n ** 3 / (gemm_ms * 1e-3) / 1e12,
                      "frac_of_measured_bf16_peak": products * 2 * n ** 3 / (gemm_ms * 1e-3) /

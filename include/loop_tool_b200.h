@@ -117,8 +117,13 @@ int ltb_batch_run(ltb_batch* b, int sync, void* stream);
 /* One eager run with device timings of its two phases (operand packing and
  * the grouped GEMM), measured with CUDA events on `stream`; synchronises. */
 int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_ms);
+/* Launch shape of the batch's grouped operand packing: tiles dealt to the
+ * CTAs in round-robin chunks of pack_chunk consecutive 64x64 tiles, grid =
+ * SMs x pack_cta_per_sm (0: the defaults, 4 and 4).  Drops a captured graph
+ * (capture again). */
+int ltb_batch_set_schedule(ltb_batch* b, int pack_chunk, int pack_cta_per_sm);
 /* "problems", "flops", "launches", "tiles", "tiles_128", "tiles_256",
- * "graph". */
+ * "graph", "pack_chunk", "pack_cta_per_sm". */
 int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value);
 int ltb_batch_release(ltb_batch* b);
 

@@ -189,9 +189,10 @@ def tune_batch(members, capture_stream=None, reps=3):
     launch (operand packing + persistent GEMMs) under each policy: the
     members' current schedules, every problem at one variant (128 or 256
     columns, each with either epilogue), and each member's own tuned
-    variant.  The best policy is left on the members,
-    recorded in the schedule cache, and returned with its Batch and a
-    report."""
+    variant.  The best policy is left on the members and recorded in the
+    schedule cache; the grouped packing's launch shape is then timed the
+    same way.  Returns the Batch (captured on capture_stream if given), the
+    tile policy and a report."""
     policies = {"current": [c.schedule(0) for c, _ in members]}
     for v in (128, 129, 256, 257):  # tile width, +1: transposed epilogue
         policies[f"all_{v}"] = [(0, 0, v)] * len(members)
@@ -214,7 +215,23 @@ def tune_batch(members, capture_stream=None, reps=3):
         c.set_schedule(0, *sc)
         c.record_schedule()
     report = "; ".join(f"{k} {v:.3f} ms" for k, v in times.items()) + f" -> {best}"
-    return Batch(members, capture_stream=capture_stream), best, report
+    # then the grouped packing's launch shape (chunk of tiles, CTAs per SM)
+    b = Batch(members)
+    pack = {}
+    for chunk, per_sm in ((4, 4), (1, 4), (16, 4), (64, 4), (16, 2), (64, 8)):
+        b.set_schedule(chunk, per_sm)
+        b.run_timed()
+        pack[(chunk, per_sm)] = min(b.run_timed()[0] for _ in range(reps))
+    del b
+    pbest = min(pack, key=pack.get)
+    report += "; pack " + ", ".join(f"{k[0]}x{k[1]} {v:.3f} ms" for k, v in pack.items()) + \
+        f" -> chunk {pbest[0]}, {pbest[1]}/SM"
+    out = Batch(members)
+    out.set_schedule(*pbest)
+    if capture_stream is not None:
+        out._capture_stream = capture_stream
+        _lib.check(_lib.lib().ltb_batch_capture(out._h, capture_stream))
+    return out, best, report
 
 
 def tune_save(path):
@@ -277,8 +294,17 @@ class Batch:
         h = ctypes.c_void_p()
         _lib.check(_lib.lib().ltb_batch_create(hs, mem, n, ctypes.byref(h)))
         self._h = h
+        self._capture_stream = capture_stream
         if capture_stream is not None:
             _lib.check(_lib.lib().ltb_batch_capture(h, capture_stream))
+
+    def set_schedule(self, pack_chunk=0, pack_cta_per_sm=0):
+        """Launch shape of the grouped operand packing (0: defaults); a
+        captured graph is captured again."""
+        _lib.check(_lib.lib().ltb_batch_set_schedule(self._h, int(pack_chunk),
+                                                      int(pack_cta_per_sm)))
+        if self._capture_stream is not None:
+            _lib.check(_lib.lib().ltb_batch_capture(self._h, self._capture_stream))
 
     def run(self, sync=True, stream=None):
         if stream is None:

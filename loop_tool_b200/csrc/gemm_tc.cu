@@ -565,14 +565,14 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
 // Every operand of a batch in one launch; the job of a tile is found by
 // binary search on tile_start once per CTA, then by stepping forward.
 __global__ void __launch_bounds__(PACK_THREADS, 4)
-    k_pack_grouped(const LtbPackJob* __restrict__ jobs, int njobs, int64_t total_tiles) {
+    k_pack_grouped(const LtbPackJob* __restrict__ jobs, int njobs, int64_t total_tiles,
+                   int kGroupChunk) {
   __shared__ float sm[PKT][PR + 1];
   __shared__ PackTables tabs;
   __shared__ LtbPackJob sj;  // the current job, read from shared memory
   // chunks of kGroupChunk consecutive tiles dealt round-robin to the CTAs:
   // every CTA sees a mix of the jobs (fast and slow layouts alike), and its
   // tile indices only grow, so the job index only moves forward
-  constexpr int kGroupChunk = 4;
   const int64_t nchunks = (total_tiles + kGroupChunk - 1) / kGroupChunk;
   int64_t ch = blockIdx.x;
   if (ch >= nchunks) return;
@@ -679,10 +679,13 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
 }
 
 cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t total_tiles,
-                                    int sms, cudaStream_t st) {
+                                    int sms, cudaStream_t st, int chunk, int cta_per_sm) {
   if (total_tiles == 0) return cudaSuccess;
-  k_pack_grouped<<<(unsigned)pack_grid(total_tiles, sms), PACK_THREADS, 0, st>>>(
-      d_jobs, njobs, total_tiles);
+  if (chunk < 1) chunk = 4;
+  const int64_t chunks = (total_tiles + chunk - 1) / chunk;
+  const int64_t cap = (int64_t)sms * (cta_per_sm > 0 ? cta_per_sm : 4);
+  const int64_t grid = chunks < cap ? chunks : cap;
+  k_pack_grouped<<<(unsigned)grid, PACK_THREADS, 0, st>>>(d_jobs, njobs, total_tiles, chunk);
   return cudaGetLastError();
 }
 

@@ -735,6 +735,7 @@ struct ltb_batch {
   LtbPackJob* d_jobs = nullptr;
   int njobs = 0;
   int64_t pack_tiles = 0;
+  int pack_chunk = 0, pack_cta_per_sm = 0;  // grouped pack schedule (0: defaults)
   // tensor-core problems grouped by schedule variant (group 2 * (tile width
   // == 256) + transposed epilogue), one persistent launch per non-empty group
   LtbTcProblem* d_tc[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -762,7 +763,8 @@ void batch_gemms(ltb_batch* b, cudaStream_t st) {
 
 void batch_launch(ltb_batch* b, cudaStream_t st) {
   if (b->tc) {
-    CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st));
+    CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st, b->pack_chunk,
+                                     b->pack_cta_per_sm));
     batch_gemms(b, st);
   } else {
     CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles, st));
@@ -963,7 +965,8 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
     CUDA_TRY(cudaEventCreate(&e1));
     CUDA_TRY(cudaEventCreate(&e2));
     CUDA_TRY(cudaEventRecord(e0, st));
-    if (b->tc) CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st));
+    if (b->tc) CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st, b->pack_chunk,
+                                     b->pack_cta_per_sm));
     CUDA_TRY(cudaEventRecord(e1, st));
     if (b->tc)
       batch_gemms(b, st);
@@ -985,6 +988,20 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
   return batch_finish(b, 1, st);
 }
 
+int ltb_batch_set_schedule(ltb_batch* b, int pack_chunk, int pack_cta_per_sm) {
+  if (!b || pack_chunk < 0 || pack_chunk > 4096 || pack_cta_per_sm < 0 || pack_cta_per_sm > 64)
+    return fail(LTB_ERR_INVALID, "bad batch schedule");
+  b->pack_chunk = pack_chunk;
+  b->pack_cta_per_sm = pack_cta_per_sm;
+  if (b->exec) {  // the captured graph holds the old launch shape
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  return LTB_OK;
+}
+
 int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   if (!b || !name || !value) return fail(LTB_ERR_INVALID, "null argument");
   std::string k = name;
@@ -998,6 +1015,8 @@ int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   else if (k == "tiles_128") *value = b->tc_tiles[0] + b->tc_tiles[1];
   else if (k == "tiles_256") *value = b->tc_tiles[2] + b->tc_tiles[3];
   else if (k == "graph") *value = b->exec ? 1 : 0;
+  else if (k == "pack_chunk") *value = b->pack_chunk ? b->pack_chunk : 4;
+  else if (k == "pack_cta_per_sm") *value = b->pack_cta_per_sm ? b->pack_cta_per_sm : 4;
   else return fail(LTB_ERR_INVALID, "unknown property " + k);
   return LTB_OK;
 }

@@ -48,3 +48,36 @@ def test_batch_of_uneven_matmuls(precision, cuda_dev):
         assert np.isfinite(got).all(), f"{(M, N, K)}: unwritten outputs"
         err = np.linalg.norm(got - exact) / np.linalg.norm(exact)
         assert err <= TOL[precision], f"{(M, N, K)} {precision}: normwise error {err:.3g}"
+
+
+@pytest.mark.gpu
+def test_pack_schedules_agree_bit_for_bit(cuda_dev):
+    """Every launch shape of the grouped operand packing (tile chunk dealt
+    per CTA, CTAs per SM) packs the same bits: results are identical."""
+    import torch
+
+    import loop_tool_b200 as ltb
+
+    sizes = uneven_sizes(12, 16, 700, seed=402)
+    g = torch.Generator(device=cuda_dev).manual_seed(6)
+    members = []
+    for M, N, K in sizes:
+        T, _ = mm(M, K, N)
+        members.append((ltb.Compiled(T.ir, precision="bf16x3"),
+                        [torch.randn(M * K, device=cuda_dev, generator=g),
+                         torch.randn(K * N, device=cuda_dev, generator=g),
+                         torch.empty(M * N, device=cuda_dev)]))
+    stream = torch.cuda.Stream()
+    b = ltb.Batch(members, capture_stream=stream.cuda_stream)
+    b.run(stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    ref = [C.clone() for _, (_, _, C) in members]
+    for chunk, per_sm in ((1, 4), (16, 2), (64, 8), (3, 1)):
+        b.set_schedule(chunk, per_sm)
+        assert b.int_property("graph") == 1 and b.int_property("pack_chunk") == chunk
+        for _, (_, _, C) in members:
+            C.fill_(float("nan"))
+        b.run(stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        for r, (_, (_, _, C)) in zip(ref, members):
+            assert torch.equal(r, C), (chunk, per_sm)
