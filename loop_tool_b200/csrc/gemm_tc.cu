@@ -120,17 +120,17 @@ __device__ __forceinline__ int find_problem(const LtbTcProblem* __restrict__ P, 
   return lo;
 }
 
-// Grouped raster: tiles advance along M in groups of kGroupM row blocks, so
-// the ~148 tiles in flight cover a compact 16 x 9 block region whose A and
-// B panels stay resident in L2.
-constexpr int kGroupM = 16;
+// Grouped raster: tiles advance along M in groups of group_m row blocks (a
+// per-problem schedule, 16 by default), so the ~148 tiles in flight cover a
+// compact block region whose A and B panels stay resident in L2.
 template <int BN>
 __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, int* m0, int* n0) {
-  const int64_t per_group = (int64_t)kGroupM * p.tiles_n;
+  const int gmax = p.group_m > 0 ? p.group_m : 16;
+  const int64_t per_group = (int64_t)gmax * p.tiles_n;
   const int g = (int)(lt / per_group);
   const int idx = (int)(lt - (int64_t)g * per_group);
-  const int gm = p.tiles_m - g * kGroupM < kGroupM ? p.tiles_m - g * kGroupM : kGroupM;
-  *m0 = (g * kGroupM + idx % gm) * BM;
+  const int gm = p.tiles_m - g * gmax < gmax ? p.tiles_m - g * gmax : gmax;
+  *m0 = (g * gmax + idx % gm) * BM;
   *n0 = (idx / gm) * BN;
 }
 
@@ -443,7 +443,16 @@ __device__ __forceinline__ void gather_fill(const LtbPackJob& J, const PackTable
 __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
                                           float (*sm)[PR + 1], PackTables* tabs) {
   const int tid = threadIdx.x;
-  const int64_t r0 = (lt / J.tiles_k) * PR, k0 = (lt % J.tiles_k) * PKT;
+  int64_t rt, kt;  // tile row / k indices (32-bit division when it fits)
+  if (lt <= 0xffffffffLL) {
+    const uint32_t q = (uint32_t)lt / (uint32_t)J.tiles_k;
+    rt = q;
+    kt = (uint32_t)lt - q * (uint32_t)J.tiles_k;
+  } else {
+    rt = lt / J.tiles_k;
+    kt = lt - rt * J.tiles_k;
+  }
+  const int64_t r0 = rt * PR, k0 = kt * PKT;
   if (J.mode == kPackDenseK) {
     float x[2][8];
 #pragma unroll
@@ -583,18 +592,22 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
     if (jobs[mid].tile_start <= t_first) j = mid;
     else hi = mid - 1;
   }
+  // first tile of the next job, kept in a register: the job table is read
+  // only when a job ends (streaming operand loads would evict it from L1)
+  int64_t next_start = j + 1 < njobs ? __ldg(&jobs[j + 1].tile_start) : total_tiles;
   for (; ch < nchunks; ch += gridDim.x) {
     const int64_t t1 = (ch + 1) * kGroupChunk < total_tiles ? (ch + 1) * kGroupChunk
                                                              : total_tiles;
     for (int64_t t = ch * kGroupChunk; t < t1; ++t) {
-      if (j + 1 < njobs && jobs[j + 1].tile_start <= t) {  // skip ahead (binary search)
+      if (t >= next_start) {  // skip ahead (binary search)
         int lo = j + 1, h2 = njobs - 1;
         while (lo < h2) {
           const int mid = (lo + h2 + 1) >> 1;
-          if (jobs[mid].tile_start <= t) lo = mid;
+          if (__ldg(&jobs[mid].tile_start) <= t) lo = mid;
           else h2 = mid - 1;
         }
         j = lo;
+        next_start = j + 1 < njobs ? __ldg(&jobs[j + 1].tile_start) : total_tiles;
       }
       if (j != cur) {  // uniform across the block
         __syncthreads();

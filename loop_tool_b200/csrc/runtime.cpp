@@ -506,6 +506,8 @@ void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
     const int epi = cfg.variant & 1;
     set_tile_n(c->gemms[g], bn, epi);
     c->cfg[i].variant = bn | epi;
+    // cta_per_sm of a contraction: the raster group (row blocks swept together)
+    c->gemms[g].prob.group_m = cfg.cta_per_sm;
   }
 }
 
@@ -631,7 +633,8 @@ std::string describe(ltb_compiled* c, int i) {
     const auto& t = c->gemms[c->gemm_of[i]];
     if (t.tc)
       o << "tile(128x" << t.bn << "x64) tensor_cores(tcgen05) parallel(persistent, "
-        << t.tiles << " tiles) epilogue(" << (t.epi ? "smem transpose" : "row stores") << ")";
+        << t.tiles << " tiles) raster(" << (t.prob.group_m ? t.prob.group_m : 16)
+        << " row blocks) epilogue(" << (t.epi ? "smem transpose" : "row stores") << ")";
     else
       o << "tile(128x128) cuda_cores";
     return o.str();
@@ -669,7 +672,8 @@ std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
     }
     case ltb::Family::contraction:
       if (c->gemms[c->gemm_of[i]].tc)
-        for (int v : {128, 129, 256, 257}) buf[n++] = LtbCfg{0, 0, v};
+        for (int v : {128, 129, 256, 257})
+          for (int gm : {0, 8, 32}) buf[n++] = LtbCfg{gm, 0, v};
       break;
   }
   return std::vector<LtbCfg>(buf, buf + n);

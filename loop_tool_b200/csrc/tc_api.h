@@ -18,6 +18,8 @@ struct LtbTcProblem {
   int M, N;
   int tiles_m, tiles_n;
   int unit_cols;         // ccol[j] == j
+  int group_m;           // raster: row blocks swept together (0: 16)
+  int pad_;
 };
 
 // Load modes of the operand packer (ltb_pack_mode picks one per operand).

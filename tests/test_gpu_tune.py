@@ -93,9 +93,10 @@ def test_tile_widths_agree(name, precision, cuda_dev):
     c = ltb.cuda(case["ir"], precision=precision)
     ins = [torch.from_numpy(a).to(cuda_dev) for a in case["inputs"]]
     stage = [i for i in range(c.int_property("stages")) if c.schedule(i)[2] in (128, 256)][0]
-    for bn in (128, 129, 256, 257):  # tile width, +1: shared-memory transposed epilogue
-        c.set_schedule(stage, variant=bn)
-        assert c.schedule(stage)[2] == bn
+    # tile width (+1: shared-memory transposed epilogue) x raster group
+    for bn, gm in ((128, 0), (129, 8), (256, 32), (257, 0), (256, 1)):
+        c.set_schedule(stage, cta_per_sm=gm, variant=bn)
+        assert c.schedule(stage) == (gm, 0, bn)
         out = torch.full((c.io_sizes[-1],), float("nan"), device=cuda_dev)
         c(ins + [out])
         torch.cuda.synchronize()
