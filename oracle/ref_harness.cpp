@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cstdio>
 #include <fstream>
+#include <thread>
 #include <iostream>
 #include <sstream>
 #include <string>
@@ -337,6 +338,10 @@ int main(int argc, char** argv) {
     }
     std::string backend = argv[3], in_dir = argv[4], out_dir = argv[5];
     int reps = argc > 6 ? std::atoi(argv[6]) : 0;
+    // optional start gate: after compiling and one untimed run, wait until
+    // this file exists before the timed reps, so that several concurrently
+    // started harness processes time their runs together
+    std::string gate = argc > 7 ? argv[7] : "";
     std::vector<std::vector<float>> bufs(n_in + n_out);
     std::vector<void*> mem;
     for (size_t i = 0; i < n_in + n_out; ++i) {
@@ -360,6 +365,11 @@ int main(int argc, char** argv) {
     }
     auto cc = loop_tool::getBackends().at(backend)->compile(lt);
     cc->run(mem, true);
+    if (!gate.empty()) {
+      std::ofstream(out_dir + "/ready").put('1');
+      for (int w = 0; w < 600000 && !std::ifstream(gate); ++w)  // at most 10 minutes
+        std::this_thread::sleep_for(std::chrono::milliseconds(1));
+    }
     if (reps > 0) {
       std::cout << "{\"seconds\": [";
       for (int r = 0; r < reps; ++r) {
