@@ -15,6 +15,10 @@
 //       Runs <program> through the lazy frontend itself (TensorImpl::data,
 //       lazy.h:219-260) with the default "cpp" backend: inputs are bound in
 //       getInputBuffers order (lazy.cpp:72-88), no serialize round trip.
+//   lt_ref_harness subtree <out_dir> <in_dir> <depth>[:backend] <program> <params...>
+//       Annotates the first loop at <depth> with "[cuda]" (or "[backend]") and runs the tree
+//       through the "cpu_interpreted" backend, which compiles that subtree
+//       with the "cuda" backend and calls it per enclosing iteration.
 //   lt_ref_harness tree <ir_file>      LoopTree::dump of the IR
 //   lt_ref_harness code <ir_file>      the C the "cpp" backend generates
 //   lt_ref_harness sizes <ir_file>     element counts of every I/O buffer
@@ -307,6 +311,56 @@ int main(int argc, char** argv) {
       std::ofstream f(out_dir + "/out0.f32", std::ios::binary);
       f.write(reinterpret_cast<const char*>(out),
               tsizes[tir.inputs().size()] * sizeof(float));
+      return 0;
+    }
+    if (mode == "subtree") {
+      // subtree <out_dir> <in_dir> <depth> <program> <params...>: annotate
+      // the first loop at <depth> with "[cuda]" and run the tree through
+      // the interpreter, which hands that subtree to the "cuda" backend
+      // (compile.cpp:273-417); inputs in the IR's input order
+      std::string out_dir = argv[2], in_dir = argv[3];
+      // <depth> or <depth>:<backend> (default backend "cuda")
+      const std::string da = argv[4];
+      const int depth = std::stoi(da.substr(0, da.find(':')));
+      const std::string sub_backend =
+          da.find(':') == std::string::npos ? "cuda" : da.substr(da.find(':') + 1);
+      std::vector<int64_t> params;
+      for (int i = 6; i < argc; ++i) params.emplace_back(std::stoll(argv[i]));
+      auto T = build(argv[5], params);
+      loop_tool::LoopTree base(T.ir());
+      loop_tool::LoopTree::TreeRef target = -1;
+      base.walk([&](loop_tool::LoopTree::TreeRef r, int d) {
+        if (target < 0 && d == depth && base.kind(r) == loop_tool::LoopTree::LOOP) target = r;
+      });
+      if (target < 0) {
+        std::cerr << "no loop at depth " << depth << "\n";
+        return 3;
+      }
+      auto alt = loop_tool::annotate(base, target, "[" + sub_backend + "]");
+      loop_tool::Compiler comp(alt);
+      auto sizes = comp.memory_sizes(true);
+      const size_t n_in = alt.ir.inputs().size(), n_out = alt.ir.outputs().size();
+      std::vector<std::vector<float>> bufs(n_in + n_out);
+      std::vector<void*> mem;
+      for (size_t i = 0; i < n_in + n_out; ++i) {
+        bufs[i].assign(std::max<int64_t>(sizes[i], 1), 0.f);
+        if (i < n_in) {
+          std::ifstream f(in_dir + "/in" + std::to_string(i) + ".f32", std::ios::binary);
+          f.read(reinterpret_cast<char*>(bufs[i].data()), bufs[i].size() * sizeof(float));
+          if ((size_t)f.gcount() != bufs[i].size() * sizeof(float)) {
+            std::cerr << "short input " << i << "\n";
+            return 3;
+          }
+        }
+        mem.emplace_back(bufs[i].data());
+      }
+      auto cc = loop_tool::getBackends().at("cpu_interpreted")->compile(alt);
+      cc->run(mem, true);
+      for (size_t j = 0; j < n_out; ++j) {
+        std::ofstream f(out_dir + "/out" + std::to_string(j) + ".f32", std::ios::binary);
+        f.write(reinterpret_cast<const char*>(bufs[n_in + j].data()),
+                bufs[n_in + j].size() * sizeof(float));
+      }
       return 0;
     }
     auto ir = loop_tool::deserialize(read_file(argv[2]));
