@@ -106,6 +106,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def max_over_ranks(x, device=None):
+    """The largest of a per-rank value (the slowest rank's time); x itself
+    when no process group spans more than one rank."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbs(bytes_per_rank_step, steps, max_seconds, world):
+    """Whole-job GB/s: every rank moves bytes_per_rank_step per step (weak
+    scaling, replicas), over the slowest rank's time."""
+    return world * bytes_per_rank_step * steps / max_seconds / 1e9
+
+
 def dist_setup():
     return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -282,14 +301,10 @@ def headline(args, world, rank, dev):
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     clocks = sampler.stop()
-    ms = t0.elapsed_time(t1)
+    ms = max_over_ranks(t0.elapsed_time(t1), dev)
     nest_ms = [statistics.mean(a.elapsed_time(b) for a, b in lst) for lst in per]
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = tt.item()
     step_bytes = sum(bytes_per)
-    value = world * step_bytes * args.steps / (ms / 1e3) / 1e9
+    value = whole_job_gbs(step_bytes, args.steps, ms / 1e3, world)
 
     # e2e: the same step through the C ABI with pinned host buffers; the
     # host->device copies of the inputs and device->host copies of the
@@ -306,16 +321,24 @@ def headline(args, world, rank, dev):
     if world > 1:
         torch.distributed.barrier()
     e2e_steps = max(1, min(args.steps, 3))
-    w0 = time.perf_counter()
+    # device time from the first upload to the last download: each nest runs
+    # on its own stream (asynchronous runs on pinned host buffers), so one
+    # nest's downloads overlap another's uploads on the host link
+    nest_streams = [torch.cuda.Stream() for _ in comps]
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for ns in nest_streams:
+        ns.wait_event(s0)
     for _ in range(e2e_steps):
-        for (_, c), hb in zip(comps, hbufs):
-            c.run(hb, sync=True)
+        for ns, (_, c), hb in zip(nest_streams, comps, hbufs):
+            c.run(hb, sync=False, stream=ns.cuda_stream)
+    for ns in nest_streams:
+        done = torch.cuda.Event()
+        done.record(ns)
+        stream.wait_event(done)
+    s1.record(stream)
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - w0) / e2e_steps
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = tt.item()
+    e2e_s = max_over_ranks(s0.elapsed_time(s1) / 1e3 / e2e_steps, dev)
     h2d = sum(4 * sum(c.io_sizes[:c.n_inputs]) for _, c in comps)
     d2h = sum(4 * sum(c.io_sizes[c.n_inputs:]) for _, c in comps)
     hbm_peak, _, peak_kind = load_peaks()
@@ -339,7 +362,7 @@ def headline(args, world, rank, dev):
         "roofline": {"bound": "hbm", "kernel": comps[dom][0], "achieved": achieved,
                      "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": read_traffic().get(comps[dom][0])},
-        "e2e": {"value": world * step_bytes / e2e_s / 1e9, "unit": "GB/s",
+        "e2e": {"value": whole_job_gbs(step_bytes, 1, e2e_s, world), "unit": "GB/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": sum(c.int_property("launches") for _, c in comps) * args.steps,
         "clocks": clocks,

@@ -68,7 +68,11 @@ int ltb_compile(const char* ir_text, const char* options, ltb_compiled** out);
  * (include/loop_tool/backend.h:20-21; CudaCompiled::run,
  * src/backends/cuda/cuda.cpp:837-850).  stream: a cudaStream_t or NULL for
  * the legacy default stream.  With sync == 0 the call returns after
- * enqueueing (Compiled::async, backend.h:41-44); host buffers force sync. */
+ * enqueueing (Compiled::async, backend.h:41-44); host buffers are then
+ * written back by stream-ordered copies, complete once the stream is (pin
+ * them for the copies to overlap).  Runs whose every buffer is in host
+ * memory and whose loop tree is one linear elementwise map stage their
+ * copies chunk by chunk on two streams (uploads overlap downloads). */
 int ltb_run(ltb_compiled* c, void* const* memory, int n, int sync,
             void* stream);
 

@@ -23,6 +23,12 @@ struct LtbCfg {
 cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
                             const LtbBufTable& bt, int sms, cudaStream_t st,
                             const LtbCfg& cfg);
+// A plain linear elementwise map (each load reads the output's own flat
+// index) run on the flat output range [lo, lo + n), lo a multiple of 8:
+// lets host-staged runs pipeline copies and compute chunk by chunk.
+int ltb_linear_range_ok(const LtbStage& h);
+cudaError_t ltb_launch_linear_range(const LtbStage& h, const LtbBufTable& bt, int64_t lo,
+                                    int64_t n, int sms, cudaStream_t st, const LtbCfg& cfg);
 // (b) block-parallel reductions; splits > 1 writes split-K partials to the
 // stage's partial buffer and combines them in order
 cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,

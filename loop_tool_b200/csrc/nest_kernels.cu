@@ -1214,6 +1214,72 @@ cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
   return cudaGetLastError();
 }
 
+// The plain linear maps (k_lin_bin / k_lin_un patterns): every load reads
+// the output's own flat index, so any flat sub-range runs on its own.
+static bool linear_map(const LtbStage& h, int* nload) {
+  if (!h.linear || (h.out_off & 3)) return false;
+  auto lin = [&](int i) {
+    const LtbLoad& L = h.loads[h.code[i].arg];
+    return L.mode == LTB_L_LINEAR && (L.off & 3) == 0;
+  };
+  if (h.ninstr == 3 && h.code[0].op == LTB_V_LOAD && h.code[1].op == LTB_V_LOAD && lin(0) &&
+      lin(1) && h.code[2].op >= LTB_V_ADD && h.code[2].op <= LTB_V_MAX) {
+    *nload = 2;
+    return true;
+  }
+  if (h.ninstr == 2 && h.code[0].op == LTB_V_LOAD && lin(0) && h.code[1].op >= LTB_V_EXP &&
+      h.code[1].op <= LTB_V_RECIP) {
+    *nload = 1;
+    return true;
+  }
+  return false;
+}
+
+int ltb_linear_range_ok(const LtbStage& h) {
+  int nl = 0;
+  if (!linear_map(h, &nl) || h.out_off) return 0;
+  for (int i = 0; i < nl; ++i)
+    if (h.loads[h.code[i].arg].off) return 0;  // element e of every buffer is flat index e
+  return 1;
+}
+
+cudaError_t ltb_launch_linear_range(const LtbStage& h, const LtbBufTable& bt, int64_t lo,
+                                    int64_t n, int sms, cudaStream_t st, const LtbCfg& cfg) {
+  int nl = 0;
+  if (!linear_map(h, &nl) || (lo & 7) || n <= 0) return cudaErrorNotSupported;
+  const int threads = pick_threads(cfg, 256, 256);
+  const int64_t work8 = (n + 7) / 8;
+  float* out = bt.p[h.out_buf] + h.out_off + lo;
+  const LtbLoad& L0 = h.loads[h.code[0].arg];
+  const float* a = bt.p[L0.buf] + L0.off + lo;
+  if (nl == 2) {
+    const LtbLoad& L1 = h.loads[h.code[1].arg];
+    const float* b = bt.p[L1.buf] + L1.off + lo;
+    switch (h.code[2].op) {
+#define LTB_BIN(O)                                                                  \
+  case O:                                                                           \
+    k_lin_bin<O><<<grid_of(k_lin_bin<O>, work8, threads, sms, cfg), threads, 0, st>>>( \
+        a, b, out, n);                                                              \
+    break;
+      LTB_BIN(LTB_V_ADD) LTB_BIN(LTB_V_SUB) LTB_BIN(LTB_V_MUL) LTB_BIN(LTB_V_DIV)
+      LTB_BIN(LTB_V_MIN) LTB_BIN(LTB_V_MAX)
+#undef LTB_BIN
+    }
+  } else {
+    switch (h.code[1].op) {
+#define LTB_UN(O)                                                                 \
+  case O:                                                                         \
+    k_lin_un<O><<<grid_of(k_lin_un<O>, work8, threads, sms, cfg), threads, 0, st>>>( \
+        a, out, n);                                                               \
+    break;
+      LTB_UN(LTB_V_EXP) LTB_UN(LTB_V_LOG) LTB_UN(LTB_V_SQRT) LTB_UN(LTB_V_ABS)
+      LTB_UN(LTB_V_NEG) LTB_UN(LTB_V_RECIP)
+#undef LTB_UN
+    }
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,
                               const LtbBufTable& bt, int splits, int sms,
                               cudaStream_t st, const LtbCfg& cfg) {

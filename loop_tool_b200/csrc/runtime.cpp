@@ -158,6 +158,8 @@ struct ltb_compiled {
   int64_t bandwidth_gbs = 0;
   int launches = 0;
   std::vector<LtbCfg> cfg;            // per stage launch schedule (autotuner)
+  cudaStream_t aux = nullptr;         // second stream of pipelined host-buffer runs
+  std::mutex aux_mu;
   uint64_t key = 0;                   // IR-text + options hash (schedule cache key)
   bool tuned = false;                 // schedules came from the tuner / cache
 };
@@ -538,8 +540,58 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
   std::vector<void*> temps;
   try {
     CUDA_TRY(cudaSetDevice(c->device));
+    // every buffer in host memory and a plain linear map: stage the copies
+    // chunk by chunk on two streams, so each chunk's download overlaps the
+    // next chunk's upload (the host link runs both directions at once)
+    bool all_host = true;
     for (int i = 0; i < n; ++i) {
       if (!memory[i]) return fail(LTB_ERR_INVALID, "null buffer " + std::to_string(i));
+      all_host = all_host && !is_device_accessible(memory[i]);
+    }
+    constexpr int64_t kChunk = int64_t(1) << 24;  // elements per chunk (64 MB of FP32)
+    const int64_t total = P.n_out ? P.io_elems[P.n_in] : 0;
+    bool same = true;
+    for (int i = 0; i < n; ++i) same = same && P.io_elems[i] == total;
+    if (all_host && same && total >= 2 * kChunk && P.stages.size() == 1 &&
+        P.stages[0].family == ltb::Family::elementwise && ltb_linear_range_ok(P.stages[0].dev)) {
+      for (int i = 0; i < n; ++i) {
+        void* d = nullptr;
+        CUDA_TRY(cudaMallocAsync(&d, (size_t)total * 4, st));
+        temps.push_back(d);
+        bt.p[i] = static_cast<float*>(d);
+      }
+      cudaStream_t aux;
+      {
+        std::lock_guard<std::mutex> g(c->aux_mu);
+        if (!c->aux) CUDA_TRY(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
+        aux = c->aux;
+      }
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      CUDA_TRY(cudaEventCreateWithFlags(&e0, cudaEventDisableTiming));
+      CUDA_TRY(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+      CUDA_TRY(cudaEventRecord(e0, st));
+      CUDA_TRY(cudaStreamWaitEvent(aux, e0, 0));  // the allocations above are visible
+      int k = 0;
+      for (int64_t lo = 0; lo < total; lo += kChunk, ++k) {
+        cudaStream_t s = (k & 1) ? aux : st;
+        const int64_t cn = std::min<int64_t>(kChunk, total - lo);
+        for (int i = 0; i < P.n_in; ++i)
+          CUDA_TRY(cudaMemcpyAsync(bt.p[i] + lo, static_cast<const float*>(memory[i]) + lo,
+                                   (size_t)cn * 4, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(ltb_launch_linear_range(P.stages[0].dev, bt, lo, cn, c->sms, s, c->cfg[0]));
+        for (int j = P.n_in; j < n; ++j)
+          CUDA_TRY(cudaMemcpyAsync(static_cast<float*>(memory[j]) + lo, bt.p[j] + lo,
+                                   (size_t)cn * 4, cudaMemcpyDeviceToHost, s));
+      }
+      CUDA_TRY(cudaEventRecord(e1, aux));
+      CUDA_TRY(cudaStreamWaitEvent(st, e1, 0));
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      for (void* d : temps) CUDA_TRY(cudaFreeAsync(d, st));
+      if (sync) CUDA_TRY(cudaStreamSynchronize(st));
+      return LTB_OK;
+    }
+    for (int i = 0; i < n; ++i) {
       if (is_device_accessible(memory[i])) {
         bt.p[i] = static_cast<float*>(memory[i]);
         continue;
@@ -563,7 +615,9 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
       CUDA_TRY(cudaMemcpyAsync(s.second, bt.p[s.first], bytes, cudaMemcpyDeviceToHost, st));
     }
     for (void* d : temps) CUDA_TRY(cudaFreeAsync(d, st));
-    if (sync || !temps.empty()) {
+    // host outputs are written by stream-ordered copies: with sync == 0 they
+    // are complete once the stream is (Compiled::async)
+    if (sync) {
       CUDA_TRY(cudaStreamSynchronize(st));
       int flag = 0;
       CUDA_TRY(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1113,6 +1167,7 @@ int ltb_run_with_scratch(ltb_compiled* c, void* const* memory, int n, int sync,
 
 int ltb_release(ltb_compiled* c) {
   if (!c) return LTB_OK;
+  if (c->aux) cudaStreamDestroy(c->aux);
   for (void* p : c->owned) cudaFree(p);
   delete c;
   return LTB_OK;

@@ -127,3 +127,34 @@ def test_mm_8192_sampled_vs_fp64(precision, tol, cuda_dev):
     got = C2[rows][:, cols].double()
     err = float((got - ref).norm() / ref.norm())
     assert err <= tol, f"{precision}: sampled normwise error {err:.3g}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("op", ["add", "exp"])
+def test_host_buffers_pipelined(op, cuda_dev):
+    """Host-buffer runs of a linear map large enough to be staged chunk by
+    chunk on two streams (and asynchronous with sync=False): the result is
+    bit-identical to the same loop tree run on device buffers, for pinned
+    and pageable host memory."""
+    import torch
+
+    import loop_tool_b200 as ltb
+    import loop_tool_b200.lazy as lt
+
+    n = (1 << 25) + 12344  # two full 2^24 chunks and a ragged third
+    A, B = lt.Tensor(n), lt.Tensor(n)
+    N = lt.Symbol("N")
+    T = A.to(N) + B.to(N) if op == "add" else A.to(N).exp()
+    c = ltb.Compiled(T.ir)
+    g = torch.Generator(device=cuda_dev).manual_seed(5)
+    dev_in = [torch.randn(n, device=cuda_dev, generator=g) for _ in range(c.n_inputs)]
+    dev_out = torch.empty(n, device=cuda_dev)
+    c(dev_in + [dev_out])
+    ref = dev_out.cpu()
+    pinned = [x.cpu().pin_memory() for x in dev_in] + [torch.full((n,), float("nan")).pin_memory()]
+    c.run(pinned, sync=False)
+    torch.cuda.synchronize()
+    assert torch.equal(pinned[-1], ref)
+    pageable = [x.cpu().numpy() for x in dev_in] + [np.full(n, np.nan, np.float32)]
+    c(pageable)
+    assert np.array_equal(pageable[-1], ref.numpy())
