@@ -92,7 +92,9 @@ int ltb_dump(ltb_compiled* c, char* buf, size_t len);
 /* Compiled::int_properties (src/backends/cuda/cuda.cpp:960-969):
  * "bandwidth" (theoretical GB/s, 2*memclk*buswidth/8 as the reference
  * computes it), plus "stages", "launches", "scratch_bytes", "inputs",
- * "outputs", "algorithmic_bytes", "flops". */
+ * "outputs", "algorithmic_bytes", "flops", "tuned" (schedules from the
+ * autotuner or its cache), "implicit_conv" (contractions whose A operand is
+ * read as an image: convolution as implicit GEMM). */
 int ltb_int_property(ltb_compiled* c, const char* name, int64_t* value);
 
 /* Element counts of the I/O buffers: elems[0..n_in+n_out). */

@@ -119,7 +119,7 @@ class Compiled:
     @property
     def int_properties(self):
         keys = ("bandwidth", "stages", "launches", "scratch_bytes", "inputs", "outputs",
-                "algorithmic_bytes", "flops", "tuned")
+                "algorithmic_bytes", "flops", "tuned", "implicit_conv")
         return {k: self.int_property(k) for k in keys}
 
     # ------------------------------------------------------------ autotuner

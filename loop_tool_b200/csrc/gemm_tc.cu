@@ -71,6 +71,33 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
+// 4-D box (image operands: channels, columns, row, image); coordinates
+// outside the image read as zeros.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int x, int y, int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
+      : "memory");
+}
+
+// Output row of tile row tr (0..127) of m-tile m0 / BM, and whether the row
+// exists: plain operands map tile rows to rows m0 + tr; image operands to
+// image row tr / img_slot, column tr % img_slot of the tile's image rows.
+__device__ __forceinline__ bool tile_row(const LtbTcProblem& p, int m0, int tr, int* row) {
+  if (!p.img) {
+    *row = m0 + tr;
+    return *row < p.M;
+  }
+  const int mt = m0 / BM, n_img = mt / p.img_hgroups;
+  const int ho0 = (mt - n_img * p.img_hgroups) * p.img_rows;
+  const int i = tr / p.img_slot, w = tr - i * p.img_slot;
+  const bool ok = i < p.img_rows && w < p.img_wo && ho0 + i < p.img_ho;
+  *row = ok ? (n_img * p.img_ho + ho0 + i) * p.img_wo + w : 0;
+  return ok;
+}
+
 // K-major, 128-byte-swizzled canonical layout: 8-row x 128-byte atoms
 // (1024 B) stacked along M/N, LBO unused (1), SBO = 1024 B, version 1.
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
@@ -141,7 +168,8 @@ __global__ void __launch_bounds__(NT, 1)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
               float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
               const __grid_constant__ CUtensorMap single_a,
-              const __grid_constant__ CUtensorMap single_b) {
+              const __grid_constant__ CUtensorMap single_b,
+              const __grid_constant__ CUtensorMap single_a2) {
   // probs == nullptr: one problem passed by value with its tensor maps as
   // kernel parameters (encoded at launch over per-run scratch)
   using T = Tile<BN>;
@@ -191,9 +219,16 @@ __global__ void __launch_bounds__(NT, 1)
           probs ? static_cast<const CUtensorMap*>(p.map_a) : &single_a;
       const CUtensorMap* mb =
           probs ? static_cast<const CUtensorMap*>(p.map_b) : &single_b;
+      const CUtensorMap* ma2 =
+          probs ? static_cast<const CUtensorMap*>(p.map_a2) : &single_a2;
       int m0, n0;
       tile_coords<BN>(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
+      // image operands: this tile's image and first output image row
+      const int mt = m0 / BM;
+      const int n_img = p.img ? mt / p.img_hgroups : 0;
+      const int ho0 = p.img ? (mt - n_img * p.img_hgroups) * p.img_rows : 0;
+      const int kseg = p.img ? p.img_kh * p.img_kw * p.img_cblocks : 1;
       for (int kb = 0; kb < nk; ++kb, ++g) {
         const int s = g % STAGES;
         const uint32_t ph = (g / STAGES) & 1u;
@@ -202,9 +237,21 @@ __global__ void __launch_bounds__(NT, 1)
           break;
         }
         const uint32_t fb = smem_u32(&full[s]);
-        mbar_expect_tx(fb, STAGE_BYTES);
         uint8_t* sa = smem + s * STAGE_BYTES;
-        tma_load_2d(smem_u32(sa), ma, fb, kb * BK, m0);
+        if (p.img) {
+          // k-block -> (segment, kh, kw, channel block); one box per image row
+          const int seg = kb / kseg, r = kb - seg * kseg;
+          const int cb = r % p.img_cblocks, r2 = r / p.img_cblocks;
+          const int kw = r2 % p.img_kw, kh = r2 / p.img_kw;
+          const CUtensorMap* m = (p.img_a_mask >> seg) & 1 ? ma : ma2;
+          mbar_expect_tx(fb, (uint32_t)(p.img_rows * p.img_wo * 128 + T::B_BYTES));
+          for (int i = 0; i < p.img_rows; ++i)
+            tma_load_4d(smem_u32(sa + i * p.img_slot * 128), m, fb, cb * 64, kw, ho0 + i + kh,
+                        n_img);
+        } else {
+          mbar_expect_tx(fb, STAGE_BYTES);
+          tma_load_2d(smem_u32(sa), ma, fb, kb * BK, m0);
+        }
         tma_load_2d(smem_u32(sa + A_BYTES), mb, fb, kb * BK, n0);
       }
     }
@@ -280,13 +327,12 @@ __global__ void __launch_bounds__(NT, 1)
       // epilogue: this warp owns rows m0 + 32*quad .. +31 (row m0 + 32*quad
       // + lane in this thread's registers) and HALF columns from cbase
       float* cb = c_override ? c_override : p.c;
-      const int row = m0 + quad * 32 + lane;
+      int row;
+      const bool rvalid = tile_row(p, m0, quad * 32 + lane, &row);
       const int cbase = n0 + half * T::HALF;
       if (kTransposeEpi && p.unit_cols) {
         float* stage = epi + (warp - 2) * (32 * kEpiPitch);
-        const int r0 = m0 + quad * 32;
-        const int rows = p.M - r0 < 32 ? p.M - r0 : 32;
-        const int64_t rb = row < p.M ? p.crow[row] : 0;
+        const int64_t rb = rvalid ? p.crow[row] : 0;
 #pragma unroll
         for (int c = 0; c < T::HALF; c += 32) {
           __syncwarp();
@@ -298,10 +344,11 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll 8
           for (int i = 0; i < 32; ++i) {  // row i of the block: 32 consecutive columns
             const int64_t rbi = __shfl_sync(0xffffffffu, rb, i);
-            if (i < rows && cok) cb[rbi + col] = stage[i * kEpiPitch + lane];
+            const int vi = __shfl_sync(0xffffffffu, (int)rvalid, i);
+            if (vi && cok) cb[rbi + col] = stage[i * kEpiPitch + lane];
           }
         }
-      } else if (row < p.M) {  // this thread's row: 16-byte stores where aligned
+      } else if (rvalid) {  // this thread's row: 16-byte stores where aligned
         const int64_t rbase = p.crow[row];
         float* dst = cb + rbase;
 #pragma unroll
@@ -622,6 +669,40 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
   }
 }
 
+// Image operand repack: one CTA per (channel block of 64, padded row, image)
+// reads the 64 channel rows of x (coalesced along w) into shared memory and
+// writes the padded row [wp, 64] of BF16 channel pairs (coalesced along c).
+__global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbImageJob J) {
+  extern __shared__ float tile[];  // [64][wp + 1]
+  const int cb = blockIdx.x, h = blockIdx.y, n = blockIdx.z;
+  const int pitch = J.wp + 1;
+  const int hs = h + J.off_h;  // source row
+  const bool row_ok = hs >= 0 && hs < J.ub_h;
+  for (int idx = threadIdx.x; idx < 64 * J.wp; idx += blockDim.x) {
+    const int c = idx / J.wp, w = idx - c * J.wp;
+    const int ws = w + J.off_w;
+    float v = 0.f;
+    if (row_ok && ws >= 0 && ws < J.ub_w)
+      v = __ldg(J.base + J.off + (int64_t)n * J.ns + (int64_t)(cb * 64 + c) * J.cs +
+                (int64_t)h * J.wx + w);
+    tile[c * pitch + w] = v;
+  }
+  __syncthreads();
+  const int64_t row = (((int64_t)n * J.hp + h) * J.wp) * J.c + cb * 64;
+  for (int idx = threadIdx.x; idx < J.wp * 32; idx += blockDim.x) {
+    const int w = idx >> 5, cp = (idx & 31) * 2;
+    const float x0 = tile[cp * pitch + w], x1 = tile[(cp + 1) * pitch + w];
+    const __nv_bfloat162 hi = __floats2bfloat162_rn(x0, x1);
+    const int64_t o = row + (int64_t)w * J.c + cp;
+    *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(J.hi) + o) = hi;
+    if (J.lo) {
+      const float2 hf = __bfloat1622float2(hi);
+      *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(J.lo) + o) =
+          __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+    }
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -649,6 +730,37 @@ cudaError_t ltb_make_tmap(void* map, const void* base, int64_t rows, int64_t Kp,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t ltb_make_tmap_image(void* map, const void* base, int n, int hp, int wp, int c,
+                                int wo) {
+  auto fn = encode_fn();
+  if (!fn || c % 64 || wo < 1 || wo > 256) return cudaErrorInvalidValue;
+  const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)wp, (cuuint64_t)hp, (cuuint64_t)n};
+  const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)wp * c * 2,
+                                 (cuuint64_t)hp * wp * c * 2};
+  const cuuint32_t box[4] = {64, (cuuint32_t)wo, 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = fn(reinterpret_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4,
+                  const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st) {
+  if (j.c % 64 || j.wp < 1 || j.wp > 1024) return cudaErrorInvalidValue;
+  const size_t smem = (size_t)64 * (j.wp + 1) * sizeof(float);
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_pack_image,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = smem;
+  }
+  dim3 grid((unsigned)(j.c / 64), (unsigned)j.hp, (unsigned)j.nimg);
+  k_pack_image<<<grid, 256, smem, st>>>(j);
+  return cudaGetLastError();
 }
 
 int ltb_tc_tile_m() { return BM; }
@@ -705,7 +817,8 @@ cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t
 template <int BN, bool TE>
 static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                              float* c_override, int sms, int* err, cudaStream_t st,
-                             const LtbTcProblem* single, const void* map_a, const void* map_b) {
+                             const LtbTcProblem* single, const void* map_a, const void* map_b,
+                             const void* map_a2) {
   static bool attr = false;
   const size_t smem = Tile<BN>::SMEM;
   if (!attr) {
@@ -716,26 +829,27 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
   }
   const int grid = (int)(total_tiles < sms ? total_tiles : sms);
   LtbTcProblem one{};
-  CUtensorMap ma{}, mb{};
+  CUtensorMap ma{}, mb{}, ma2{};
   if (!d_probs) {
     if (!single || !map_a || !map_b) return cudaErrorInvalidValue;
     one = *single;
     ma = *static_cast<const CUtensorMap*>(map_a);
     mb = *static_cast<const CUtensorMap*>(map_b);
+    ma2 = map_a2 ? *static_cast<const CUtensorMap*>(map_a2) : ma;
   }
   k_gemm_tc<BN, TE><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err, one, ma,
-                                            mb);
+                                            mb, ma2);
   return cudaGetLastError();
 }
 
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single, const void* map_a,
-                               const void* map_b) {
+                               const void* map_b, const void* map_a2) {
   if (total_tiles == 0) return cudaSuccess;
 #define LTB_TC(BN, TE)                                                                      \
   return launch_tc<BN, TE>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a, \
-                           map_b)
+                           map_b, map_a2)
   switch (bn) {
     case 128: LTB_TC(128, false);
     case 129: LTB_TC(128, true);

@@ -86,6 +86,12 @@ struct GemmTables {
   LtbTcProblem prob{};                // launch template (maps/c bound per run)
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
   bool a_off32 = false, b_off32 = false;  // operand offsets fit in int32
+  // implicit-GEMM convolution: A packed as NHWC BF16 image(s) read by 4-D
+  // TMA boxes (LtbTcProblem::img); B's K order permuted to (kh, kw, c)
+  bool img = false;
+  int img_kinds = 1;                  // images in the A slot: hi (+ lo)
+  int64_t img_elems = 0;              // elements of one image
+  LtbImageJob ijob{};                 // base / hi / lo bound at launch
   int bn = 256;                       // tensor-core tile width (128 or 256)
   int epi = 0;                        // 1: shared-memory transposed epilogue
 };
@@ -170,6 +176,63 @@ int64_t stage_outs(const LtbStage& d) {
   int64_t o = 1;
   for (int k = 0; k < d.nout; ++k) o *= d.size[k];
   return o;
+}
+
+// A stride-1 2-D window over an NCHW-like operand: rows (n, ho, wo) or
+// (ho, wo), k (c, kh, kw) in any order, x(n, c, ho + kh + off_h,
+// wo + kw + off_w) with unit column stride, row pitch wx, channel pitch cs,
+// zero outside [0, ub_h) x [0, ub_w) (padding guards) or no guards.
+struct ImageGeom {
+  int64_t nimg = 1, ns = 0, ho = 0, wo = 0, c = 0, kh = 0, kw = 0, wx = 0, cs = 0;
+  int kh_dim = -1, kw_dim = -1, c_dim = -1;
+  int off_h = 0, ub_h = 1 << 30, off_w = 0, ub_w = 1 << 30;
+};
+
+bool detect_image(const LtbStage& d, const LtbLoad& A, const std::vector<int>& md,
+                  const std::vector<int>& kd, ImageGeom& g) {
+  if (kd.size() != 3 || (md.size() != 2 && md.size() != 3) || A.nq) return false;
+  const int wo = md.back(), ho = md[md.size() - 2];
+  g.wx = A.coef[ho];
+  if (A.coef[wo] != 1 || g.wx < 2) return false;
+  for (int k : kd) {
+    if (A.coef[k] == 1 && g.kw_dim < 0) g.kw_dim = k;
+    else if (A.coef[k] == g.wx && g.kh_dim < 0) g.kh_dim = k;
+    else g.c_dim = k;
+  }
+  if (g.kw_dim < 0 || g.kh_dim < 0 || g.c_dim < 0) return false;
+  g.cs = A.coef[g.c_dim];
+  g.c = d.size[g.c_dim];
+  g.kh = d.size[g.kh_dim];
+  g.kw = d.size[g.kw_dim];
+  g.ho = d.size[ho];
+  g.wo = d.size[wo];
+  if (g.cs < 1 || g.c % 64 || g.wo % 8 || g.wo > 128) return false;
+  if (md.size() == 3) {
+    g.nimg = d.size[md[0]];
+    g.ns = A.coef[md[0]];
+  }
+  if (A.ng == 0) return A.off == 0;
+  if (A.ng != 2) return false;
+  bool fh = false, fw = false;
+  for (int q = A.g0; q < A.g0 + A.ng; ++q) {
+    const LtbGuard& G = d.guards[q];
+    for (int k = 0; k < d.ndim; ++k) {
+      const bool on_h = k == ho || k == g.kh_dim, on_w = k == wo || k == g.kw_dim;
+      const bool h_guard = G.coef[ho] == 1 && G.coef[g.kh_dim] == 1;
+      if (G.coef[k] != ((h_guard ? on_h : on_w) ? 1 : 0)) return false;
+    }
+    if (G.off < -(1 << 20) || G.off > (1 << 20) || G.ub > (1 << 30)) return false;
+    if (G.coef[ho] == 1) {
+      fh = true;
+      g.off_h = (int)G.off;
+      g.ub_h = (int)G.ub;
+    } else {
+      fw = true;
+      g.off_w = (int)G.off;
+      g.ub_w = (int)G.ub;
+    }
+  }
+  return fh && fw && A.off == (int64_t)g.off_h * g.wx + g.off_w;
 }
 
 // Split a contraction's affine operand loads into per-row / per-k tables.
@@ -302,6 +365,71 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     e.N = (int)con.N;
     e.tiles_m = tm;
     e.unit_cols = t.unit_cols ? 1 : 0;
+    ImageGeom ig;
+    if (t.nbatch == 1 && t.Kp == t.nseg * con.K && detect_image(d, A, md, kd, ig)) {
+      // implicit GEMM: A' never materialises; the A slot holds the padded
+      // NHWC image(s), hi (+ lo for split modes)
+      t.img = true;
+      const int segs = (1 << t.nseg) - 1;
+      t.img_kinds = (~t.a_mask & segs) ? 2 : 1;
+      const int64_t hp = ig.ho + ig.kh - 1, wp = ig.wo + ig.kw - 1;
+      t.img_elems = ig.nimg * hp * wp * ig.c;
+      P.scratch_elems[t.a_slot - (P.n_in + P.n_out)] = (t.img_kinds * t.img_elems + 1) / 2;
+      LtbImageJob& j = t.ijob;
+      j.off = A.off;
+      j.ns = ig.ns;
+      j.cs = ig.cs;
+      j.wx = ig.wx;
+      j.nimg = (int)ig.nimg;
+      j.c = (int)ig.c;
+      j.hp = (int)hp;
+      j.wp = (int)wp;
+      j.off_h = ig.off_h;
+      j.ub_h = ig.ub_h;
+      j.off_w = ig.off_w;
+      j.ub_w = ig.ub_w;
+      e.img = 1;
+      e.img_slot = (int)ig.wo;
+      e.img_rows = 128 / e.img_slot;
+      e.img_wo = (int)ig.wo;
+      e.img_ho = (int)ig.ho;
+      e.img_hgroups = (int)((ig.ho + e.img_rows - 1) / e.img_rows);
+      e.img_kh = (int)ig.kh;
+      e.img_kw = (int)ig.kw;
+      e.img_cblocks = (int)(ig.c / 64);
+      e.img_a_mask = t.a_mask;
+      e.tiles_m = (int)(ig.nimg * e.img_hgroups);
+      // B' in the image's K order: k' = (kh * KW + kw) * C + c
+      std::vector<int64_t> kstride(kd.size());
+      {
+        int64_t st = 1;
+        for (int q = (int)kd.size() - 1; q >= 0; --q) {
+          kstride[q] = st;
+          st *= d.size[kd[q]];
+        }
+      }
+      auto pos = [&](int dim) { return (int)(std::find(kd.begin(), kd.end(), dim) - kd.begin()); };
+      const int pc = pos(ig.c_dim), ph = pos(ig.kh_dim), pw = pos(ig.kw_dim);
+      std::vector<int64_t> perm(con.K);
+      for (int64_t kh = 0, k2 = 0; kh < ig.kh; ++kh)
+        for (int64_t kw = 0; kw < ig.kw; ++kw)
+          for (int64_t ch = 0; ch < ig.c; ++ch, ++k2)
+            perm[k2] = ch * kstride[pc] + kh * kstride[ph] + kw * kstride[pw];
+      std::vector<int64_t> bk(con.K);
+      for (int64_t q = 0; q < con.K; ++q) bk[q] = ktab_b[perm[q]];
+      ar.add(bk, &t.b_k);
+      if (t.b_ng) {
+        std::vector<int32_t> vk;
+        for (int g = B.g0; g < B.g0 + B.ng; ++g) {
+          auto gk = table(kd, d.guards[g].coef, 0);
+          for (int64_t q = 0; q < con.K; ++q) vk.push_back((int32_t)gk[perm[q]]);
+        }
+        ar.add(vk, &t.bg_k);
+      }
+      auto rb = table(nd, B.coef, B.off);
+      t.b_dense = B.ng == 0 && rb[0] == 0 && arith(rb, &t.b_ldr) && arith(bk, &t.b_ldk);
+      t.b_kcontig = unit_frac(bk) >= unit_frac(rb);
+    }
     // narrow outputs take 128-wide tiles (no half-empty MMA), the rest 256
     set_tile_n(t, con.N <= 128 ? 128 : 256, 0);
   }
@@ -465,13 +593,26 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         }
         void* ap = bt.p[t.a_slot];
         void* bp = bt.p[t.b_slot];
-        e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, t.a_off32,
-                            c->sms, st);
+        alignas(64) unsigned char maps[384];  // A (hi image), B, A lo image
+        if (t.img) {
+          LtbImageJob j = t.ijob;
+          j.base = p.a.base;
+          j.hi = ap;
+          j.lo = t.img_kinds == 2 ? static_cast<char*>(ap) + t.img_elems * 2 : nullptr;
+          e = ltb_launch_pack_image(j, st);
+          if (e == cudaSuccess)
+            e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.prob.img_wo);
+          if (e == cudaSuccess)
+            e = ltb_make_tmap_image(maps + 256, j.lo ? j.lo : j.hi, j.nimg, j.hp, j.wp, j.c,
+                                    t.prob.img_wo);
+        } else {
+          e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, t.a_off32,
+                              c->sms, st);
+          if (e == cudaSuccess) e = ltb_make_tmap(maps, ap, p.M, t.Kp, ltb_tc_tile_m());
+        }
         if (e == cudaSuccess)
           e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, t.b_off32,
                               c->sms, st);
-        alignas(64) unsigned char maps[256];
-        if (e == cudaSuccess) e = ltb_make_tmap(maps, ap, p.M, t.Kp, ltb_tc_tile_m());
         if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, t.bn);
         if (e == cudaSuccess) {
           LtbTcProblem one = t.prob;
@@ -479,7 +620,7 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           one.crow = t.c_row;
           one.ccol = t.c_col;
           e = ltb_launch_gemm_tc(t.bn | t.epi, nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st,
-                                 &one, maps, maps + 128);
+                                 &one, maps, maps + 128, t.img ? maps + 256 : nullptr);
         }
       }
       break;
@@ -688,7 +829,8 @@ std::string describe(ltb_compiled* c, int i) {
     if (t.tc)
       o << "tile(128x" << t.bn << "x64) tensor_cores(tcgen05) parallel(persistent, "
         << t.tiles << " tiles) raster(" << (t.prob.group_m ? t.prob.group_m : 16)
-        << " row blocks) epilogue(" << (t.epi ? "smem transpose" : "row stores") << ")";
+        << " row blocks) epilogue(" << (t.epi ? "smem transpose" : "row stores") << ")"
+        << (t.img ? " implicit_conv(A from NHWC image via 4-D TMA)" : "");
     else
       o << "tile(128x128) cuda_cores";
     return o.str();
@@ -794,6 +936,7 @@ struct ltb_batch {
   int njobs = 0;
   int64_t pack_tiles = 0;
   int pack_chunk = 0, pack_cta_per_sm = 0;  // grouped pack schedule (0: defaults)
+  std::vector<LtbImageJob> img_jobs;        // image operands, repacked before the pack
   // tensor-core problems grouped by schedule variant (group 2 * (tile width
   // == 256) + transposed epilogue), one persistent launch per non-empty group
   LtbTcProblem* d_tc[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -821,6 +964,7 @@ void batch_gemms(ltb_batch* b, cudaStream_t st) {
 
 void batch_launch(ltb_batch* b, cudaStream_t st) {
   if (b->tc) {
+    for (const auto& j : b->img_jobs) CUDA_TRY(ltb_launch_pack_image(j, st));
     CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st, b->pack_chunk,
                                      b->pack_cta_per_sm));
     batch_gemms(b, st);
@@ -911,17 +1055,30 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
           jobs.push_back(j);
         };
         void *ap = nullptr, *bp = nullptr;
-        CUDA_TRY(cudaMalloc(&ap, (size_t)p.M * t.Kp * 2));
+        const size_t a_bytes =
+            t.img ? (size_t)t.img_kinds * t.img_elems * 2 : (size_t)p.M * t.Kp * 2;
+        CUDA_TRY(cudaMalloc(&ap, a_bytes));
         b->owned.push_back(ap);
         CUDA_TRY(cudaMalloc(&bp, (size_t)p.N * t.Kp * 2));
         b->owned.push_back(bp);
-        job(p.a, p.M, ap, t.a_mask, t.a_kcontig, t.a_off32);
+        if (!t.img) job(p.a, p.M, ap, t.a_mask, t.a_kcontig, t.a_off32);
         job(p.b, p.N, bp, t.b_mask, t.b_kcontig, t.b_off32);
         const int grp = (t.bn == 256 ? 2 : 0) + t.epi;
         auto& mv = maps[grp];
-        mv.resize(mv.size() + 256);
-        unsigned char* m = mv.data() + mv.size() - 256;
-        CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
+        mv.resize(mv.size() + 384);  // A (hi image), B, A lo image
+        unsigned char* m = mv.data() + mv.size() - 384;
+        if (t.img) {
+          LtbImageJob j = t.ijob;
+          j.base = p.a.base;
+          j.hi = ap;
+          j.lo = t.img_kinds == 2 ? static_cast<char*>(ap) + t.img_elems * 2 : nullptr;
+          b->img_jobs.push_back(j);
+          CUDA_TRY(ltb_make_tmap_image(m, j.hi, j.nimg, j.hp, j.wp, j.c, t.prob.img_wo));
+          CUDA_TRY(ltb_make_tmap_image(m + 256, j.lo ? j.lo : j.hi, j.nimg, j.hp, j.wp, j.c,
+                                       t.prob.img_wo));
+        } else {
+          CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
+        }
         CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, t.bn));
         LtbTcProblem q = t.prob;
         q.c = p.c;
@@ -943,8 +1100,9 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         // tensor maps in device memory (cudaMalloc is 256-byte aligned)
         unsigned char* d_maps = upload(maps[g], b->owned);
         for (size_t i = 0; i < tcp[g].size(); ++i) {
-          tcp[g][i].map_a = d_maps + 256 * i;
-          tcp[g][i].map_b = d_maps + 256 * i + 128;
+          tcp[g][i].map_a = d_maps + 384 * i;
+          tcp[g][i].map_b = d_maps + 384 * i + 128;
+          tcp[g][i].map_a2 = d_maps + 384 * i + 256;
         }
         b->ntc[g] = (int)tcp[g].size();
         b->d_tc[g] = upload(tcp[g], b->owned);
@@ -1023,6 +1181,7 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
     CUDA_TRY(cudaEventCreate(&e1));
     CUDA_TRY(cudaEventCreate(&e2));
     CUDA_TRY(cudaEventRecord(e0, st));
+    for (const auto& j : b->img_jobs) CUDA_TRY(ltb_launch_pack_image(j, st));
     if (b->tc) CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st, b->pack_chunk,
                                      b->pack_cta_per_sm));
     CUDA_TRY(cudaEventRecord(e1, st));
@@ -1190,6 +1349,11 @@ int ltb_int_property(ltb_compiled* c, const char* name, int64_t* value) {
   else if (k == "algorithmic_bytes") *value = c->plan.algorithmic_bytes;
   else if (k == "flops") *value = (int64_t)c->plan.flops;
   else if (k == "tuned") *value = c->tuned ? 1 : 0;
+  else if (k == "implicit_conv") {
+    int64_t n = 0;
+    for (const auto& t : c->gemms) n += t.img ? 1 : 0;
+    *value = n;
+  }
   else return fail(LTB_ERR_INVALID, "unknown property " + k);
   return LTB_OK;
 }

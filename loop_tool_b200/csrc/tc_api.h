@@ -19,8 +19,37 @@ struct LtbTcProblem {
   int tiles_m, tiles_n;
   int unit_cols;         // ccol[j] == j
   int group_m;           // raster: row blocks swept together (0: 16)
-  int pad_;
+  // Image operand (implicit-GEMM convolution, stride 1): A is read straight
+  // from a zero-padded NHWC BF16 image [n, Hp, Wp, C] through 4-D boxes of
+  // 64 channels x wo output columns, one box per output image row; a
+  // 128-row tile holds img_rows image rows of img_slot rows each (wo
+  // rounded up to 8), i.e. output rows m = (n * ho + h) * wo + w.  K runs
+  // (kh, kw, c): k-block = (kh * kw_n + kw) * cblocks + channel block.
+  int img;               // 0: A' [M, Kp] dense as above
+  int img_rows, img_slot, img_wo, img_ho, img_hgroups;
+  int img_kh, img_kw, img_cblocks;
+  int img_a_mask;        // bit s: segment s reads the hi image (1) or lo (0)
+  const void* map_a2;    // image mode: CUtensorMap over the lo image
 };
+
+// Repacks an image operand x(n, c, h + off_h, w + off_w) (FP32 at
+// base + n*ns + c*cs + h*wx + w, element (h, w) of the window valid iff
+// 0 <= h + off_h < ub_h and 0 <= w + off_w < ub_w, else 0) into zero-padded
+// NHWC BF16 images [n, hp, wp, c]: the hi part into hi, the lo part
+// (x - hi rounded to BF16) into lo when lo is not null.
+struct LtbImageJob {
+  const float* base;     // the operand's buffer; element (n,c,h,w) at base + off
+  int64_t off, ns, cs, wx;
+  int nimg, c, hp, wp;
+  int off_h, ub_h, off_w, ub_w;
+  void* hi;
+  void* lo;
+};
+cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st);
+// CUtensorMap over an NHWC BF16 image [n, hp, wp, c] with boxes of
+// 64 channels x wo columns (128-byte swizzle): c % 64 == 0, wo <= 256.
+cudaError_t ltb_make_tmap_image(void* map, const void* base, int n, int hp, int wp, int c,
+                                int wo);
 
 // Load modes of the operand packer (ltb_pack_mode picks one per operand).
 enum { kPackDenseK = 0, kPackDenseR = 1, kPackGatherK = 2, kPackGatherR = 3 };
@@ -68,5 +97,6 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single = nullptr,
-                               const void* map_a = nullptr, const void* map_b = nullptr);
+                               const void* map_a = nullptr, const void* map_b = nullptr,
+                               const void* map_a2 = nullptr);
 int ltb_tc_tile_m();

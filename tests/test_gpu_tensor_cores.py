@@ -105,3 +105,85 @@ def test_pack_layouts(shape, precision, cuda_dev):
     assert np.isfinite(got).all()
     err = normwise(got, exact)
     assert err <= TOL[precision], f"{shape} {precision}: normwise error {err:.3g}"
+
+
+# Convolution as implicit GEMM: NCHW inputs with 64-channel blocks and output
+# widths that are multiples of 8 are read by the tensor-core kernel straight
+# from a padded NHWC image (4-D TMA boxes per output image row); the other
+# shapes take the gathered-operand path.  (N, C, H, W, CO, K, pad, implicit)
+IMPLICIT = [(2, 64, 8, 8, 16, 3, 1, True), (2, 64, 16, 16, 40, 3, 1, True),
+            (1, 128, 10, 10, 24, 3, 0, True), (3, 64, 24, 24, 64, 5, 2, True),
+            (1, 64, 56, 56, 128, 3, 1, True), (1, 64, 14, 14, 32, 3, 1, False),
+            (2, 32, 16, 16, 16, 3, 1, False)]
+
+
+def _conv_check(c, N, C, H, W, CO, K, pad, dev, tol):
+    import torch
+
+    g = torch.Generator(device=dev).manual_seed(N * 1000 + C + H + CO + K)
+    x = torch.randn(N * C * H * W, device=dev, generator=g)
+    w = torch.randn(CO * C * K * K, device=dev, generator=g) / (C * K * K) ** 0.5
+    Ho, Wo = H + 2 * pad - K + 1, W + 2 * pad - K + 1
+    y = torch.full((N * Ho * Wo * CO,), float("nan"), device=dev)
+    for _ in range(2):  # scratch reused: the padded image must be rewritten whole
+        c([x, w, y])
+    torch.cuda.synchronize()
+    ref = torch.nn.functional.conv2d(x.view(N, C, H, W).double(),
+                                     w.view(CO, C, K, K).double(), padding=pad)
+    got = y.view(N, Ho, Wo, CO).permute(0, 3, 1, 2).double()
+    assert torch.isfinite(got).all()
+    err = float((got - ref).norm() / ref.norm())
+    assert err <= tol, f"normwise error {err:.3g}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
+@pytest.mark.parametrize("shape", IMPLICIT)
+def test_conv_implicit_gemm(shape, precision, cuda_dev):
+    import loop_tool_b200 as lt
+    from programs import conv
+
+    N, C, H, W, CO, K, pad, implicit = shape
+    T, _ = conv(N, C, H, W, CO, K, pad, 1)
+    c = lt.cuda(T.ir, precision=precision)
+    assert c.int_property("implicit_conv") == (1 if implicit else 0)
+    _conv_check(c, N, C, H, W, CO, K, pad, cuda_dev, TOL[precision])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
+def test_conv_implicit_in_batch(precision, cuda_dev):
+    """An implicit-GEMM convolution and plain matmuls in one grouped launch."""
+    import torch
+
+    import loop_tool_b200 as ltb
+    from programs import conv, mm
+
+    T, _ = conv(2, 64, 16, 16, 40, 3, 1, 1)
+    cc = ltb.Compiled(T.ir, precision=precision)
+    assert cc.int_property("implicit_conv") == 1
+    g = torch.Generator(device=cuda_dev).manual_seed(17)
+    x = torch.randn(2 * 64 * 16 * 16, device=cuda_dev, generator=g)
+    w = torch.randn(40 * 64 * 9, device=cuda_dev, generator=g) / 24.0
+    y = torch.full((2 * 16 * 16 * 40,), float("nan"), device=cuda_dev)
+    members = [(cc, [x, w, y])]
+    mms = []
+    for M, K, N in ((96, 64, 48), (300, 128, 200)):
+        Tm, _ = mm(M, K, N)
+        cm = ltb.Compiled(Tm.ir, precision=precision)
+        bufs = [torch.randn(M * K, device=cuda_dev, generator=g) / K ** 0.5,
+                torch.randn(K * N, device=cuda_dev, generator=g),
+                torch.full((M * N,), float("nan"), device=cuda_dev)]
+        members.append((cm, bufs))
+        mms.append((M, K, N, bufs))
+    stream = torch.cuda.Stream()
+    b = ltb.Batch(members, capture_stream=stream.cuda_stream)
+    b.run(stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    ref = torch.nn.functional.conv2d(x.view(2, 64, 16, 16).double(),
+                                     w.view(40, 64, 3, 3).double(), padding=1)
+    got = y.view(2, 16, 16, 40).permute(0, 3, 1, 2).double()
+    assert float((got - ref).norm() / ref.norm()) <= TOL[precision]
+    for M, K, N, (A, B, C) in mms:
+        exact = A.view(M, K).double() @ B.view(K, N).double()
+        assert float((C.view(M, N).double() - exact).norm() / exact.norm()) <= TOL[precision]
