@@ -194,7 +194,7 @@ def tune_batch(members, capture_stream=None, reps=3):
     same way.  Returns the Batch (captured on capture_stream if given), the
     tile policy and a report."""
     policies = {"current": [c.schedule(0) for c, _ in members]}
-    for v in (128, 129, 256, 257):  # tile width, +1: transposed epilogue
+    for v in (128, 129, 130, 256, 257):  # tile width | form (1: transposed epilogue, 2: 2 CTAs/SM)
         policies[f"all_{v}"] = [(0, 0, v)] * len(members)
     tuned = []
     for c, bufs in members:

@@ -47,11 +47,13 @@ constexpr int kEpiBytes = 8 * 32 * kEpiPitch * 4;
 
 // Tile shapes: BM x BN output tiles, BN = 256 (4-stage ring of 48 KB) or
 // BN = 128 (6-stage ring of 32 KB; narrow outputs and small problems).
-template <int BN_>
+// CTAS = 2: two CTAs share an SM (BN = 128, 3-stage rings, row-store
+// epilogue), each hiding the other's load latency and epilogue.
+template <int BN_, int CTAS = 1>
 struct Tile {
   static constexpr int B_BYTES = BN_ * BK * 2;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int STAGES = BN_ == 256 ? 4 : 6;
+  static constexpr int STAGES = CTAS == 2 ? 3 : BN_ == 256 ? 4 : 6;
   static constexpr uint32_t TMEM_COLS = 2 * BN_;  // two accumulator buffers
   static constexpr int HALF = BN_ / 2;            // columns per drain thread
   // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
@@ -163,8 +165,8 @@ __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, i
 
 // 10 warps per CTA: the SM's four register partitions (16K each) hold up to
 // three warps each, so at most 168 registers per thread.
-template <int BN, bool kTransposeEpi>
-__global__ void __launch_bounds__(NT, 1)
+template <int BN, bool kTransposeEpi, int CTAS>
+__global__ void __launch_bounds__(NT, CTAS)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
               float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
               const __grid_constant__ CUtensorMap single_a,
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(NT, 1)
               const __grid_constant__ CUtensorMap single_a2) {
   // probs == nullptr: one problem passed by value with its tensor maps as
   // kernel parameters (encoded at launch over per-run scratch)
-  using T = Tile<BN>;
+  using T = Tile<BN, CTAS>;
   constexpr int STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -675,29 +677,34 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
 __global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbImageJob J) {
   extern __shared__ float tile[];  // [64][wp + 1]
   const int cb = blockIdx.x, h = blockIdx.y, n = blockIdx.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int pitch = J.wp + 1;
   const int hs = h + J.off_h;  // source row
   const bool row_ok = hs >= 0 && hs < J.ub_h;
-  for (int idx = threadIdx.x; idx < 64 * J.wp; idx += blockDim.x) {
-    const int c = idx / J.wp, w = idx - c * J.wp;
-    const int ws = w + J.off_w;
-    float v = 0.f;
-    if (row_ok && ws >= 0 && ws < J.ub_w)
-      v = __ldg(J.base + J.off + (int64_t)n * J.ns + (int64_t)(cb * 64 + c) * J.cs +
-                (int64_t)h * J.wx + w);
-    tile[c * pitch + w] = v;
+  // warp per channel row, lanes along the columns (coalesced reads)
+  const float* src = J.base + J.off + (int64_t)n * J.ns + (int64_t)(cb * 64) * J.cs +
+                     (int64_t)h * J.wx;
+  for (int c = warp; c < 64; c += 8) {
+    const float* r = src + (int64_t)c * J.cs;
+    for (int w = lane; w < J.wp; w += 32) {
+      const int ws = w + J.off_w;
+      tile[c * pitch + w] = row_ok && ws >= 0 && ws < J.ub_w ? __ldg(r + w) : 0.f;
+    }
   }
   __syncthreads();
-  const int64_t row = (((int64_t)n * J.hp + h) * J.wp) * J.c + cb * 64;
-  for (int idx = threadIdx.x; idx < J.wp * 32; idx += blockDim.x) {
-    const int w = idx >> 5, cp = (idx & 31) * 2;
-    const float x0 = tile[cp * pitch + w], x1 = tile[(cp + 1) * pitch + w];
-    const __nv_bfloat162 hi = __floats2bfloat162_rn(x0, x1);
-    const int64_t o = row + (int64_t)w * J.c + cp;
-    *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(J.hi) + o) = hi;
-    if (J.lo) {
-      const float2 hf = __bfloat1622float2(hi);
-      *reinterpret_cast<__nv_bfloat162*>(static_cast<__nv_bfloat16*>(J.lo) + o) =
+  // warp per padded column, lanes over channel pairs (coalesced 128-byte rows)
+  __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(J.hi) +
+                      (((int64_t)n * J.hp + h) * J.wp) * J.c + cb * 64 + 2 * lane;
+  __nv_bfloat16* lo = J.lo ? static_cast<__nv_bfloat16*>(J.lo) +
+                                 (((int64_t)n * J.hp + h) * J.wp) * J.c + cb * 64 + 2 * lane
+                           : nullptr;
+  for (int w = warp; w < J.wp; w += 8) {
+    const float x0 = tile[2 * lane * pitch + w], x1 = tile[(2 * lane + 1) * pitch + w];
+    const __nv_bfloat162 hv = __floats2bfloat162_rn(x0, x1);
+    *reinterpret_cast<__nv_bfloat162*>(hi + (int64_t)w * J.c) = hv;
+    if (lo) {
+      const float2 hf = __bfloat1622float2(hv);
+      *reinterpret_cast<__nv_bfloat162*>(lo + (int64_t)w * J.c) =
           __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
     }
   }
@@ -814,20 +821,21 @@ cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t
   return cudaGetLastError();
 }
 
-template <int BN, bool TE>
+template <int BN, bool TE, int CTAS = 1>
 static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b,
                              const void* map_a2) {
   static bool attr = false;
-  const size_t smem = Tile<BN>::SMEM;
+  const size_t smem = Tile<BN, CTAS>::SMEM;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN, TE>,
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN, TE, CTAS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int grid = (int)(total_tiles < sms ? total_tiles : sms);
+  const int64_t slots = (int64_t)sms * CTAS;
+  const int grid = (int)(total_tiles < slots ? total_tiles : slots);
   LtbTcProblem one{};
   CUtensorMap ma{}, mb{}, ma2{};
   if (!d_probs) {
@@ -837,8 +845,8 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
     mb = *static_cast<const CUtensorMap*>(map_b);
     ma2 = map_a2 ? *static_cast<const CUtensorMap*>(map_a2) : ma;
   }
-  k_gemm_tc<BN, TE><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err, one, ma,
-                                            mb, ma2);
+  k_gemm_tc<BN, TE, CTAS><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err,
+                                                  one, ma, mb, ma2);
   return cudaGetLastError();
 }
 
@@ -855,6 +863,9 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
     case 129: LTB_TC(128, true);
     case 256: LTB_TC(256, false);
     case 257: LTB_TC(256, true);
+    case 130:  // 128 wide, two CTAs per SM
+      return launch_tc<128, false, 2>(d_probs, nprob, total_tiles, c_override, sms, err, st,
+                                      single, map_a, map_b, map_a2);
   }
 #undef LTB_TC
   return cudaErrorInvalidValue;

@@ -644,9 +644,12 @@ void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
 void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
   c->cfg[i] = cfg;
   const int g = c->gemm_of[i];
-  if (g >= 0 && c->gemms[g].tc) {  // variant: tile width, +1 for the transposed epilogue
-    const int bn = (cfg.variant & ~1) == 128 ? 128 : 256;
-    const int epi = cfg.variant & 1;
+  if (g >= 0 && c->gemms[g].tc) {
+    // variant: tile width | form, form 0: row-store epilogue, 1: transposed
+    // epilogue, 2: two CTAs per SM (128 wide only)
+    const int v = cfg.variant;
+    const int bn = v == 256 || v == 257 ? 256 : 128;
+    const int epi = v == 129 || v == 257 ? 1 : v == 130 ? 2 : 0;
     set_tile_n(c->gemms[g], bn, epi);
     c->cfg[i].variant = bn | epi;
     // cta_per_sm of a contraction: the raster group (row blocks swept together)
@@ -829,7 +832,9 @@ std::string describe(ltb_compiled* c, int i) {
     if (t.tc)
       o << "tile(128x" << t.bn << "x64) tensor_cores(tcgen05) parallel(persistent, "
         << t.tiles << " tiles) raster(" << (t.prob.group_m ? t.prob.group_m : 16)
-        << " row blocks) epilogue(" << (t.epi ? "smem transpose" : "row stores") << ")"
+        << " row blocks) epilogue("
+        << (t.epi == 1 ? "smem transpose" : t.epi == 2 ? "row stores, 2 CTAs/SM" : "row stores")
+        << ")"
         << (t.img ? " implicit_conv(A from NHWC image via 4-D TMA)" : "");
     else
       o << "tile(128x128) cuda_cores";
@@ -868,7 +873,7 @@ std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
     }
     case ltb::Family::contraction:
       if (c->gemms[c->gemm_of[i]].tc)
-        for (int v : {128, 129, 256, 257})
+        for (int v : {128, 129, 130, 256, 257})
           for (int gm : {0, 8, 32}) buf[n++] = LtbCfg{gm, 0, v};
       break;
   }
@@ -937,11 +942,11 @@ struct ltb_batch {
   int64_t pack_tiles = 0;
   int pack_chunk = 0, pack_cta_per_sm = 0;  // grouped pack schedule (0: defaults)
   std::vector<LtbImageJob> img_jobs;        // image operands, repacked before the pack
-  // tensor-core problems grouped by schedule variant (group 2 * (tile width
-  // == 256) + transposed epilogue), one persistent launch per non-empty group
-  LtbTcProblem* d_tc[4] = {nullptr, nullptr, nullptr, nullptr};
-  int ntc[4] = {0, 0, 0, 0};
-  int64_t tc_tiles[4] = {0, 0, 0, 0};
+  // tensor-core problems grouped by schedule variant (kGroupCode), one
+  // persistent launch per non-empty group
+  LtbTcProblem* d_tc[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int ntc[5] = {0, 0, 0, 0, 0};
+  int64_t tc_tiles[5] = {0, 0, 0, 0, 0};
   LtbGemmProblem* d_simt = nullptr;
   int64_t* d_simt_start = nullptr;
   int64_t simt_tiles = 0;
@@ -954,10 +959,19 @@ struct ltb_batch {
 
 namespace {
 
+constexpr int kGroupCode[5] = {128, 129, 256, 257, 130};  // launch variant per group
+
+int group_of(const GemmTables& t) {
+  const int v = t.bn | t.epi;
+  for (int g = 0; g < 5; ++g)
+    if (kGroupCode[g] == v) return g;
+  return 0;
+}
+
 void batch_gemms(ltb_batch* b, cudaStream_t st) {
-  for (int g = 0; g < 4; ++g)
+  for (int g = 0; g < 5; ++g)
     if (b->ntc[g])
-      CUDA_TRY(ltb_launch_gemm_tc((g >= 2 ? 256 : 128) | (g & 1), b->d_tc[g], b->ntc[g],
+      CUDA_TRY(ltb_launch_gemm_tc(kGroupCode[g], b->d_tc[g], b->ntc[g],
                                   b->tc_tiles[g], nullptr,
                                   b->sms, b->d_err, st));
 }
@@ -1001,8 +1015,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->device = cs[0]->device;
     b->sms = cs[0]->sms;
     std::vector<LtbPackJob> jobs;
-    std::vector<LtbTcProblem> tcp[4];
-    std::vector<unsigned char> maps[4];  // two 128-byte CUtensorMaps per problem
+    std::vector<LtbTcProblem> tcp[5];
+    std::vector<unsigned char> maps[5];  // two 128-byte CUtensorMaps per problem
     std::vector<LtbGemmProblem> sp;
     std::vector<int64_t> sstart;
     for (int i = 0; i < n; ++i) {
@@ -1063,7 +1077,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         b->owned.push_back(bp);
         if (!t.img) job(p.a, p.M, ap, t.a_mask, t.a_kcontig, t.a_off32);
         job(p.b, p.N, bp, t.b_mask, t.b_kcontig, t.b_off32);
-        const int grp = (t.bn == 256 ? 2 : 0) + t.epi;
+        const int grp = group_of(t);
         auto& mv = maps[grp];
         mv.resize(mv.size() + 384);  // A (hi image), B, A lo image
         unsigned char* m = mv.data() + mv.size() - 384;
@@ -1096,7 +1110,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->njobs = (int)jobs.size();
     if (b->tc) {
       b->d_jobs = upload(jobs, b->owned);
-      for (int g = 0; g < 4; ++g) {
+      for (int g = 0; g < 5; ++g) {
         // tensor maps in device memory (cudaMalloc is 256-byte aligned)
         unsigned char* d_maps = upload(maps[g], b->owned);
         for (size_t i = 0; i < tcp[g].size(); ++i) {
@@ -1225,11 +1239,14 @@ int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   if (k == "problems") *value = b->n;
   else if (k == "flops") *value = (int64_t)b->flops;
   else if (k == "launches")
-    *value = b->tc ? 1 + (b->ntc[0] > 0) + (b->ntc[1] > 0) + (b->ntc[2] > 0) + (b->ntc[3] > 0) : 1;
+    *value = b->tc ? 1 + (b->ntc[0] > 0) + (b->ntc[1] > 0) + (b->ntc[2] > 0) + (b->ntc[3] > 0) +
+                         (b->ntc[4] > 0)
+                   : 1;
   else if (k == "tiles")
-    *value = b->tc ? b->tc_tiles[0] + b->tc_tiles[1] + b->tc_tiles[2] + b->tc_tiles[3]
+    *value = b->tc ? b->tc_tiles[0] + b->tc_tiles[1] + b->tc_tiles[2] + b->tc_tiles[3] +
+                         b->tc_tiles[4]
                    : b->simt_tiles;
-  else if (k == "tiles_128") *value = b->tc_tiles[0] + b->tc_tiles[1];
+  else if (k == "tiles_128") *value = b->tc_tiles[0] + b->tc_tiles[1] + b->tc_tiles[4];
   else if (k == "tiles_256") *value = b->tc_tiles[2] + b->tc_tiles[3];
   else if (k == "graph") *value = b->exec ? 1 : 0;
   else if (k == "pack_chunk") *value = b->pack_chunk ? b->pack_chunk : 4;

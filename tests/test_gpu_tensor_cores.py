@@ -151,6 +151,21 @@ def test_conv_implicit_gemm(shape, precision, cuda_dev):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("variant", [128, 129, 130])
+def test_conv_implicit_every_variant(variant, cuda_dev):
+    """Every tile form of the implicit-GEMM convolution (row stores, shared
+    memory transposed epilogue, two CTAs per SM) agrees with FP64."""
+    import loop_tool_b200 as lt
+    from programs import conv
+
+    T, _ = conv(2, 64, 16, 16, 40, 3, 1, 1)
+    c = lt.cuda(T.ir, precision="bf16x3")
+    c.set_schedule(0, variant=variant)
+    assert c.schedule(0)[2] == variant and c.int_property("implicit_conv") == 1
+    _conv_check(c, 2, 64, 16, 16, 40, 3, 1, cuda_dev, TOL["bf16x3"])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
 def test_conv_implicit_in_batch(precision, cuda_dev):
     """An implicit-GEMM convolution and plain matmuls in one grouped launch."""
