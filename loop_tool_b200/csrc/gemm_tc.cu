@@ -4,26 +4,35 @@
 // contraction, hundreds for a batch of uneven matmuls in one launch).
 //
 // Operands arrive as dense K-major BF16 matrices A'[M, Kp], B'[N, Kp] made by
-// k_pack from the contraction's separable FP32 operand description (so the
-// same kernel runs matmul, batched matmul and padded convolution).  The
-// split-BF16 modes pack A' = [Ah | Al | Ah (| Al)], B' = [Bh | Bh | Bl (| Bl)]
-// along K, so one BF16 GEMM accumulates Ah*Bh + Al*Bh + Ah*Bl (+ Al*Bl).
+// the operand packer (k_pack_one / k_pack_grouped) from the contraction's
+// separable FP32 operand description, so the same kernel runs matmul,
+// batched matmul and gathered operands.  A convolution's input can instead
+// be an image operand: packed once as a zero-padded NHWC BF16 image
+// (k_pack_image) and loaded as 4-D TMA boxes per output image row (implicit
+// GEMM, no im2col matrix).  The split-BF16 modes pack A' = [Ah | Al | Ah
+// (| Al)], B' = [Bh | Bh | Bl (| Bl)] along K, so one BF16 GEMM accumulates
+// Ah*Bh + Al*Bh + Ah*Bl (+ Al*Bl).
 //
 // Chunked accumulation.  The tensor core's FP32 accumulation truncates, so
 // its error grows linearly with the number of K steps summed into one TMEM
 // accumulator (measured: ~1.9e-5 relative at K = 16384 with BF16-exact
-// inputs).  The K loop is therefore cut into chunks of kChunk elements, each
-// accumulated from zero in one of two TMEM buffers (256 columns each); drain
-// warps read a finished chunk back and add it into FP32 registers with
-// round-to-nearest adds while the tensor core fills the other buffer.  The
-// split-BF16 correction segments land in their own chunks, so they are never
-// truncated against the much larger main product.
+// inputs).  The K loop is therefore cut into chunks of 512 elements, each
+// accumulated from zero in one of two TMEM buffers; drain warps read a
+// finished chunk back (16 columns per tcgen05.ld) and add it into FP32
+// registers with round-to-nearest adds while the tensor core fills the other
+// buffer.  The split-BF16 correction segments land in their own chunks, so
+// they are never truncated against the much larger main product.
 //
-// Roles (320 threads per CTA, one CTA per SM):
+// Tile forms (a tuned schedule): 128 x 256 or 128 x 128 output tiles, one CTA
+// per SM (4- or 6-stage ring), or two 128 x 128 CTAs per SM (3-stage rings);
+// epilogue by per-thread row stores or through a 32 x 32 shared-memory
+// transpose into whole-row stores.
+//
+// Roles (320 threads per CTA):
 //   warp 0 lane 0 : TMA producer                  warp 0 : TMEM alloc/free
 //   warp 1 lane 0 : MMA issuer (4 x K=16 tcgen05.mma per 64-wide k block)
 //   warps 2..9    : drain + epilogue; warp w reads TMEM lanes 32*(w%4)..+31
-//                   and columns 128*((w-2)/4)..+127 of each 128 x 256 tile
+//                   and half (w-2)/4 of the tile's columns
 // Every wait is bounded: on timeout a flag is raised for the host
 // (LTB_ERR_TIMEOUT) and the CTA winds down without hanging.
 #include <cuda.h>

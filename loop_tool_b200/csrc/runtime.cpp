@@ -1196,8 +1196,9 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
     CUDA_TRY(cudaEventCreate(&e2));
     CUDA_TRY(cudaEventRecord(e0, st));
     for (const auto& j : b->img_jobs) CUDA_TRY(ltb_launch_pack_image(j, st));
-    if (b->tc) CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st, b->pack_chunk,
-                                     b->pack_cta_per_sm));
+    if (b->tc)
+      CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st,
+                                       b->pack_chunk, b->pack_cta_per_sm));
     CUDA_TRY(cudaEventRecord(e1, st));
     if (b->tc)
       batch_gemms(b, st);
