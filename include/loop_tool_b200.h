@@ -147,6 +147,22 @@ int ltb_batch_release(ltb_batch* b);
 int ltb_row_sum_noalloc(const float* x, int64_t rows, int64_t cols, float* out,
                         void* stream);
 
+/* ------------------------------------------------------- captured runs
+ * The reference launches a multi-kernel nest's kernels one by one from the
+ * host (and leaves nests that need a grid-wide sync unimplemented,
+ * src/backends/cuda/cuda.cpp:726-782).  ltb_graph_create captures one run
+ * of a compiled loop tree on fixed device or managed buffers -- operand
+ * packing, every stage, split-K combines -- into a CUDA graph;
+ * ltb_graph_run replays it with one launch, reading the buffers' current
+ * contents.  scratch: caller scratch as for ltb_run_with_scratch, or NULL
+ * for the compiled object's own.  Schedules changed after the capture are
+ * not seen by it; the compiled object must outlive the captured run. */
+typedef struct ltb_graph ltb_graph;
+int ltb_graph_create(ltb_compiled* c, void* const* memory, int n, void* scratch,
+                     void* stream, ltb_graph** out);
+int ltb_graph_run(ltb_graph* g, int sync, void* stream);
+int ltb_graph_release(ltb_graph* g);
+
 /* ---------------------------------------------------------- autotuner
  * Replaces the reference's manual schedule search: python/ui.py:34-45
  * (benchmark a tensor's loop tree) driving the LoopTree mutations of

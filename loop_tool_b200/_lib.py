@@ -61,6 +61,11 @@ SIGNATURES = {
                                         ctypes.c_int]),
     "ltb_tune_record": (ctypes.c_int, [ctypes.c_void_p]),
     "ltb_batch_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "ltb_graph_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "ltb_graph_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "ltb_graph_release": (ctypes.c_int, [ctypes.c_void_p]),
     "ltb_tune_save": (ctypes.c_int, [ctypes.c_char_p]),
     "ltb_tune_load": (ctypes.c_int, [ctypes.c_char_p]),
     "ltb_tune_clear": (ctypes.c_int, []),

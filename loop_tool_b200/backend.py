@@ -122,6 +122,11 @@ class Compiled:
                 "algorithmic_bytes", "flops", "tuned", "implicit_conv")
         return {k: self.int_property(k) for k in keys}
 
+    def capture(self, memory, stream=None, scratch=None):
+        """One run on these device buffers captured as a CUDA graph: every
+        launch of the loop tree replayed with one graph launch."""
+        return CapturedRun(self, memory, stream, scratch)
+
     # ------------------------------------------------------------ autotuner
     def tune(self, memory, reps=10, stream=None):
         """Time every candidate schedule of every stage on `memory` (device
@@ -171,6 +176,34 @@ class Compiled:
                     "algorithmic_bytes"):
             return self.int_property(name)
         raise AttributeError(name)
+
+
+class CapturedRun:
+    """A compiled loop tree's launches on fixed device buffers, captured
+    once into a CUDA graph (ltb_graph_create) and replayed by run()."""
+
+    def __init__(self, compiled, memory, stream=None, scratch=None):
+        self._compiled = compiled
+        self._keep = list(memory)
+        ptrs = [_ptr_and_keep(t)[0] for t in memory]
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        if stream is None:
+            stream = _current_stream()
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ltb_graph_create(compiled._h, arr, len(ptrs), scratch, stream,
+                                               ctypes.byref(h)))
+        self._h = h
+
+    def run(self, sync=True, stream=None):
+        if stream is None:
+            stream = _current_stream()
+        _lib.check(_lib.lib().ltb_graph_run(self._h, int(bool(sync)), stream))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib._lib is not None:
+            _lib.lib().ltb_graph_release(h)
+            self._h = None
 
 
 def _current_stream():

@@ -1405,6 +1405,102 @@ int ltb_free(void* ptr) {
   return LTB_OK;
 }
 
+// ------------------------------------------------------- captured runs
+struct ltb_graph {
+  ltb_compiled* c = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+int ltb_graph_create(ltb_compiled* c, void* const* memory, int n, void* scratch, void* stream,
+                     ltb_graph** out) {
+  if (!c || !memory || !out) return fail(LTB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  auto& P = c->plan;
+  if (n != P.n_in + P.n_out)
+    return fail(LTB_ERR_INVALID, "expected " + std::to_string(P.n_in + P.n_out) +
+                                     " buffers, got " + std::to_string(n));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStream_t own = nullptr;
+  auto g = new ltb_graph();
+  g->c = c;
+  try {
+    CUDA_TRY(cudaSetDevice(c->device));
+    LtbBufTable bt{};
+    for (int i = 0; i < n; ++i) {
+      if (!memory[i] || !is_device_accessible(memory[i]))
+        throw ltb::Error("captured runs need device or managed buffers");
+      bt.p[i] = static_cast<float*>(memory[i]);
+    }
+    if (!scratch) {
+      std::lock_guard<std::mutex> lock(c->mu);
+      if (!c->scratch && c->scratch_bytes) {
+        CUDA_TRY(cudaMalloc(&c->scratch, c->scratch_bytes));
+        c->owned.push_back(c->scratch);
+      }
+      scratch = c->scratch;
+    }
+    for (size_t k = 0; k < P.scratch_elems.size(); ++k)
+      bt.p[P.n_in + P.n_out + k] =
+          reinterpret_cast<float*>(static_cast<char*>(scratch) + c->scratch_off[k]);
+    if (!st) {  // the legacy default stream cannot be captured
+      CUDA_TRY(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+      st = own;
+    }
+    CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      launch_plan(c, bt, st);
+    } catch (...) {
+      cudaGraph_t tmp = nullptr;
+      cudaStreamEndCapture(st, &tmp);
+      if (tmp) cudaGraphDestroy(tmp);
+      throw;
+    }
+    CUDA_TRY(cudaStreamEndCapture(st, &g->graph));
+    CUDA_TRY(cudaGraphInstantiate(&g->exec, g->graph, 0));
+  } catch (const CudaFailure& e) {
+    if (own) cudaStreamDestroy(own);
+    ltb_graph_release(g);
+    return fail(LTB_ERR_CUDA, e.what());
+  } catch (const std::exception& e) {
+    if (own) cudaStreamDestroy(own);
+    ltb_graph_release(g);
+    return fail(LTB_ERR_INVALID, e.what());
+  }
+  if (own) cudaStreamDestroy(own);
+  *out = g;
+  return LTB_OK;
+}
+
+int ltb_graph_run(ltb_graph* g, int sync, void* stream) {
+  if (!g || !g->exec) return fail(LTB_ERR_INVALID, "null captured run");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  try {
+    CUDA_TRY(cudaSetDevice(g->c->device));
+    CUDA_TRY(cudaGraphLaunch(g->exec, st));
+    if (sync) {
+      CUDA_TRY(cudaStreamSynchronize(st));
+      int flag = 0;
+      CUDA_TRY(cudaMemcpy(&flag, g->c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (flag) {
+        CUDA_TRY(cudaMemset(g->c->d_err, 0, sizeof(int)));
+        return fail(LTB_ERR_TIMEOUT, "a bounded wait in a tensor-core kernel gave up");
+      }
+    }
+  } catch (const std::exception& e) {
+    return fail(LTB_ERR_CUDA, e.what());
+  }
+  return LTB_OK;
+}
+
+int ltb_graph_release(ltb_graph* g) {
+  if (!g) return LTB_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return LTB_OK;
+}
+
 // ------------------------------------------------------------ autotuner
 int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps, char* report,
              size_t len) {

@@ -18,6 +18,7 @@ reads (compile.cpp:653-660), so the reference's CPU backends run the same
 IR text with the same meaning.
 """
 import itertools
+import threading
 from collections import OrderedDict
 
 import numpy as np
@@ -696,34 +697,40 @@ def _resolve_sizes(t, sizes):
 # ------------------------------------------------------------ kernel cache
 _CACHE = OrderedDict()
 _CACHE_MAX = 4096
+_CACHE_LOCK = threading.Lock()  # serving threads share the cache
 
 
 def compiled(ir_text, **opts):
     """Compiled loop tree for an IR text, reused across calls (the
-    compilation cache of lazy.cpp:12-21, keyed by IR text + options)."""
+    compilation cache of lazy.cpp:12-21, keyed by IR text + options).
+    Thread-safe: concurrent callers of one key get one compiled object."""
     key = (ir_text, tuple(sorted(opts.items())))
-    c = _CACHE.get(key)
-    if c is None:
+    with _CACHE_LOCK:
+        c = _CACHE.get(key)
+        if c is not None:
+            _CACHE.move_to_end(key)
+            return c
         c = Compiled(ir_text, **opts)
         _CACHE[key] = c
         if len(_CACHE) > _CACHE_MAX:
             _CACHE.popitem(last=False)
-    else:
-        _CACHE.move_to_end(key)
-    return c
+        return c
 
 
 def cache_info():
-    return {"entries": len(_CACHE), "max": _CACHE_MAX}
+    with _CACHE_LOCK:
+        return {"entries": len(_CACHE), "max": _CACHE_MAX}
 
 
 def set_cache_limit(n):
     """Most compiled loop trees kept (least recently used evicted first)."""
     global _CACHE_MAX
-    _CACHE_MAX = max(1, int(n))
-    while len(_CACHE) > _CACHE_MAX:
-        _CACHE.popitem(last=False)
+    with _CACHE_LOCK:
+        _CACHE_MAX = max(1, int(n))
+        while len(_CACHE) > _CACHE_MAX:
+            _CACHE.popitem(last=False)
 
 
 def clear_cache():
-    _CACHE.clear()
+    with _CACHE_LOCK:
+        _CACHE.clear()
