@@ -72,7 +72,10 @@ int ltb_compile(const char* ir_text, const char* options, ltb_compiled** out);
  * written back by stream-ordered copies, complete once the stream is (pin
  * them for the copies to overlap).  Runs whose every buffer is in host
  * memory and whose loop tree is one linear elementwise map stage their
- * copies chunk by chunk on two streams (uploads overlap downloads). */
+ * copies chunk by chunk on two streams (uploads overlap downloads).
+ * Managed buffers are prefetched to the device before the launch and, for
+ * sync != 0, the outputs back to the host after it (bulk migration instead
+ * of demand paging; the reference frontend reads results on the host). */
 int ltb_run(ltb_compiled* c, void* const* memory, int n, int sync,
             void* stream);
 
@@ -102,8 +105,12 @@ int ltb_io_sizes(ltb_compiled* c, int* n_in, int* n_out, int64_t* elems,
                  int cap);
 
 /* Hardware "cuda" (CudaGPUHardware, src/backends/cuda/cuda.cpp:800-816):
- * alloc with managed != 0 is cudaMallocManaged like the reference (CPU
- * compatible); managed == 0 is plain device memory. */
+ * managed == 1 is cudaMallocManaged like the reference (CPU compatible);
+ * managed == 2 is pinned host memory (also CPU and GPU compatible: runs
+ * stage it through HBM with overlapped copies, and the CPU reads and writes
+ * it without page migration -- faster when every run's inputs are written
+ * and its outputs read on the host); managed == 0 is plain device memory.
+ * ltb_free releases any of them. */
 int ltb_alloc(size_t bytes, int managed, void** out);
 int ltb_free(void* ptr);
 

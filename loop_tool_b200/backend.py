@@ -292,13 +292,15 @@ def cuda(loop_tree, **opts):
 
 
 class RawTensor:
-    """Device buffer from the backend's "cuda" hardware allocator
-    (CudaGPUHardware::alloc/free, cuda.cpp:800-816)."""
+    """Buffer from the backend's "cuda" hardware allocator
+    (CudaGPUHardware::alloc/free, cuda.cpp:800-816): device memory, managed
+    memory (managed=True) or pinned host memory (pinned=True)."""
 
-    def __init__(self, size, managed=False):
+    def __init__(self, size, managed=False, pinned=False):
         self.size = int(size)
         p = ctypes.c_void_p()
-        _lib.check(_lib.lib().ltb_alloc(max(self.size, 1) * 4, int(managed), ctypes.byref(p)))
+        kind = 2 if pinned else int(bool(managed))
+        _lib.check(_lib.lib().ltb_alloc(max(self.size, 1) * 4, kind, ctypes.byref(p)))
         self.ptr = p.value
         self.managed = managed
 

@@ -542,6 +542,15 @@ bool is_device_accessible(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+bool is_managed(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeManaged;
+}
+
 // Launches of stage i (nothing for a row-chain member that is not the
 // chain's first stage: the chain launches as one kernel).
 cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStream_t st) {
@@ -735,6 +744,16 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
       if (sync) CUDA_TRY(cudaStreamSynchronize(st));
       return LTB_OK;
     }
+    // managed buffers (the reference's "cuda" hardware allocates them) move
+    // in bulk before the launch instead of page by page on first touch
+    std::vector<int> managed;
+    for (int i = 0; i < n; ++i)
+      if (is_managed(memory[i])) {
+        managed.push_back(i);
+        const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[i], 1) * 4;
+        if (cudaMemPrefetchAsync(memory[i], bytes, c->device, st) != cudaSuccess)
+          cudaGetLastError();  // advisory only
+      }
     for (int i = 0; i < n; ++i) {
       if (is_device_accessible(memory[i])) {
         bt.p[i] = static_cast<float*>(memory[i]);
@@ -759,6 +778,15 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
       CUDA_TRY(cudaMemcpyAsync(s.second, bt.p[s.first], bytes, cudaMemcpyDeviceToHost, st));
     }
     for (void* d : temps) CUDA_TRY(cudaFreeAsync(d, st));
+    // a synchronous run's managed outputs go back to the host in bulk: the
+    // caller waits for them in order to read them there
+    if (sync)
+      for (int i : managed)
+        if (i >= P.n_in) {
+          const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[i], 1) * 4;
+          if (cudaMemPrefetchAsync(memory[i], bytes, cudaCpuDeviceId, st) != cudaSuccess)
+            cudaGetLastError();
+        }
     // host outputs are written by stream-ordered copies: with sync == 0 they
     // are complete once the stream is (Compiled::async)
     if (sync) {
@@ -1387,8 +1415,10 @@ int ltb_io_sizes(ltb_compiled* c, int* n_in, int* n_out, int64_t* elems, int cap
 
 int ltb_alloc(size_t bytes, int managed, void** out) {
   if (!out) return fail(LTB_ERR_INVALID, "null output pointer");
-  cudaError_t e = managed ? cudaMallocManaged(out, bytes, cudaMemAttachGlobal)
-                          : cudaMalloc(out, bytes);
+  if (managed < 0 || managed > 2) return fail(LTB_ERR_INVALID, "bad allocation kind");
+  cudaError_t e = managed == 1   ? cudaMallocManaged(out, bytes, cudaMemAttachGlobal)
+                  : managed == 2 ? cudaHostAlloc(out, bytes, cudaHostAllocPortable)
+                                 : cudaMalloc(out, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(LTB_ERR_CUDA, std::string("allocation failed: ") + cudaGetErrorString(e));
@@ -1397,6 +1427,16 @@ int ltb_alloc(size_t bytes, int managed, void** out) {
 }
 
 int ltb_free(void* ptr) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, ptr) == cudaSuccess && a.type == cudaMemoryTypeHost) {
+    const cudaError_t e = cudaFreeHost(ptr);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(LTB_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return LTB_OK;
+  }
+  cudaGetLastError();
   cudaError_t e = cudaFree(ptr);
   if (e != cudaSuccess) {
     cudaGetLastError();

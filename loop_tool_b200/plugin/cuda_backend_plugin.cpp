@@ -36,12 +36,19 @@ bool autotune() {
   return a && std::string(a) == "1";
 }
 
+// LOOP_TOOL_B200_HOST_MEMORY=pinned: the "cuda" hardware hands out pinned
+// host memory instead of managed memory (both CPU and GPU compatible).
+int alloc_kind() {
+  const char* m = std::getenv("LOOP_TOOL_B200_HOST_MEMORY");
+  return m && std::string(m) == "pinned" ? 2 : 1;
+}
+
 // CudaGPUHardware (cuda.cpp:800-816): managed memory, usable by the CPU too.
 struct B200Hardware : public loop_tool::Hardware {
   B200Hardware() : Hardware("cuda", ltb_device_count()) {}
   loop_tool::Memory alloc(size_t size) override {
     void* p = nullptr;
-    ASSERT(ltb_alloc(size, 1, &p) == LTB_OK) << ltb_last_error();
+    ASSERT(ltb_alloc(size, alloc_kind(), &p) == LTB_OK) << ltb_last_error();
     return loop_tool::Memory{0x1 | (1 << id_), p};
   }
   void free(loop_tool::Memory& m) override {

@@ -73,3 +73,26 @@ def test_plugin_autotunes_and_persists_schedules(name, cuda_dev):
                 assert_accuracy(got, case["expected"], fp64_oracle(case), what=name)
             text = open(sched, "rb").read()
             assert text.startswith(b"loop_tool_b200 schedules 1\n") and b"\nentry " in text
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["add_4099", "softmax_16x4096", "mm_200x130x70",
+                                  "conv_2x4x8x8_pad1"])
+def test_plugin_pinned_host_memory(name, cuda_dev):
+    """LOOP_TOOL_B200_HOST_MEMORY=pinned: the "cuda" hardware allocates the
+    reference frontend's buffers as pinned host memory; results unchanged."""
+    if not (os.path.exists(HARNESS) and os.path.exists(PLUGIN)):
+        pytest.skip("reference CPU build (oracle/_ref) not present")
+    case = load(name)
+    with tempfile.TemporaryDirectory() as td:
+        for i, a in enumerate(case["inputs"]):
+            a.tofile(os.path.join(td, f"in{i}.f32"))
+        env = dict(os.environ, LT_PLUGIN=PLUGIN, LOOP_TOOL_B200_HOST_MEMORY="pinned")
+        r = subprocess.run([HARNESS, "lazyrun", td, td, case["program"],
+                            *map(str, case["params"])], env=env, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        got = np.fromfile(os.path.join(td, "out0.f32"), dtype=np.float32)
+    if case["program"] in EXACT_PROGRAMS:
+        assert_parity(got, case["expected"], True, what=name)
+    else:
+        assert_accuracy(got, case["expected"], fp64_oracle(case), what=name)
