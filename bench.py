@@ -593,17 +593,24 @@ def extra_c5(dev, n_requests, rates):
 
 
 # ------------------------------------------------------- profiling cases
-NCU_CASES = ("add", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "conv_bf16", "batch_bf16",
-             "mm_bf16_batch")
+NCU_CASES = ("add", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "mm_fp32", "conv_bf16",
+             "conv_fp32", "batch_bf16", "mm_bf16_batch")
 
 
-def ncu_case(name, reps, tune=True):
+def ncu_case(name, reps, tune=True, schedules=None):
     """One workload at a profiling size (inputs above L2, about 1 GB on the
     device), autotuned as in the benchmark, then run `reps` times inside the
-    NVTX range "profile" (capture with ncu --nvtx --nvtx-include profile/)."""
+    NVTX range "profile" (capture with ncu --nvtx --nvtx-include profile/).
+    With `schedules` (a file path): if the file exists its schedules are
+    loaded and nothing is tuned, else the tuned schedules are written there,
+    so a capture under ncu runs what the plain run before it chose."""
     import torch
 
     import loop_tool_b200 as ltb
+
+    if schedules and os.path.exists(schedules):
+        ltb.tune_load(schedules)
+        tune = False
 
     dev = torch.device("cuda", 0)
     g = torch.Generator(device=dev).manual_seed(9)
@@ -617,6 +624,8 @@ def ncu_case(name, reps, tune=True):
         bufs.append(torch.empty(n * n, device=dev))
         if tune:
             c.tune(bufs, reps=2)
+            if schedules:
+                ltb.tune_save(schedules)
         b = ltb.Batch([(c, bufs)])
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("profile")
@@ -627,8 +636,8 @@ def ncu_case(name, reps, tune=True):
         return
     elif name.startswith("mm_"):
         ir, opts = mm_ir(8192, 8192, 8192), {"precision": name[3:]}
-    elif name == "conv_bf16":
-        ir, opts = conv_ir(32), {"precision": "bf16"}
+    elif name.startswith("conv_"):
+        ir, opts = conv_ir(32), {"precision": name[5:]}
     else:
         rng = np.random.default_rng(401)
         v = np.exp(rng.uniform(math.log(64), math.log(4096), size=(128, 3)))
@@ -641,6 +650,8 @@ def ncu_case(name, reps, tune=True):
                                 torch.empty(M * N, device=dev)]))
         if tune:
             b, _, _ = ltb.tune_batch(members)
+            if schedules:
+                ltb.tune_save(schedules)
         else:
             b = ltb.Batch(members)
         torch.cuda.synchronize()
@@ -655,6 +666,9 @@ def ncu_case(name, reps, tune=True):
     bufs += [torch.empty(n, device=dev) for n in c.io_sizes[c.n_inputs:]]
     if tune:
         print(c.tune(bufs, reps=3))
+        if schedules:
+            ltb.tune_save(schedules)
+    print(c.code.splitlines()[-1] if c.code else "")
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_push("profile")
     for _ in range(reps):
@@ -678,11 +692,14 @@ def main():
     ap.add_argument("--ncu-case", choices=NCU_CASES,
                     help="run one workload at a profiling size and exit")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--schedules",
+                    help="with --ncu-case: schedule file written by a tuning run and loaded "
+                         "(no tuning) by a later run, e.g. the same case under ncu")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.ncu_case:
-        return ncu_case(args.ncu_case, args.reps, args.tune)
+        return ncu_case(args.ncu_case, args.reps, args.tune, args.schedules)
 
     import torch
 

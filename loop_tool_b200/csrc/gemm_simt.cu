@@ -1,35 +1,249 @@
 // Family (c), plain FP32 path: register-blocked CUDA-core GEMM over
 // "separable" operands, C[i, j] = sum_k A(i, k) * B(j, k) with
 //   A(i, k) = a.base[a.rowoff[i] + a.koff[k]]   (0 if a guard fails)
-// so the same kernel serves row-major matmul, transposed operands, batched
-// matmul (grid.z) and padded convolution as an implicit GEMM (the im2col
-// gather happens in the tile loader, never in HBM).
+// so the same kernel serves row-major matmul, transposed operands and padded
+// convolution as an implicit GEMM (the im2col gather happens in the tile
+// loader, never in HBM).  Every output is one FP32 FMA chain over k = 0..K-1
+// in order, whatever the tile loader's form.
+//
+// CTA tile 128 x 128, 16 k per step, 256 threads with 8 x 8 outputs each
+// (rows ty*4 + {0..3} and 64 + ty*4 + {0..3}, likewise columns); both
+// operand tiles sit in shared memory k-major ([16][128 + 4]) so a thread
+// reads its 8 A and 8 B values of one k as four 16-byte loads, double
+// buffered with the next step's global loads held in registers.  Each
+// operand is loaded in one of three forms chosen per launch
+// (ltb_simt_mode):
+//   kGather  any operand: offsets from tables (or computed for a dense
+//            operand), guards; one operand row per thread, fixed for the
+//            whole K loop (its row offset and guard partials stay in
+//            registers), 8 k per step -> a warp reads 32 neighbouring rows
+//   kVecK    dense with unit stride along k (row-major A): 16-byte loads of
+//            4 consecutive k, two rows per thread
+//   kVecR    dense with unit stride along rows (row-major B read by
+//            columns): 16-byte loads of 4 consecutive rows, two k per thread
+#include <stdint.h>
+
 #include "kernels.h"
 
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8, NT = 256;
+constexpr int BM = 128, BK = 16, NT = 256, LDS = BM + 4;
+constexpr int kHoistG = 4;  // guards whose row partials are kept in registers
 
-__device__ __forceinline__ float gather(const LtbGemmOperand& op, int64_t r,
-                                        int64_t k, int64_t rows, int64_t K) {
-  if (r >= rows || k >= K) return 0.f;
-  if (op.dense) return __ldg(op.base + r * op.ld_row + k * op.ld_k);
-  for (int g = 0; g < op.nguard; ++g) {
-    const int32_t v = op.grow[(int64_t)g * rows + r] + op.gk[(int64_t)g * K + k];
-    if (v < 0 || v >= op.gub[g]) return 0.f;
+struct Tile {
+  float s[2][BK][LDS];
+};
+
+// Loader of one operand for one CTA tile (rows row0 .. row0 + 127).  The
+// operand's fields are read in place from the launch parameters (constant
+// bank for single launches), not copied into registers.
+template <int MODE>
+struct Loader;
+
+template <>
+struct Loader<kSimtGather> {
+  const LtbGemmOperand& op;
+  const int64_t rows, K, r;  // r: this thread's row
+  int64_t off;               // element offset of that row
+  int32_t g[kHoistG];        // its guard partials (first kHoistG guards)
+  bool ok;
+  float v[8];
+
+  __device__ __forceinline__ Loader(const LtbGemmOperand& o, int64_t row0, int64_t rows_,
+                                    int64_t K_)
+      : op(o), rows(rows_), K(K_), r(row0 + (threadIdx.x & (BM - 1))) {
+    ok = r < rows;
+    off = 0;
+    if (ok) off = op.dense ? r * op.ld_row : op.rowoff[r];
+#pragma unroll
+    for (int q = 0; q < kHoistG; ++q)
+      g[q] = q < op.nguard && ok ? op.grow[(int64_t)q * rows + r] : 0;
   }
-  return __ldg(op.base + op.rowoff[r] + op.koff[k]);
+  __device__ __forceinline__ float one(int k) const {
+    if (!ok || k >= K) return 0.f;
+    const int ng = op.nguard;
+#pragma unroll
+    for (int q = 0; q < kHoistG; ++q)
+      if (q < ng && (uint32_t)(g[q] + op.gk[(int64_t)q * K + k]) >= (uint32_t)op.gub[q])
+        return 0.f;
+    for (int q = kHoistG; q < ng; ++q)
+      if ((uint32_t)(op.grow[(int64_t)q * rows + r] + op.gk[(int64_t)q * K + k]) >=
+          (uint32_t)op.gub[q])
+        return 0.f;
+    return __ldg(op.base + off + (op.dense ? k * op.ld_k : op.koff[k]));
+  }
+  __device__ __forceinline__ void fetch(int k0) {
+    const int kk0 = threadIdx.x >> 7;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = one(k0 + kk0 + 2 * q);
+  }
+  __device__ __forceinline__ void stash(float (*s)[LDS]) const {
+    const int c = threadIdx.x & (BM - 1), kk0 = threadIdx.x >> 7;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s[kk0 + 2 * q][c] = v[q];
+  }
+};
+
+template <>
+struct Loader<kSimtVecK> {
+  const float* p[2];  // row starts of this thread's two rows (null: past the end)
+  const int64_t K;
+  float4 v[2];
+
+  __device__ __forceinline__ Loader(const LtbGemmOperand& op, int64_t row0, int64_t rows,
+                                    int64_t K_)
+      : K(K_) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int64_t r = row0 + (threadIdx.x >> 2) + 64 * i;
+      p[i] = r < rows ? op.base + r * op.ld_row + (threadIdx.x & 3) * 4 : nullptr;
+    }
+  }
+  __device__ __forceinline__ void fetch(int k0) {
+    const bool kin = k0 + (threadIdx.x & 3) * 4 < K;  // K % 4 == 0: all 4 or none
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      v[i] = (p[i] && kin) ? __ldg(reinterpret_cast<const float4*>(p[i] + k0))
+                           : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __device__ __forceinline__ void stash(float (*s)[LDS]) const {
+    const int k = (threadIdx.x & 3) * 4, c = threadIdx.x >> 2;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      s[k + 0][c + 64 * i] = v[i].x;
+      s[k + 1][c + 64 * i] = v[i].y;
+      s[k + 2][c + 64 * i] = v[i].z;
+      s[k + 3][c + 64 * i] = v[i].w;
+    }
+  }
+};
+
+template <>
+struct Loader<kSimtVecR> {
+  const LtbGemmOperand& op;
+  const float* p;  // this thread's 4 rows at k = 0 (null: past the end)
+  const int64_t K;
+  float4 v[2];
+
+  __device__ __forceinline__ Loader(const LtbGemmOperand& o, int64_t row0, int64_t rows,
+                                    int64_t K_)
+      : op(o), K(K_) {
+    const int64_t r = row0 + (threadIdx.x & 31) * 4;  // rows % 4 == 0: all 4 or none
+    p = r < rows ? op.base + r : nullptr;
+  }
+  __device__ __forceinline__ void fetch(int k0) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int k = k0 + (threadIdx.x >> 5) + 8 * i;
+      v[i] = (p && k < K) ? __ldg(reinterpret_cast<const float4*>(p + (int64_t)k * op.ld_k))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  __device__ __forceinline__ void stash(float (*s)[LDS]) const {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      *reinterpret_cast<float4*>(&s[(threadIdx.x >> 5) + 8 * i][(threadIdx.x & 31) * 4]) = v[i];
+  }
+};
+
+template <int AM, int BMODE>
+__device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, int64_t j0) {
+  __shared__ __align__(16) Tile ta, tb;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // warps 4 (rows) x 2 (columns), lanes 4 x 8: a warp's A reads touch 4
+  // distinct 16-byte words and its B reads 8
+  const int ty = (warp >> 1) * 4 + (lane >> 3), tx = (warp & 1) * 8 + (lane & 7);
+  Loader<AM> la(p.a, i0, p.M, p.K);
+  Loader<BMODE> lb(p.b, j0, p.N, p.K);
+  float acc[8][8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.f;
+
+  const int nk = (int)((p.K + BK - 1) / BK);  // K <= kSimtMaxK (checked at launch)
+  la.fetch(0);
+  lb.fetch(0);
+  la.stash(ta.s[0]);
+  lb.stash(tb.s[0]);
+  __syncthreads();
+  for (int t = 0; t < nk; ++t) {
+    const int cur = t & 1;
+    if (t + 1 < nk) {
+      la.fetch((t + 1) * BK);
+      lb.fetch((t + 1) * BK);
+    }
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&ta.s[cur][kk][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&ta.s[cur][kk][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&tb.s[cur][kk][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&tb.s[cur][kk][64 + tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+    }
+    if (t + 1 < nk) {
+      la.stash(ta.s[cur ^ 1]);
+      lb.stash(tb.s[cur ^ 1]);
+    }
+    __syncthreads();
+  }
+
+  // epilogue: 16-byte stores where four neighbouring columns are adjacent
+  // and aligned in the output, scalar stores otherwise
+  int64_t c0[2];
+  bool cvec[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int64_t j = j0 + h * 64 + tx * 4;
+    c0[h] = j < p.N ? p.ccol[j] : 0;
+    cvec[h] = j + 3 < p.N && p.ccol[j + 1] == c0[h] + 1 && p.ccol[j + 2] == c0[h] + 2 &&
+              p.ccol[j + 3] == c0[h] + 3;
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int64_t i = i0 + (a >> 2) * 64 + ty * 4 + (a & 3);
+    if (i >= p.M) continue;
+    float* row = p.c + p.crow[i];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float* dst = row + c0[h];
+      if (cvec[h] && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+        *reinterpret_cast<float4*>(dst) =
+            make_float4(acc[a][h * 4], acc[a][h * 4 + 1], acc[a][h * 4 + 2], acc[a][h * 4 + 3]);
+      } else {
+        const int64_t j = j0 + h * 64 + tx * 4;
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (j + b < p.N) row[p.ccol[j + b]] = acc[a][h * 4 + b];
+      }
+    }
+  }
 }
 
-__device__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, int64_t j0);
+// CTAs per SM the register budget is sized for (launch bounds): two (128
+// registers per thread) hide load latency for gathered operands and small
+// grouped problems; a single launch of a row-major matmul (16-byte loads on
+// both sides) runs faster with one CTA and no register cap (measured:
+// 49 vs 44 TFLOP/s at 8192^3, 13.8 vs 11.7 at 1000^3).
+template <int AM, int BMODE>
+constexpr int simt_min_ctas() {
+  return AM == kSimtVecK && BMODE == kSimtVecR ? 1 : 2;
+}
 
-__global__ void __launch_bounds__(NT)
+template <int AM, int BMODE>
+__global__ void __launch_bounds__(NT, (simt_min_ctas<AM, BMODE>()))
     k_gemm_simt(LtbGemmProblem p) {
-  gemm_tile(p, (int64_t)blockIdx.y * BM, (int64_t)blockIdx.x * BN);
+  gemm_tile<AM, BMODE>(p, (int64_t)blockIdx.y * BM, (int64_t)blockIdx.x * BM);
 }
 
 // one CTA per 128 x 128 tile of any problem of the batch
-__global__ void __launch_bounds__(NT)
+template <int AM, int BMODE>
+__global__ void __launch_bounds__(NT, 2)
     k_gemm_simt_grouped(const LtbGemmProblem* __restrict__ probs,
                         const int64_t* __restrict__ tile_start, int nprob) {
   const int64_t t = blockIdx.x;
@@ -41,91 +255,76 @@ __global__ void __launch_bounds__(NT)
   }
   const LtbGemmProblem p = probs[lo];
   const int64_t lt = t - tile_start[lo];
-  const int64_t tn = (p.N + BN - 1) / BN;
-  gemm_tile(p, (lt / tn) * BM, (lt % tn) * BN);
+  const int64_t tn = (p.N + BM - 1) / BM;
+  gemm_tile<AM, BMODE>(p, (lt / tn) * BM, (lt % tn) * BM);
 }
 
-__device__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, int64_t j0) {
-  __shared__ float As[2][BK][BM];
-  __shared__ float Bs[2][BK][BN];
-  const int tid = threadIdx.x;
-  // loader mapping: A tile 128 rows x 8 k -> thread loads 4 k of one row
-  const int a_r = tid >> 1, a_k = (tid & 1) * 4;
-  // B tile 8 k x 128 cols -> thread loads 4 cols of one k
-  const int b_k = tid >> 5, b_c = (tid & 31) * 4;
-  const int ty = tid >> 4, tx = tid & 15;
-  float acc[TM][TN];
-#pragma unroll
-  for (int a = 0; a < TM; ++a)
-#pragma unroll
-    for (int b = 0; b < TN; ++b) acc[a][b] = 0.f;
+template <int AM, int BMODE>
+cudaError_t launch_one(const LtbGemmProblem& p, cudaStream_t st) {
+  dim3 grid((unsigned)((p.N + BM - 1) / BM), (unsigned)((p.M + BM - 1) / BM));
+  if (grid.y > 65535) return cudaErrorInvalidConfiguration;
+  k_gemm_simt<AM, BMODE><<<grid, NT, 0, st>>>(p);
+  return cudaGetLastError();
+}
 
-  float ra[4], rb[4];
-  auto fetch = [&](int64_t k0) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) ra[q] = gather(p.a, i0 + a_r, k0 + a_k + q, p.M, p.K);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) rb[q] = gather(p.b, j0 + b_c + q, k0 + b_k, p.N, p.K);
-  };
-  auto stash = [&](int buf) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) As[buf][a_k + q][a_r] = ra[q];
-    *reinterpret_cast<float4*>(&Bs[buf][b_k][b_c]) = make_float4(rb[0], rb[1], rb[2], rb[3]);
-  };
-  const int64_t nk = (p.K + BK - 1) / BK;
-  fetch(0);
-  stash(0);
-  __syncthreads();
-  for (int64_t t = 0; t < nk; ++t) {
-    const int cur = t & 1;
-    if (t + 1 < nk) fetch((t + 1) * BK);
-#pragma unroll
-    for (int kk = 0; kk < BK; ++kk) {
-      float av[TM], bv[TN];
-      const float4 a0 = *reinterpret_cast<const float4*>(&As[cur][kk][ty * 4]);
-      const float4 a1 = *reinterpret_cast<const float4*>(&As[cur][kk][64 + ty * 4]);
-      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[cur][kk][tx * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[cur][kk][64 + tx * 4]);
-      av[0] = a0.x; av[1] = a0.y; av[2] = a0.z; av[3] = a0.w;
-      av[4] = a1.x; av[5] = a1.y; av[6] = a1.z; av[7] = a1.w;
-      bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w;
-      bv[4] = b1.x; bv[5] = b1.y; bv[6] = b1.z; bv[7] = b1.w;
-#pragma unroll
-      for (int a = 0; a < TM; ++a)
-#pragma unroll
-        for (int b = 0; b < TN; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
-    }
-    if (t + 1 < nk) stash(cur ^ 1);
-    __syncthreads();
+template <int AM, int BMODE>
+cudaError_t launch_grouped(const LtbGemmProblem* d_probs, const int64_t* d_tile_start, int nprob,
+                           int64_t total_tiles, cudaStream_t st) {
+  k_gemm_simt_grouped<AM, BMODE><<<(unsigned)total_tiles, NT, 0, st>>>(d_probs, d_tile_start,
+                                                                        nprob);
+  return cudaGetLastError();
+}
+
+template <int AM>
+cudaError_t dispatch_b(int bm, const LtbGemmProblem* p, const LtbGemmProblem* d_probs,
+                       const int64_t* d_tile_start, int nprob, int64_t tiles, cudaStream_t st) {
+  switch (bm) {
+    case kSimtVecK:
+      return p ? launch_one<AM, kSimtVecK>(*p, st)
+               : launch_grouped<AM, kSimtVecK>(d_probs, d_tile_start, nprob, tiles, st);
+    case kSimtVecR:
+      return p ? launch_one<AM, kSimtVecR>(*p, st)
+               : launch_grouped<AM, kSimtVecR>(d_probs, d_tile_start, nprob, tiles, st);
+    default:
+      return p ? launch_one<AM, kSimtGather>(*p, st)
+               : launch_grouped<AM, kSimtGather>(d_probs, d_tile_start, nprob, tiles, st);
   }
-#pragma unroll
-  for (int a = 0; a < TM; ++a) {
-    const int64_t i = i0 + (a < 4 ? ty * 4 + a : 64 + ty * 4 + (a - 4));
-    if (i >= p.M) continue;
-    const int64_t rbase = p.crow[i];
-#pragma unroll
-    for (int b = 0; b < TN; ++b) {
-      const int64_t j = j0 + (b < 4 ? tx * 4 + b : 64 + tx * 4 + (b - 4));
-      if (j < p.N) p.c[rbase + p.ccol[j]] = acc[a][b];
-    }
+}
+
+cudaError_t dispatch(int modes, const LtbGemmProblem* p, const LtbGemmProblem* d_probs,
+                     const int64_t* d_tile_start, int nprob, int64_t tiles, cudaStream_t st) {
+  const int am = modes & 15, bm = (modes >> 4) & 15;
+  switch (am) {
+    case kSimtVecK:
+      return dispatch_b<kSimtVecK>(bm, p, d_probs, d_tile_start, nprob, tiles, st);
+    case kSimtVecR:
+      return dispatch_b<kSimtVecR>(bm, p, d_probs, d_tile_start, nprob, tiles, st);
+    default:
+      return dispatch_b<kSimtGather>(bm, p, d_probs, d_tile_start, nprob, tiles, st);
   }
 }
 
 }  // namespace
 
-cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms,
-                                 cudaStream_t st) {
+int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K) {
+  if (!op.dense || op.nguard != 0 || (reinterpret_cast<uintptr_t>(op.base) & 15) != 0)
+    return kSimtGather;
+  if (op.ld_k == 1 && op.ld_row % 4 == 0 && K % 4 == 0) return kSimtVecK;
+  if (op.ld_row == 1 && op.ld_k % 4 == 0 && rows % 4 == 0) return kSimtVecR;
+  return kSimtGather;
+}
+
+cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms, cudaStream_t st) {
   (void)sms;
-  dim3 grid((unsigned)((p.N + BN - 1) / BN), (unsigned)((p.M + BM - 1) / BM));
-  if (grid.y > 65535) return cudaErrorInvalidConfiguration;
-  k_gemm_simt<<<grid, NT, 0, st>>>(p);
-  return cudaGetLastError();
+  if (p.K > kSimtMaxK) return cudaErrorInvalidValue;
+  const int modes = ltb_simt_mode(p.a, p.M, p.K) | ltb_simt_mode(p.b, p.N, p.K) << 4;
+  return dispatch(modes, &p, nullptr, nullptr, 0, 0, st);
 }
 
 cudaError_t ltb_launch_gemm_simt_grouped(const LtbGemmProblem* d_probs,
                                          const int64_t* d_tile_start, int nprob,
-                                         int64_t total_tiles, cudaStream_t st) {
+                                         int64_t total_tiles, int modes, cudaStream_t st) {
   if (total_tiles > 0x7fffffff) return cudaErrorInvalidConfiguration;
-  k_gemm_simt_grouped<<<(unsigned)total_tiles, NT, 0, st>>>(d_probs, d_tile_start, nprob);
-  return cudaGetLastError();
+  if (total_tiles == 0) return cudaSuccess;
+  return dispatch(modes, nullptr, d_probs, d_tile_start, nprob, total_tiles, st);
 }

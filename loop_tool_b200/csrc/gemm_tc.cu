@@ -116,6 +116,11 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
          (uint64_t)1 << 46 | (uint64_t)2 << 61;
 }
 
+// An operand may also start at any 128-byte row inside a 1024-byte swizzle
+// atom (a halo tile read from row kw): the swizzle follows the absolute
+// shared-memory address bits, as the TMA wrote it, so the matrix base offset
+// field stays 0 (measured: setting it to the row phase gives wrong sums).
+
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
                                          uint32_t accumulate) {
   asm volatile(
@@ -174,7 +179,14 @@ __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, i
 
 // 10 warps per CTA: the SM's four register partitions (16K each) hold up to
 // three warps each, so at most 168 registers per thread.
-template <int BN, bool kTransposeEpi, int CTAS>
+// Halo tiles: resident B' (every 64-wide k block of the 128-row panel) and
+// a ring of at most kMaxHaloStages halo slots, within the 227 KB a CTA may
+// use.
+constexpr int kMaxHaloStages = 8;
+constexpr size_t kHaloSmemMax = 227 * 1024;
+constexpr size_t kHaloBBytes = (size_t)128 * BK * 2;
+
+template <int BN, bool kTransposeEpi, int CTAS, bool kHalo = false>
 __global__ void __launch_bounds__(NT, CTAS)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
               float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
@@ -188,9 +200,22 @@ __global__ void __launch_bounds__(NT, CTAS)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint64_t* empty = full + STAGES;
-  uint64_t* chunk_full = empty + STAGES;     // [2] MMA -> drain
+  // ring of STAGES slots, or (halo tiles) resident B' then the halo ring
+  int nst = STAGES;
+  uint32_t slot_bytes = STAGE_BYTES;
+  uint8_t* ring = smem;
+  uint8_t* bres = smem;  // halo tiles: B' k block kb at bres + kb * B_BYTES
+  int kbt = 0;
+  if constexpr (kHalo) {
+    kbt = (int)(single.Kp / BK);
+    ring = smem + (size_t)kbt * T::B_BYTES;
+    nst = single.img_stages;
+    slot_bytes = (uint32_t)single.img_slot_bytes;
+  }
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)nst * slot_bytes);
+  uint64_t* empty = full + nst;
+  uint64_t* b_full = empty + nst;            // halo tiles: resident B' loaded
+  uint64_t* chunk_full = b_full + 1;         // [2] MMA -> drain
   uint64_t* chunk_empty = chunk_full + 2;    // [2] drain -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(chunk_empty + 2);
   __shared__ float epi[kTransposeEpi ? 8 * 32 * kEpiPitch : 1];  // drain warps' transposes
@@ -199,10 +224,11 @@ __global__ void __launch_bounds__(NT, CTAS)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < nst; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
+    mbar_init(smem_u32(b_full), 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&chunk_full[b]), 1);
       mbar_init(smem_u32(&chunk_empty[b]), 8 * 32);  // every drain thread
@@ -220,7 +246,79 @@ __global__ void __launch_bounds__(NT, CTAS)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0 && lane == 0) {
+  if (kHalo && warp == 0 && lane == 0) {
+    // ------------------------------------------------- producer (halo tiles)
+    const LtbTcProblem& p = single;
+    mbar_expect_tx(smem_u32(b_full), (uint32_t)(kbt * T::B_BYTES));
+    for (int kb = 0; kb < kbt; ++kb)
+      tma_load_2d(smem_u32(bres + (size_t)kb * T::B_BYTES), &single_b, smem_u32(b_full), kb * BK,
+                  0);
+    const uint32_t box_bytes = (uint32_t)(p.img_rows * p.img_slot * 128);
+    uint32_t g = 0;  // stages issued
+    bool alive = true;
+    for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
+      int m0, n0;
+      tile_coords<BN>(p, t, &m0, &n0);
+      const int mt = m0 / BM, n_img = mt / p.img_hgroups;
+      const int ho0 = (mt - n_img * p.img_hgroups) * p.img_rows;
+      for (int kh = 0; kh < p.img_kh && alive; ++kh)
+        for (int cb = 0; cb < p.img_cblocks; ++cb, ++g) {
+          const int s = (int)(g % (uint32_t)nst);
+          if (!mbar_wait(smem_u32(&empty[s]), ((g / (uint32_t)nst) & 1u) ^ 1u, err)) {
+            alive = false;
+            break;
+          }
+          const uint32_t fb = smem_u32(&full[s]);
+          mbar_expect_tx(fb, box_bytes);
+          tma_load_4d(smem_u32(ring + (size_t)s * slot_bytes), &single_a, fb, cb * 64, 0,
+                      ho0 + kh, n_img);
+        }
+    }
+  } else if (kHalo && warp == 1 && lane == 0) {
+    // ----------------------------------------------- MMA issuer (halo tiles)
+    const LtbTcProblem& p = single;
+    uint32_t g = 0, q = 0;  // stages consumed, chunks produced
+    bool alive = mbar_wait(smem_u32(b_full), 0u, err);
+    const int nkb = kbt;
+    for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
+      int issued = 0, buf = 0;
+      uint32_t acc = tmem;
+      for (int kh = 0; kh < p.img_kh && alive; ++kh)
+        for (int cb = 0; cb < p.img_cblocks && alive; ++cb, ++g) {
+          const int s = (int)(g % (uint32_t)nst);
+          if (!mbar_wait(smem_u32(&full[s]), (g / (uint32_t)nst) & 1u, err)) {
+            alive = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a_slot = smem_u32(ring + (size_t)s * slot_bytes);
+          for (int kw = 0; kw < p.img_kw; ++kw) {
+            if (issued % kChunkBlocks == 0) {  // a new accumulation chunk
+              buf = (int)(q & 1u);
+              if (!mbar_wait(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
+                alive = false;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+              acc = tmem + (uint32_t)(buf * BN);
+            }
+            const int kb = (kh * p.img_kw + kw) * p.img_cblocks + cb;
+            const uint64_t ad = sw128_desc(a_slot + (uint32_t)kw * 128u);
+            const uint64_t bd = sw128_desc(smem_u32(bres + (size_t)kb * T::B_BYTES));
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+              mma_bf16(acc, ad + 2 * kk, bd + 2 * kk, T::IDESC,
+                       (issued % kChunkBlocks != 0) || (kk != 0));
+            ++issued;
+            if (issued % kChunkBlocks == 0 || issued == nkb) {
+              mma_commit(smem_u32(&chunk_full[buf]));  // chunk complete in TMEM
+              ++q;
+            }
+          }
+          mma_commit(smem_u32(&empty[s]));  // slot reusable once these finish
+        }
+    }
+  } else if (!kHalo && warp == 0 && lane == 0) {
     // ------------------------------------------------------------ producer
     uint32_t g = 0;  // k blocks issued by this CTA so far
     bool alive = true;
@@ -266,7 +364,7 @@ __global__ void __launch_bounds__(NT, CTAS)
         tma_load_2d(smem_u32(sa + A_BYTES), mb, fb, kb * BK, n0);
       }
     }
-  } else if (warp == 1 && lane == 0) {
+  } else if (!kHalo && warp == 1 && lane == 0) {
     // ---------------------------------------------------------- MMA issuer
     uint32_t g = 0, q = 0;  // k blocks consumed, chunks produced
     bool alive = true;
@@ -310,6 +408,11 @@ __global__ void __launch_bounds__(NT, CTAS)
       int m0, n0;
       tile_coords<BN>(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
+      // this thread's output row (row m0 + 32*quad + lane of the tile): its
+      // offset is loaded now, its latency hidden behind the chunk waits
+      int row;
+      const bool rvalid = tile_row(p, m0, quad * 32 + lane, &row);
+      const int64_t rbase = rvalid ? p.crow[row] : 0;
       float run[T::HALF];
 #pragma unroll
       for (int i = 0; i < T::HALF; ++i) run[i] = 0.f;
@@ -338,12 +441,10 @@ __global__ void __launch_bounds__(NT, CTAS)
       // epilogue: this warp owns rows m0 + 32*quad .. +31 (row m0 + 32*quad
       // + lane in this thread's registers) and HALF columns from cbase
       float* cb = c_override ? c_override : p.c;
-      int row;
-      const bool rvalid = tile_row(p, m0, quad * 32 + lane, &row);
       const int cbase = n0 + half * T::HALF;
       if (kTransposeEpi && p.unit_cols) {
         float* stage = epi + (warp - 2) * (32 * kEpiPitch);
-        const int64_t rb = rvalid ? p.crow[row] : 0;
+        const int64_t rb = rbase;
 #pragma unroll
         for (int c = 0; c < T::HALF; c += 32) {
           __syncwarp();
@@ -360,7 +461,6 @@ __global__ void __launch_bounds__(NT, CTAS)
           }
         }
       } else if (rvalid) {  // this thread's row: 16-byte stores where aligned
-        const int64_t rbase = p.crow[row];
         float* dst = cb + rbase;
 #pragma unroll
         for (int c = 0; c < T::HALF; c += 4) {
@@ -686,6 +786,9 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
 // Image operand repack: one CTA per (channel block of 64, padded row, image)
 // reads the 64 channel rows of x (coalesced along w) into shared memory and
 // writes the padded row [wp, 64] of BF16 channel pairs (coalesced along c).
+// The reads of a 160-column chunk are all issued before any is stored, so
+// each thread has up to 40 loads in flight.
+constexpr int kImgChunkJ = 5;  // 32-column slices per chunk
 __global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbImageJob J) {
   extern __shared__ float tile[];  // [64][wp + 1]
   const int cb = blockIdx.x, h = blockIdx.y, n = blockIdx.z;
@@ -693,15 +796,27 @@ __global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbI
   const int pitch = J.wp + 1;
   const int hs = h + J.off_h;  // source row
   const bool row_ok = hs >= 0 && hs < J.ub_h;
-  // warp per channel row, lanes along the columns (coalesced reads)
-  const float* src = J.base + J.off + (int64_t)n * J.ns + (int64_t)(cb * 64) * J.cs +
+  // warp per channel row (8 rows per warp), lanes along the columns
+  const float* src = J.base + J.off + (int64_t)n * J.ns + (int64_t)(cb * 64 + warp) * J.cs +
                      (int64_t)h * J.wx;
-  for (int c = warp; c < 64; c += 8) {
-    const float* r = src + (int64_t)c * J.cs;
-    for (int w = lane; w < J.wp; w += 32) {
-      const int ws = w + J.off_w;
-      tile[c * pitch + w] = row_ok && ws >= 0 && ws < J.ub_w ? __ldg(r + w) : 0.f;
-    }
+  for (int w0 = 0; w0 < J.wp; w0 += 32 * kImgChunkJ) {
+    float v[8][kImgChunkJ];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < kImgChunkJ; ++j) {
+        const int w = w0 + lane + 32 * j, ws = w + J.off_w;
+        v[i][j] = row_ok && w < J.wp && ws >= 0 && ws < J.ub_w
+                      ? __ldg(src + (int64_t)(8 * i) * J.cs + w)
+                      : 0.f;
+      }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < kImgChunkJ; ++j) {
+        const int w = w0 + lane + 32 * j;
+        if (w < J.wp) tile[(warp + 8 * i) * pitch + w] = v[i][j];
+      }
   }
   __syncthreads();
   // warp per padded column, lanes over channel pairs (coalesced 128-byte rows)
@@ -752,19 +867,39 @@ cudaError_t ltb_make_tmap(void* map, const void* base, int64_t rows, int64_t Kp,
 }
 
 cudaError_t ltb_make_tmap_image(void* map, const void* base, int n, int hp, int wp, int c,
-                                int wo) {
+                                int wo, int rows) {
   auto fn = encode_fn();
-  if (!fn || c % 64 || wo < 1 || wo > 256) return cudaErrorInvalidValue;
+  if (!fn || c % 64 || wo < 1 || wo > 256 || rows < 1 || rows > 256) return cudaErrorInvalidValue;
   const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)wp, (cuuint64_t)hp, (cuuint64_t)n};
   const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)wp * c * 2,
                                  (cuuint64_t)hp * wp * c * 2};
-  const cuuint32_t box[4] = {64, (cuuint32_t)wo, 1, 1};
+  const cuuint32_t box[4] = {64, (cuuint32_t)wo, (cuuint32_t)rows, 1};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn(reinterpret_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4,
                   const_cast<void*>(base), dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+bool ltb_tc_halo_geometry(LtbTcProblem& p, int wp) {
+  if (!p.img || p.N > 128 || p.Kp % BK || wp > 128) return false;
+  // a kw-shifted operand reads halo rows kw .. kw + 127
+  const int slot_bytes = ((127 + p.img_kw) * 128 + 1023) / 1024 * 1024;
+  const size_t fixed = (size_t)(p.Kp / BK) * kHaloBBytes + 1024 + 256;
+  if (fixed + 2 * (size_t)slot_bytes > kHaloSmemMax) return false;
+  int stages = (int)((kHaloSmemMax - fixed) / slot_bytes);
+  stages = stages < kMaxHaloStages ? stages : kMaxHaloStages;
+  const int nimg = p.tiles_m / p.img_hgroups;  // per-row form: tiles_m = nimg * hgroups
+  p.img_halo = 1;
+  p.img_slot = wp;
+  p.img_rows = 128 / wp;
+  p.img_hgroups = (p.img_ho + p.img_rows - 1) / p.img_rows;
+  p.tiles_m = nimg * p.img_hgroups;
+  p.tiles_n = 1;
+  p.img_stages = stages;
+  p.img_slot_bytes = slot_bytes;
+  return true;
 }
 
 cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st) {
@@ -833,16 +968,27 @@ cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t
   return cudaGetLastError();
 }
 
-template <int BN, bool TE, int CTAS = 1>
+static size_t halo_smem(const LtbTcProblem& p) {
+  return (size_t)(p.Kp / BK) * kHaloBBytes + (size_t)p.img_stages * p.img_slot_bytes + 1024 +
+         256;
+}
+
+template <int BN, bool TE, int CTAS = 1, bool HALO = false>
 static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b,
                              const void* map_a2) {
   static bool attr = false;
-  const size_t smem = Tile<BN, CTAS>::SMEM;
+  size_t smem = Tile<BN, CTAS>::SMEM;
+  if (HALO) {
+    if (d_probs || !single || !single->img_halo) return cudaErrorInvalidValue;
+    smem = halo_smem(*single);
+    if (smem > kHaloSmemMax) return cudaErrorInvalidValue;
+  }
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN, TE, CTAS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN, TE, CTAS, HALO>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(HALO ? kHaloSmemMax : smem));
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -857,8 +1003,8 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
     mb = *static_cast<const CUtensorMap*>(map_b);
     ma2 = map_a2 ? *static_cast<const CUtensorMap*>(map_a2) : ma;
   }
-  k_gemm_tc<BN, TE, CTAS><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override, err,
-                                                  one, ma, mb, ma2);
+  k_gemm_tc<BN, TE, CTAS, HALO><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override,
+                                                        err, one, ma, mb, ma2);
   return cudaGetLastError();
 }
 
@@ -878,6 +1024,9 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
     case 130:  // 128 wide, two CTAs per SM
       return launch_tc<128, false, 2>(d_probs, nprob, total_tiles, c_override, sms, err, st,
                                       single, map_a, map_b, map_a2);
+    case 131:  // 128 wide halo image tiles, resident weights
+      return launch_tc<128, false, 1, true>(d_probs, nprob, total_tiles, c_override, sms, err,
+                                            st, single, map_a, map_b, map_a2);
   }
 #undef LTB_TC
   return cudaErrorInvalidValue;

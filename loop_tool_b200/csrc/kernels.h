@@ -72,10 +72,17 @@ struct LtbGemmProblem {
 };
 
 // FP32 CUDA-core path (exact fp32 FMA): the "plain FP32" baseline family.
+// Operand tile loader forms (gemm_simt.cu); ltb_simt_mode picks the fastest
+// one the operand's layout allows.
+enum { kSimtGather = 0, kSimtVecK = 1, kSimtVecR = 2 };
+constexpr int64_t kSimtMaxK = (int64_t(1) << 31) - 64;  // k indices are 32-bit
+int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K);
 cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms,
                                  cudaStream_t st);
 // Many problems in one launch: tile_start[i] = first 128 x 128 tile of
-// problem i (device arrays), total_tiles tiles in all.
+// problem i (device arrays), total_tiles tiles in all; modes = A form |
+// B form << 4, a form every problem's operands allow (kSimtGather always
+// does).
 cudaError_t ltb_launch_gemm_simt_grouped(const LtbGemmProblem* d_probs,
                                          const int64_t* d_tile_start, int nprob,
-                                         int64_t total_tiles, cudaStream_t st);
+                                         int64_t total_tiles, int modes, cudaStream_t st);

@@ -93,16 +93,22 @@ struct GemmTables {
   int64_t img_elems = 0;              // elements of one image
   LtbImageJob ijob{};                 // base / hi / lo bound at launch
   int bn = 256;                       // tensor-core tile width (128 or 256)
-  int epi = 0;                        // 1: shared-memory transposed epilogue
+  int epi = 0;                        // 1: shared-memory transposed epilogue,
+                                      // 2: two CTAs per SM, 3: halo image tiles
+  // halo image tiles (single-segment image operands, N <= 128): the launch
+  // template in halo geometry, valid when halo_ok
+  LtbTcProblem halo{};
+  bool halo_ok = false;
 };
 
 // Tile width of a tensor-core contraction: output tiles are 128 x bn.
 void set_tile_n(GemmTables& t, int bn, int epi) {
+  if (epi == 3 && !(t.halo_ok && bn == 128)) epi = 0;
   t.bn = bn;
   t.epi = epi;
   const int64_t tn = (t.prob.N + bn - 1) / bn;
   t.prob.tiles_n = (int)tn;
-  t.tiles = (int64_t)t.prob.tiles_m * tn;
+  t.tiles = epi == 3 ? (int64_t)t.halo.tiles_m : (int64_t)t.prob.tiles_m * tn;
 }
 
 // All of a compiled object's constant device data (stage descriptors,
@@ -399,6 +405,10 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
       e.img_cblocks = (int)(ig.c / 64);
       e.img_a_mask = t.a_mask;
       e.tiles_m = (int)(ig.nimg * e.img_hgroups);
+      if (t.nseg == 1) {
+        t.halo = e;
+        t.halo_ok = ltb_tc_halo_geometry(t.halo, (int)wp);
+      }
       // B' in the image's K order: k' = (kh * KW + kw) * C + c
       std::vector<int64_t> kstride(kd.size());
       {
@@ -609,7 +619,10 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           j.hi = ap;
           j.lo = t.img_kinds == 2 ? static_cast<char*>(ap) + t.img_elems * 2 : nullptr;
           e = ltb_launch_pack_image(j, st);
-          if (e == cudaSuccess)
+          if (e == cudaSuccess && t.epi == 3)  // halo boxes: img_rows padded rows, full width
+            e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.halo.img_slot,
+                                    t.halo.img_rows);
+          else if (e == cudaSuccess)
             e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.prob.img_wo);
           if (e == cudaSuccess)
             e = ltb_make_tmap_image(maps + 256, j.lo ? j.lo : j.hi, j.nimg, j.hp, j.wp, j.c,
@@ -624,7 +637,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
                               c->sms, st);
         if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, t.bn);
         if (e == cudaSuccess) {
-          LtbTcProblem one = t.prob;
+          LtbTcProblem one = t.epi == 3 ? t.halo : t.prob;
+          one.group_m = t.prob.group_m;
           one.c = p.c;
           one.crow = t.c_row;
           one.ccol = t.c_col;
@@ -658,9 +672,9 @@ void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
     // epilogue, 2: two CTAs per SM (128 wide only)
     const int v = cfg.variant;
     const int bn = v == 256 || v == 257 ? 256 : 128;
-    const int epi = v == 129 || v == 257 ? 1 : v == 130 ? 2 : 0;
-    set_tile_n(c->gemms[g], bn, epi);
-    c->cfg[i].variant = bn | epi;
+    const int epi = v == 129 || v == 257 ? 1 : v == 130 ? 2 : v == 131 ? 3 : 0;
+    set_tile_n(c->gemms[g], bn, epi);  // 131 falls back to 128 without halo geometry
+    c->cfg[i].variant = bn | c->gemms[g].epi;
     // cta_per_sm of a contraction: the raster group (row blocks swept together)
     c->gemms[g].prob.group_m = cfg.cta_per_sm;
   }
@@ -863,7 +877,10 @@ std::string describe(ltb_compiled* c, int i) {
         << " row blocks) epilogue("
         << (t.epi == 1 ? "smem transpose" : t.epi == 2 ? "row stores, 2 CTAs/SM" : "row stores")
         << ")"
-        << (t.img ? " implicit_conv(A from NHWC image via 4-D TMA)" : "");
+        << (t.epi == 3 ? " implicit_conv(halo tiles: one 4-D TMA box per kernel row, kw shifts "
+                         "read in place; weights resident in shared memory)"
+            : t.img   ? " implicit_conv(A from NHWC image via 4-D TMA)"
+                      : "");
     else
       o << "tile(128x128) cuda_cores";
     return o.str();
@@ -900,9 +917,11 @@ std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
       break;
     }
     case ltb::Family::contraction:
-      if (c->gemms[c->gemm_of[i]].tc)
+      if (c->gemms[c->gemm_of[i]].tc) {
         for (int v : {128, 129, 130, 256, 257})
           for (int gm : {0, 8, 32}) buf[n++] = LtbCfg{gm, 0, v};
+        if (c->gemms[c->gemm_of[i]].halo_ok) buf[n++] = LtbCfg{0, 0, 131};
+      }
       break;
   }
   return std::vector<LtbCfg>(buf, buf + n);
@@ -978,6 +997,7 @@ struct ltb_batch {
   LtbGemmProblem* d_simt = nullptr;
   int64_t* d_simt_start = nullptr;
   int64_t simt_tiles = 0;
+  int simt_modes = 0;  // tile loader forms every FP32 member allows
   int* d_err = nullptr;
   double flops = 0;
   cudaGraph_t graph = nullptr;
@@ -1011,7 +1031,8 @@ void batch_launch(ltb_batch* b, cudaStream_t st) {
                                      b->pack_cta_per_sm));
     batch_gemms(b, st);
   } else {
-    CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles, st));
+    CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles,
+                                           b->simt_modes, st));
   }
 }
 
@@ -1127,9 +1148,12 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         q.crow = t.c_row;
         q.ccol = t.c_col;
         q.tile_start = b->tc_tiles[grp];
-        b->tc_tiles[grp] += t.tiles;
+        // halo tiles are a single-launch form: in a group the member runs
+        // its per-row image tiles at the same width
+        b->tc_tiles[grp] += t.epi == 3 ? (int64_t)t.prob.tiles_m * t.prob.tiles_n : t.tiles;
         tcp[grp].push_back(q);
       } else {
+        if (p.K > kSimtMaxK) throw ltb::Error("contraction too long for the FP32 kernel");
         sstart.push_back(b->simt_tiles);
         b->simt_tiles += ((p.M + 127) / 128) * ((p.N + 127) / 128);
         sp.push_back(p);
@@ -1152,6 +1176,15 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     } else {
       b->d_simt = upload(sp, b->owned);
       b->d_simt_start = upload(sstart, b->owned);
+      // one loader form per operand for the whole launch: the members' common
+      // form, else the gather form, which serves every operand
+      int am = -1, bm = -1;
+      for (const auto& q : sp) {
+        const int a = ltb_simt_mode(q.a, q.M, q.K), bb = ltb_simt_mode(q.b, q.N, q.K);
+        am = am < 0 || am == a ? a : kSimtGather;
+        bm = bm < 0 || bm == bb ? bb : kSimtGather;
+      }
+      b->simt_modes = std::max(am, 0) | std::max(bm, 0) << 4;
     }
     CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&b->d_err), sizeof(int)));
     b->owned.push_back(b->d_err);
@@ -1231,7 +1264,8 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
     if (b->tc)
       batch_gemms(b, st);
     else
-      CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles, st));
+      CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles,
+                                           b->simt_modes, st));
     CUDA_TRY(cudaEventRecord(e2, st));
     CUDA_TRY(cudaEventSynchronize(e2));
     CUDA_TRY(cudaEventElapsedTime(pack_ms, e0, e1));

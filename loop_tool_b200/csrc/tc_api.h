@@ -30,6 +30,16 @@ struct LtbTcProblem {
   int img_kh, img_kw, img_cblocks;
   int img_a_mask;        // bit s: segment s reads the hi image (1) or lo (0)
   const void* map_a2;    // image mode: CUtensorMap over the lo image
+  // Halo image tiles (single-segment image operands, N <= 128, single
+  // launches): img_slot = the padded width wp, so tile row i * wp + w is
+  // output column w of image row i; one 4-D box of img_rows padded rows per
+  // (kh, channel block) stage, and the kw shifts of that box are read by the
+  // MMA at row offsets of kw * 128 bytes.  B' stays resident in shared
+  // memory (every k block loaded once per CTA).
+  int img_halo;
+  int img_stages;        // halo ring depth
+  int img_slot_bytes;    // bytes per halo ring slot (1024-aligned)
+  int img_pad_;
 };
 
 // Repacks an image operand x(n, c, h + off_h, w + off_w) (FP32 at
@@ -47,9 +57,15 @@ struct LtbImageJob {
 };
 cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st);
 // CUtensorMap over an NHWC BF16 image [n, hp, wp, c] with boxes of
-// 64 channels x wo columns (128-byte swizzle): c % 64 == 0, wo <= 256.
+// 64 channels x wo columns x rows image rows (128-byte swizzle):
+// c % 64 == 0, wo <= 256, rows <= 256.
 cudaError_t ltb_make_tmap_image(void* map, const void* base, int n, int hp, int wp, int c,
-                                int wo);
+                                int wo, int rows = 1);
+// Halo tile geometry of an image problem (fills img_halo, img_slot,
+// img_rows, img_hgroups, tiles_m, img_stages, img_slot_bytes of p from its
+// per-row form); false if the weights or the ring do not fit in shared
+// memory.
+bool ltb_tc_halo_geometry(LtbTcProblem& p, int img_wp);
 
 // Load modes of the operand packer (ltb_pack_mode picks one per operand).
 enum { kPackDenseK = 0, kPackDenseR = 1, kPackGatherK = 2, kPackGatherR = 3 };
@@ -90,7 +106,9 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
 // (tiles_m * ceil(N / tile) tiles per problem, tile = bn & ~1 = 128 or 256:
 // the tile width the problems' tiles_n and B tensor maps were made for;
 // odd bn selects the epilogue that transposes 32 x 32 blocks through shared
-// memory into whole-row stores instead of per-thread 16-byte row stores).
+// memory into whole-row stores instead of per-thread 16-byte row stores;
+// 130: 128 wide, two CTAs per SM; 131: 128 wide halo image tiles with
+// resident weights, single problems only).
 // c_override, if not null, replaces every problem's output pointer.
 // d_probs == nullptr: a single problem passed by value with its two tensor
 // maps (host copies, passed as kernel parameters).

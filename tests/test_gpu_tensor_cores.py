@@ -165,6 +165,52 @@ def test_conv_implicit_every_variant(variant, cuda_dev):
     _conv_check(c, 2, 64, 16, 16, 40, 3, 1, cuda_dev, TOL["bf16x3"])
 
 
+# Halo image tiles (variant 131, BF16): one TMA box per kernel row covers the
+# tile's padded image rows; the kw shifts are read in place at row offsets
+# inside the 128-byte swizzle atoms; the weights stay in shared memory.
+# Shapes: partial last row group, several images, a 2 x 2 kernel, and the
+# 56 x 56 image with 128 output channels.  (N, C, H, W, CO, K, pad)
+HALO = [(2, 64, 8, 8, 16, 3, 1), (2, 64, 16, 16, 40, 3, 1), (2, 64, 17, 17, 24, 2, 0),
+        (4, 64, 32, 32, 128, 3, 1), (1, 64, 56, 56, 128, 3, 1)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", HALO)
+def test_conv_halo_tiles(shape, cuda_dev):
+    import loop_tool_b200 as lt
+    from programs import conv
+
+    N, C, H, W, CO, K, pad = shape
+    T, _ = conv(N, C, H, W, CO, K, pad, 1)
+    c = lt.cuda(T.ir, precision="bf16")
+    c.set_schedule(0, variant=131)
+    assert c.schedule(0)[2] == 131
+    _conv_check(c, N, C, H, W, CO, K, pad, cuda_dev, TOL["bf16"])
+    # and back to the per-row image tiles on the same compiled object
+    c.set_schedule(0, variant=128)
+    assert c.schedule(0)[2] == 128
+    _conv_check(c, N, C, H, W, CO, K, pad, cuda_dev, TOL["bf16"])
+
+
+@pytest.mark.gpu
+def test_conv_halo_not_applicable(cuda_dev):
+    """Weights too large for shared memory (C x KH x KW = 1152) or a split
+    precision: variant 131 falls back to the per-row image tiles."""
+    import loop_tool_b200 as lt
+    from programs import conv
+
+    T, _ = conv(1, 128, 10, 10, 24, 3, 0, 1)
+    c = lt.cuda(T.ir, precision="bf16")
+    c.set_schedule(0, variant=131)
+    assert c.schedule(0)[2] == 128
+    _conv_check(c, 1, 128, 10, 10, 24, 3, 0, cuda_dev, TOL["bf16"])
+    T, _ = conv(2, 64, 16, 16, 40, 3, 1, 1)
+    c = lt.cuda(T.ir, precision="bf16x3")
+    c.set_schedule(0, variant=131)
+    assert c.schedule(0)[2] == 128
+    _conv_check(c, 2, 64, 16, 16, 40, 3, 1, cuda_dev, TOL["bf16x3"])
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
 def test_conv_implicit_in_batch(precision, cuda_dev):
