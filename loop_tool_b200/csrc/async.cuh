@@ -10,6 +10,10 @@
 namespace {
 
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+// The error flag lives in global memory: a wait reads it only once it has
+// lasted this long (~50 us), so ordinary hand-offs never pay a global load's
+// latency between two polls of the barrier.
+constexpr long long kFlagCycles = 100000LL;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -36,7 +40,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* er
   if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles || *(volatile int*)err) {
+    const long long dt = clock64() - t0;
+    if (dt > kWaitCycles || (dt > kFlagCycles && *(volatile int*)err)) {
       atomicExch(err, 1);
       return false;
     }

@@ -146,6 +146,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
       : "r"(taddr));
 }
 
+// 32 bytes (8 floats) to a 32-byte aligned global address: one whole L2
+// sector per thread and instruction.
+__device__ __forceinline__ void st_global_v8(float* dst, const float* v) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "f"(v[0]),
+               "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -183,8 +191,12 @@ __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, i
 // a ring of at most kMaxHaloStages halo slots, within the 227 KB a CTA may
 // use.
 constexpr int kMaxHaloStages = 8;
+constexpr int kMaxHaloKb = 16;  // resident B' k blocks (one mbarrier each)
 constexpr size_t kHaloSmemMax = 227 * 1024;
 constexpr size_t kHaloBBytes = (size_t)128 * BK * 2;
+// barriers: full/empty per ring slot, one per resident k block, 2 + 2 chunk
+// barriers, the TMEM address word
+constexpr size_t kHaloBarBytes = (2 * kMaxHaloStages + kMaxHaloKb + 4) * 8 + 8;
 
 template <int BN, bool kTransposeEpi, int CTAS, bool kHalo = false>
 __global__ void __launch_bounds__(NT, CTAS)
@@ -214,8 +226,8 @@ __global__ void __launch_bounds__(NT, CTAS)
   }
   uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)nst * slot_bytes);
   uint64_t* empty = full + nst;
-  uint64_t* b_full = empty + nst;            // halo tiles: resident B' loaded
-  uint64_t* chunk_full = b_full + 1;         // [2] MMA -> drain
+  uint64_t* b_full = empty + nst;            // halo tiles: [kbt] resident B' k block loaded
+  uint64_t* chunk_full = b_full + (kHalo ? kbt : 1);  // [2] MMA -> drain
   uint64_t* chunk_empty = chunk_full + 2;    // [2] drain -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(chunk_empty + 2);
   __shared__ float epi[kTransposeEpi ? 8 * 32 * kEpiPitch : 1];  // drain warps' transposes
@@ -228,7 +240,7 @@ __global__ void __launch_bounds__(NT, CTAS)
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    mbar_init(smem_u32(b_full), 1);
+    for (int kb = 0; kb < (kHalo ? kbt : 1); ++kb) mbar_init(smem_u32(&b_full[kb]), 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&chunk_full[b]), 1);
       mbar_init(smem_u32(&chunk_empty[b]), 8 * 32);  // every drain thread
@@ -249,11 +261,8 @@ __global__ void __launch_bounds__(NT, CTAS)
   if (kHalo && warp == 0 && lane == 0) {
     // ------------------------------------------------- producer (halo tiles)
     const LtbTcProblem& p = single;
-    mbar_expect_tx(smem_u32(b_full), (uint32_t)(kbt * T::B_BYTES));
-    for (int kb = 0; kb < kbt; ++kb)
-      tma_load_2d(smem_u32(bres + (size_t)kb * T::B_BYTES), &single_b, smem_u32(b_full), kb * BK,
-                  0);
     const uint32_t box_bytes = (uint32_t)(p.img_rows * p.img_slot * 128);
+    bool first = true;  // the first tile also loads the resident B' blocks, in first-use order
     uint32_t g = 0;  // stages issued
     bool alive = true;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
@@ -268,17 +277,26 @@ __global__ void __launch_bounds__(NT, CTAS)
             alive = false;
             break;
           }
+          if (first)
+            for (int kw = 0; kw < p.img_kw; ++kw) {
+              const int kb = (kh * p.img_kw + kw) * p.img_cblocks + cb;
+              const uint32_t bb = smem_u32(&b_full[kb]);
+              mbar_expect_tx(bb, (uint32_t)T::B_BYTES);
+              tma_load_2d(smem_u32(bres + (size_t)kb * T::B_BYTES), &single_b, bb, kb * BK, 0);
+            }
           const uint32_t fb = smem_u32(&full[s]);
           mbar_expect_tx(fb, box_bytes);
           tma_load_4d(smem_u32(ring + (size_t)s * slot_bytes), &single_a, fb, cb * 64, 0,
                       ho0 + kh, n_img);
         }
+      first = false;
     }
   } else if (kHalo && warp == 1 && lane == 0) {
     // ----------------------------------------------- MMA issuer (halo tiles)
     const LtbTcProblem& p = single;
     uint32_t g = 0, q = 0;  // stages consumed, chunks produced
-    bool alive = mbar_wait(smem_u32(b_full), 0u, err);
+    bool alive = true;
+    bool first = true;  // B' blocks are waited for on first use
     const int nkb = kbt;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       int issued = 0, buf = 0;
@@ -303,6 +321,10 @@ __global__ void __launch_bounds__(NT, CTAS)
               acc = tmem + (uint32_t)(buf * BN);
             }
             const int kb = (kh * p.img_kw + kw) * p.img_cblocks + cb;
+            if (first && !mbar_wait(smem_u32(&b_full[kb]), 0u, err)) {
+              alive = false;
+              break;
+            }
             const uint64_t ad = sw128_desc(a_slot + (uint32_t)kw * 128u);
             const uint64_t bd = sw128_desc(smem_u32(bres + (size_t)kb * T::B_BYTES));
 #pragma unroll
@@ -317,6 +339,7 @@ __global__ void __launch_bounds__(NT, CTAS)
           }
           mma_commit(smem_u32(&empty[s]));  // slot reusable once these finish
         }
+      first = false;
     }
   } else if (!kHalo && warp == 0 && lane == 0) {
     // ------------------------------------------------------------ producer
@@ -460,18 +483,26 @@ __global__ void __launch_bounds__(NT, CTAS)
             if (vi && cok) cb[rbi + col] = stage[i * kEpiPitch + lane];
           }
         }
-      } else if (rvalid) {  // this thread's row: 16-byte stores where aligned
+      } else if (rvalid) {  // this thread's row: 32-byte (whole sector) stores where aligned
         float* dst = cb + rbase;
 #pragma unroll
-        for (int c = 0; c < T::HALF; c += 4) {
+        for (int c = 0; c < T::HALF; c += 8) {
           const int j = cbase + c;
-          if (p.unit_cols && j + 4 <= p.N && ((rbase + j) & 3) == 0) {
-            *reinterpret_cast<float4*>(dst + j) =
-                make_float4(run[c], run[c + 1], run[c + 2], run[c + 3]);
-          } else {
+          if (p.unit_cols && j + 8 <= p.N && (reinterpret_cast<uintptr_t>(dst + j) & 31) == 0) {
+            st_global_v8(dst + j, &run[c]);
+            continue;
+          }
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
-              if (j + e < p.N) dst[p.unit_cols ? j + e : p.ccol[j + e]] = run[c + e];
+          for (int h = 0; h < 8; h += 4) {
+            const int jh = j + h;
+            if (p.unit_cols && jh + 4 <= p.N && ((rbase + jh) & 3) == 0) {
+              *reinterpret_cast<float4*>(dst + jh) =
+                  make_float4(run[c + h], run[c + h + 1], run[c + h + 2], run[c + h + 3]);
+            } else {
+#pragma unroll
+              for (int e = 0; e < 4; ++e)
+                if (jh + e < p.N) dst[p.unit_cols ? jh + e : p.ccol[jh + e]] = run[c + h + e];
+            }
           }
         }
       }
@@ -789,9 +820,8 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
 // The reads of a 160-column chunk are all issued before any is stored, so
 // each thread has up to 40 loads in flight.
 constexpr int kImgChunkJ = 5;  // 32-column slices per chunk
-__global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbImageJob J) {
-  extern __shared__ float tile[];  // [64][wp + 1]
-  const int cb = blockIdx.x, h = blockIdx.y, n = blockIdx.z;
+__device__ __forceinline__ void pack_image_row(const LtbImageJob& J, int cb, int h, int n,
+                                               float* tile /* [64][wp + 1] */) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int pitch = J.wp + 1;
   const int hs = h + J.off_h;  // source row
@@ -835,6 +865,30 @@ __global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbI
           __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbImageJob J) {
+  extern __shared__ float tile[];  // [64][wp + 1]
+  pack_image_row(J, blockIdx.x, blockIdx.y, blockIdx.z, tile);
+}
+
+// A convolution's two operands in one launch: the first nb CTAs pack the
+// weight tiles (B'), the rest repack one image row each; the small weight
+// job runs beside the image instead of as a launch of its own.
+__global__ void __launch_bounds__(256, 3)
+    k_pack_conv(const __grid_constant__ LtbImageJob J, const __grid_constant__ LtbPackJob JB,
+                int64_t b_tiles, int nb) {
+  extern __shared__ float tile[];  // image: [64][wp + 1]; weights: [64][65]
+  __shared__ PackTables tabs;
+  const int b = blockIdx.x;
+  if (b < nb) {
+    const int64_t t0 = b_tiles * b / nb, t1 = b_tiles * (b + 1) / nb;
+    for (int64_t t = t0; t < t1; ++t)
+      pack_tile(JB, t, reinterpret_cast<float (*)[PR + 1]>(tile), &tabs);
+    return;
+  }
+  const int cblocks = J.c / 64, r = (b - nb) / cblocks;
+  pack_image_row(J, (b - nb) - r * cblocks, r % J.hp, r / J.hp, tile);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -883,10 +937,10 @@ cudaError_t ltb_make_tmap_image(void* map, const void* base, int n, int hp, int 
 }
 
 bool ltb_tc_halo_geometry(LtbTcProblem& p, int wp) {
-  if (!p.img || p.N > 128 || p.Kp % BK || wp > 128) return false;
+  if (!p.img || p.N > 128 || p.Kp % BK || wp > 128 || p.Kp / BK > kMaxHaloKb) return false;
   // a kw-shifted operand reads halo rows kw .. kw + 127
   const int slot_bytes = ((127 + p.img_kw) * 128 + 1023) / 1024 * 1024;
-  const size_t fixed = (size_t)(p.Kp / BK) * kHaloBBytes + 1024 + 256;
+  const size_t fixed = (size_t)(p.Kp / BK) * kHaloBBytes + 1024 + kHaloBarBytes;
   if (fixed + 2 * (size_t)slot_bytes > kHaloSmemMax) return false;
   int stages = (int)((kHaloSmemMax - fixed) / slot_bytes);
   stages = stages < kMaxHaloStages ? stages : kMaxHaloStages;
@@ -917,6 +971,31 @@ cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+static LtbPackJob make_pack_job(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
+                                int64_t Kp, int nseg, int seg_mask, int k_contig, int off32);
+
+cudaError_t ltb_launch_pack_conv(const LtbImageJob& j, const LtbGemmOperand& bop, int64_t rows,
+                                 int64_t K, void* out, int64_t Kp, int nseg, int seg_mask,
+                                 int k_contig, int off32, cudaStream_t st) {
+  if (j.c % 64 || j.wp < 1 || j.wp > 1024) return cudaErrorInvalidValue;
+  const LtbPackJob JB = make_pack_job(bop, rows, K, out, Kp, nseg, seg_mask, k_contig, off32);
+  const int64_t b_tiles = ltb_pack_tiles(rows, K);
+  const int64_t img_ctas = (int64_t)(j.c / 64) * j.hp * j.nimg;
+  const int nb = (int)(b_tiles < 64 ? b_tiles : 64);
+  if (img_ctas + nb > 0x7fffffff) return cudaErrorInvalidValue;
+  size_t smem = (size_t)64 * (j.wp + 1) * sizeof(float);
+  if (smem < (size_t)PKT * (PR + 1) * sizeof(float)) smem = (size_t)PKT * (PR + 1) * sizeof(float);
+  static size_t attr = 0;
+  if (smem > 40 * 1024 && smem > attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_pack_conv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = smem;
+  }
+  k_pack_conv<<<(unsigned)(img_ctas + nb), 256, smem, st>>>(j, JB, b_tiles, nb);
+  return cudaGetLastError();
+}
+
 int ltb_tc_tile_m() { return BM; }
 
 int ltb_pack_mode(const LtbGemmOperand& op, int64_t rows, int64_t K, int k_contig) {
@@ -937,9 +1016,8 @@ static int64_t pack_grid(int64_t tiles, int sms) {
   return tiles < g ? tiles : g;
 }
 
-cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
-                            int64_t Kp, int nseg, int seg_mask, int k_contig, int off32, int sms,
-                            cudaStream_t st) {
+static LtbPackJob make_pack_job(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
+                                int64_t Kp, int nseg, int seg_mask, int k_contig, int off32) {
   LtbPackJob J{};
   J.op = op;
   J.out = out;
@@ -951,6 +1029,13 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
   J.seg_mask = seg_mask;
   J.mode = ltb_pack_mode(op, rows, K, k_contig);
   J.off32 = off32;
+  return J;
+}
+
+cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
+                            int64_t Kp, int nseg, int seg_mask, int k_contig, int off32, int sms,
+                            cudaStream_t st) {
+  const LtbPackJob J = make_pack_job(op, rows, K, out, Kp, nseg, seg_mask, k_contig, off32);
   const int64_t tiles = ltb_pack_tiles(rows, K);
   if (tiles == 0) return cudaSuccess;
   k_pack_one<<<(unsigned)pack_grid(tiles, sms), PACK_THREADS, 0, st>>>(J, tiles);
@@ -970,7 +1055,7 @@ cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t
 
 static size_t halo_smem(const LtbTcProblem& p) {
   return (size_t)(p.Kp / BK) * kHaloBBytes + (size_t)p.img_stages * p.img_slot_bytes + 1024 +
-         256;
+         kHaloBarBytes;
 }
 
 template <int BN, bool TE, int CTAS = 1, bool HALO = false>

@@ -618,7 +618,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           j.base = p.a.base;
           j.hi = ap;
           j.lo = t.img_kinds == 2 ? static_cast<char*>(ap) + t.img_elems * 2 : nullptr;
-          e = ltb_launch_pack_image(j, st);
+          e = ltb_launch_pack_conv(j, p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig,
+                                   t.b_off32, st);
           if (e == cudaSuccess && t.epi == 3)  // halo boxes: img_rows padded rows, full width
             e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.halo.img_slot,
                                     t.halo.img_rows);
@@ -632,7 +633,7 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
                               c->sms, st);
           if (e == cudaSuccess) e = ltb_make_tmap(maps, ap, p.M, t.Kp, ltb_tc_tile_m());
         }
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && !t.img)  // image operands packed B' with the image
           e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, t.b_off32,
                               c->sms, st);
         if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, t.bn);

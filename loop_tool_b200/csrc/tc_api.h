@@ -56,6 +56,11 @@ struct LtbImageJob {
   void* lo;
 };
 cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st);
+// The image repack and the B' packing of the same contraction (arguments
+// as ltb_launch_pack) in one launch.
+cudaError_t ltb_launch_pack_conv(const LtbImageJob& j, const LtbGemmOperand& bop, int64_t rows,
+                                 int64_t K, void* out, int64_t Kp, int nseg, int seg_mask,
+                                 int k_contig, int off32, cudaStream_t st);
 // CUtensorMap over an NHWC BF16 image [n, hp, wp, c] with boxes of
 // 64 channels x wo columns x rows image rows (128-byte swizzle):
 // c % 64 == 0, wo <= 256, rows <= 256.
