@@ -272,16 +272,6 @@ def headline(args, world, rank, dev):
                                if ln.startswith("  ")]
     stream = torch.cuda.current_stream()
 
-    def step(times=None):
-        for i, ((_, c), b) in enumerate(zip(comps, bufs)):
-            if times is not None:
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-            c.run(b, sync=False)
-            if times is not None:
-                e1.record(stream)
-                times[i].append((e0, e1))
-
     # the three nests are independent programs: each runs on its own stream,
     # so one nest's tail overlaps the next one's start
     nest_streams = [torch.cuda.Stream() for _ in comps]
@@ -315,11 +305,19 @@ def headline(args, world, rank, dev):
     clocks = sampler.stop()
     ms = max_over_ranks(t0.elapsed_time(t1), dev)
     # per-nest device times (roofline of each kernel) from a serial pass
-    per = [[] for _ in comps]
-    for _ in range(args.steps):
-        step(per)
-    torch.cuda.synchronize()
-    nest_ms = [statistics.mean(a.elapsed_time(b) for a, b in lst) for lst in per]
+    # per-nest kernel times for the roofline: each nest alone, launched
+    # `steps` times back to back (steady state: a kernel's own L2 write-back
+    # lands in its own launches, not in the next nest's)
+    nest_ms = []
+    for (_, c), b in zip(comps, bufs):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c.run(b, sync=False)
+        e0.record(stream)
+        for _ in range(args.steps):
+            c.run(b, sync=False)
+        e1.record(stream)
+        e1.synchronize()
+        nest_ms.append(e0.elapsed_time(e1) / args.steps)
     step_bytes = sum(bytes_per)
     value = whole_job_gbs(step_bytes, args.steps, ms / 1e3, world)
 
@@ -356,6 +354,7 @@ def headline(args, world, rank, dev):
     s1.record(stream)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(s0.elapsed_time(s1) / 1e3 / e2e_steps, dev)
+    link = host_link_gbs(dev)
     h2d = sum(4 * sum(c.io_sizes[:c.n_inputs]) for _, c in comps)
     d2h = sum(4 * sum(c.io_sizes[c.n_inputs:]) for _, c in comps)
     hbm_peak, _, peak_kind = load_peaks()
@@ -370,7 +369,8 @@ def headline(args, world, rank, dev):
                                "64x128x112x112 (FP32 lazy-frontend loop trees)",
                    "l2": "inputs larger than L2 (126 MB), no flush needed",
                    "issue": "each step's three independent nests on three streams; per-nest "
-                            "times (roofline) from a serial pass",
+                            "times (roofline): each nest alone, launched `steps` times back "
+                            "to back",
                    "schedules": "autotuned before warm-up" if args.tune else "heuristic",
                    "parallelism": f"replicas{world}"},
         "schedules": schedules,
@@ -382,10 +382,35 @@ def headline(args, world, rank, dev):
                      "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": read_traffic().get(comps[dom][0])},
         "e2e": {"value": whole_job_gbs(step_bytes, 1, e2e_s, world), "unit": "GB/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "host_link_gbs": link},
         "gpu_launches": sum(c.int_property("launches") for _, c in comps) * args.steps,
         "clocks": clocks,
     }
+
+
+def host_link_gbs(dev, nbytes=256 << 20, reps=3):
+    """Plain pinned-memory copy bandwidth of this GPU's host link (GB/s per
+    direction, best of reps), the ceiling the e2e figure is read against."""
+    import torch
+
+    h = torch.empty(nbytes // 4, pin_memory=True)
+    d = torch.empty(nbytes // 4, device=dev)
+    out = {}
+    for name, fn in (("h2d", lambda: d.copy_(h, non_blocking=True)),
+                     ("d2h", lambda: h.copy_(d, non_blocking=True))):
+        fn()
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            best = max(best, nbytes / (a.elapsed_time(b) / 1e3) / 1e9)
+        out[name] = best
+    return out
 
 
 def timed(fn, reps, stream=None):

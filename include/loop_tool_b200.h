@@ -189,7 +189,12 @@ int ltb_graph_release(ltb_graph* g);
 int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps,
              char* report, size_t len);
 /* Read or set one stage's schedule (zeros = the built-in heuristic;
- * threads in {0, 64, 128, 256, 512}; variant: family-specific). */
+ * threads in {0, 64, 128, 256, 512}; variant: family-specific).  For a
+ * tensor-core contraction, variant = tile width | form: 128 / 256 row-store
+ * epilogue, 129 / 257 shared-memory transposed epilogue, 130 two 128-wide
+ * CTAs per SM, 131 halo image tiles with resident weights (single-segment
+ * convolutions whose weights fit in shared memory; elsewhere it reads back
+ * as 128); cta_per_sm is the raster group. */
 int ltb_get_schedule(ltb_compiled* c, int stage, int* cta_per_sm, int* threads,
                      int* variant);
 int ltb_set_schedule(ltb_compiled* c, int stage, int cta_per_sm, int threads,

@@ -259,6 +259,103 @@ __global__ void __launch_bounds__(NT, 2)
   gemm_tile<AM, BMODE>(p, (lt / tn) * BM, (lt % tn) * BM);
 }
 
+// ------------------------------------------------------------ 64 x 64 tiles
+// Problems with fewer 128 x 128 tiles than SMs: 64 x 64 CTA tiles, 256
+// threads with 4 x 4 outputs each (rows ty*4 + {0..3}, columns tx*4 +
+// {0..3}), 16 k per step, elements fetched one by one (dense offsets
+// computed, others from the tables, guards applied).  Each output is the
+// same FMA chain over k in order as in the 128 x 128 kernel, so both give
+// the same bits.
+constexpr int MBM = 64, MLD = MBM + 4;
+
+__device__ __forceinline__ float fetch_one(const LtbGemmOperand& op, int64_t r, int64_t k,
+                                           int64_t rows, int64_t K) {
+  if (r >= rows || k >= K) return 0.f;
+  if (op.dense) return __ldg(op.base + r * op.ld_row + k * op.ld_k);
+  for (int g = 0; g < op.nguard; ++g) {
+    const int32_t v = op.grow[(int64_t)g * rows + r] + op.gk[(int64_t)g * K + k];
+    if ((uint32_t)v >= (uint32_t)op.gub[g]) return 0.f;
+  }
+  return __ldg(op.base + op.rowoff[r] + op.koff[k]);
+}
+
+// 64 rows x 16 k of one operand, 4 elements per thread into s[k][row]:
+// lanes along k for a k-contiguous dense operand (a warp reads 8 rows x
+// 16 k), along rows otherwise (a warp reads 32 neighbouring rows of one k).
+struct MidLoader {
+  float v[4];
+  __device__ __forceinline__ void fetch(const LtbGemmOperand& op, int64_t row0, int64_t rows,
+                                        int64_t K, int k0, bool kfast) {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = kfast ? t >> 2 : t & 63, k = kfast ? (t & 3) * 4 + q : (t >> 6) + 4 * q;
+      v[q] = fetch_one(op, row0 + r, k0 + k, rows, K);
+    }
+  }
+  __device__ __forceinline__ void stash(float (*s)[MLD], bool kfast) const {
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = kfast ? t >> 2 : t & 63, k = kfast ? (t & 3) * 4 + q : (t >> 6) + 4 * q;
+      s[k][r] = v[q];
+    }
+  }
+};
+
+__global__ void __launch_bounds__(NT) k_gemm_simt_mid(LtbGemmProblem p) {
+  __shared__ __align__(16) float sa[2][BK][MLD], sb[2][BK][MLD];
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int64_t i0 = (int64_t)blockIdx.y * MBM, j0 = (int64_t)blockIdx.x * MBM;
+  const bool akf = p.a.dense && p.a.ld_k == 1, bkf = p.b.dense && p.b.ld_k == 1;
+  MidLoader la, lb;
+  float acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+  const int nk = (int)((p.K + BK - 1) / BK);  // K <= kSimtMaxK (checked at launch)
+  la.fetch(p.a, i0, p.M, p.K, 0, akf);
+  lb.fetch(p.b, j0, p.N, p.K, 0, bkf);
+  la.stash(sa[0], akf);
+  lb.stash(sb[0], bkf);
+  __syncthreads();
+  for (int t = 0; t < nk; ++t) {
+    const int cur = t & 1;
+    if (t + 1 < nk) {
+      la.fetch(p.a, i0, p.M, p.K, (t + 1) * BK, akf);
+      lb.fetch(p.b, j0, p.N, p.K, (t + 1) * BK, bkf);
+    }
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      const float4 a4 = *reinterpret_cast<const float4*>(&sa[cur][kk][ty * 4]);
+      const float4 b4 = *reinterpret_cast<const float4*>(&sb[cur][kk][tx * 4]);
+      const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+      const float bv[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+    }
+    if (t + 1 < nk) {
+      la.stash(sa[cur ^ 1], akf);
+      lb.stash(sb[cur ^ 1], bkf);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int64_t i = i0 + ty * 4 + a;
+    if (i >= p.M) continue;
+    float* row = p.c + p.crow[i];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int64_t j = j0 + tx * 4 + b;
+      if (j < p.N) row[p.ccol[j]] = acc[a][b];
+    }
+  }
+}
+
 template <int AM, int BMODE>
 cudaError_t launch_one(const LtbGemmProblem& p, cudaStream_t st) {
   dim3 grid((unsigned)((p.N + BM - 1) / BM), (unsigned)((p.M + BM - 1) / BM));
@@ -314,9 +411,23 @@ int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K) {
   return kSimtGather;
 }
 
-cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms, cudaStream_t st) {
-  (void)sms;
+int ltb_simt_tile(const LtbGemmProblem& p, int sms, int tile) {
+  if (tile == 64 || tile == 128) return tile;
+  const int64_t tiles128 = ((p.M + BM - 1) / BM) * ((p.N + BM - 1) / BM);
+  // 64-wide tiles pay scalar element fetches; they win only where 128-wide
+  // tiles leave most SMs idle (measured: 512^3 63 vs 69 us, 1000^3 134 vs
+  // 118 us)
+  return tiles128 * 4 <= sms ? 64 : 128;
+}
+
+cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms, cudaStream_t st, int tile) {
   if (p.K > kSimtMaxK) return cudaErrorInvalidValue;
+  if (ltb_simt_tile(p, sms, tile) == 64) {
+    dim3 grid((unsigned)((p.N + MBM - 1) / MBM), (unsigned)((p.M + MBM - 1) / MBM));
+    if (grid.y > 65535) return cudaErrorInvalidConfiguration;
+    k_gemm_simt_mid<<<grid, NT, 0, st>>>(p);
+    return cudaGetLastError();
+  }
   const int modes = ltb_simt_mode(p.a, p.M, p.K) | ltb_simt_mode(p.b, p.N, p.K) << 4;
   return dispatch(modes, &p, nullptr, nullptr, 0, 0, st);
 }

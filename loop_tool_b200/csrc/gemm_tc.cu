@@ -449,13 +449,18 @@ __global__ void __launch_bounds__(NT, CTAS)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t base =
             tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * BN + half * T::HALF);
+        // LD columns per wait: two loads in flight for 128-wide tiles; 256-wide
+        // tiles wait after each (their 128 running sums fill the register
+        // budget)
+        constexpr int LD = BN == 128 ? 32 : 16;
 #pragma unroll
-        for (int c = 0; c < T::HALF / 16; ++c) {  // 16 columns at a time: fewer live registers
-          uint32_t r[16];
-          tmem_ld16(base + (uint32_t)(c * 16), r);
+        for (int c = 0; c < T::HALF / LD; ++c) {
+          uint32_t r[LD];
+#pragma unroll
+          for (int u = 0; u < LD / 16; ++u) tmem_ld16(base + (uint32_t)(c * LD + u * 16), r + u * 16);
           tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i) run[c * 16 + i] += __uint_as_float(r[i]);
+          for (int i = 0; i < LD; ++i) run[c * LD + i] += __uint_as_float(r[i]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive(smem_u32(&chunk_empty[buf]));  // buffer free for the MMA

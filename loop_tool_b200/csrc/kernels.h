@@ -77,8 +77,13 @@ struct LtbGemmProblem {
 enum { kSimtGather = 0, kSimtVecK = 1, kSimtVecR = 2 };
 constexpr int64_t kSimtMaxK = (int64_t(1) << 31) - 64;  // k indices are 32-bit
 int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K);
+// tile: 128 (128 x 128 CTA tiles, the loader forms above), 64 (64 x 64
+// tiles for problems that 128-wide tiles leave SMs idle in), 0 = 64 when
+// there are at most SMs / 4 tiles of 128 x 128, else 128.  Same bits either
+// way.
 cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms,
-                                 cudaStream_t st);
+                                 cudaStream_t st, int tile = 0);
+int ltb_simt_tile(const LtbGemmProblem& p, int sms, int tile);
 // Many problems in one launch: tile_start[i] = first 128 x 128 tile of
 // problem i (device arrays), total_tiles tiles in all; modes = A form |
 // B form << 4, a form every problem's operands allow (kSimtGather always

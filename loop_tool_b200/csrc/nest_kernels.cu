@@ -725,7 +725,10 @@ __global__ void __launch_bounds__(256)
 // consecutive outputs; for each outer reduced coordinate it loads the
 // contiguous span of 3S+K inputs those outputs cover with 128-bit loads,
 // then folds in the reference's sequential order (exact for max/min).
-template <int S_, int K_>
+// U work items per thread per step (a tuned variant: 2 or 4) have all their
+// span loads issued before any fold; inputs and outputs are streamed (read
+// and written once, evict-first).
+template <int S_, int K_, int U>
 __global__ void __launch_bounds__(256)
     k_window(const LtbStage* __restrict__ gst, LtbBufTable bt, uint32_t nvec_mul,
              uint32_t nvec_shr) {
@@ -754,16 +757,14 @@ __global__ void __launch_bounds__(256)
   const uint32_t total = outer * nvec;
   const float* __restrict__ src = bt.p[L.buf];
   float* __restrict__ out = bt.p[S.out_buf];
-  // two work items per thread per step: their span loads are all issued
-  // before either fold, doubling the bytes in flight per thread
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t w0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w0 < total;
-       w0 += 2 * stride) {
-    int64_t base[2], obase[2];
-    int nv[2];
-    bool live[2];
+       w0 += U * stride) {
+    int64_t base[U], obase[U];
+    int nv[U];
+    bool live[U];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < U; ++u) {
       const uint64_t w = w0 + u * stride;
       live[u] = w < total;
       const uint32_t ww = (uint32_t)(live[u] ? w : w0);  // < total < 2^32
@@ -783,45 +784,45 @@ __global__ void __launch_bounds__(256)
       obase[u] = ob + o0;
       nv[u] = (int)(inner - o0 < 4 ? inner - o0 : 4);
     }
-    float acc[2][4];
+    float acc[U][4];
 #pragma unroll
-    for (int u = 0; u < 2; ++u)
+    for (int u = 0; u < U; ++u)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[u][j] = S.red_init;
 #pragma unroll 2
     for (int64_t rc = 0; rc < RC; ++rc) {
-      float span[2][N];
+      float span[U][N];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
+      for (int u = 0; u < U; ++u) {
         const float* p = src + base[u] + roff[rc];
         if (nv[u] == 4 && ((base[u] + roff[rc]) & 3) == 0) {
 #pragma unroll
           for (int q = 0; q + 4 <= N; q += 4) {
-            const float4 t = __ldg(reinterpret_cast<const float4*>(p + q));
+            const float4 t = __ldcs(reinterpret_cast<const float4*>(p + q));
             span[u][q] = t.x; span[u][q + 1] = t.y; span[u][q + 2] = t.z; span[u][q + 3] = t.w;
           }
 #pragma unroll
-          for (int q = N & ~3; q < N; ++q) span[u][q] = __ldg(p + q);
+          for (int q = N & ~3; q < N; ++q) span[u][q] = __ldcs(p + q);
         } else {
 #pragma unroll
           for (int q = 0; q < N; ++q)
-            span[u][q] = q <= (nv[u] - 1) * S_ + K_ - 1 ? __ldg(p + q) : 0.f;
+            span[u][q] = q <= (nv[u] - 1) * S_ + K_ - 1 ? __ldcs(p + q) : 0.f;
         }
       }
 #pragma unroll
-      for (int u = 0; u < 2; ++u)
+      for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int q = 0; q < K_; ++q)
 #pragma unroll
           for (int j = 0; j < 4; ++j) acc[u][j] = fold(S.red_op, acc[u][j], span[u][j * S_ + q]);
     }
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < U; ++u) {
       if (!live[u]) continue;
       float* o = out + obase[u];
       if (nv[u] == 4 && (obase[u] & 3) == 0) {
-        *reinterpret_cast<float4*>(o) =
-            make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+        __stcs(reinterpret_cast<float4*>(o),
+               make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]));
       } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -1111,11 +1112,30 @@ static int pick_threads(const LtbCfg& cfg, int dflt, int maxt) {
 
 static const int kWaves[] = {0, 1, 2, 4, 8, 16, 32};
 
+// Pooling-shaped reductions (k_window): one operand, unit-stride innermost
+// window, at most 64 outer window positions; *s = output stride, *k =
+// innermost window extent.
+static bool window_shape(const LtbStage& h, int64_t* s, int64_t* k) {
+  const LtbLoad& L0 = h.loads[0];
+  if (!(h.small && h.nout >= 1 && h.ndim > h.nout && h.nload == 1 && h.ninstr == 2 &&
+        h.code[0].op == LTB_V_LOAD && h.code[1].op == LTB_V_FOLD && L0.nq == 0 && L0.ng == 0 &&
+        h.out_coef[h.nout - 1] == 1 && L0.coef[h.ndim - 1] == 1 &&
+        h.red_total / h.size[h.ndim - 1] <= 64 && h.red_op != LTB_R_SUB &&
+        h.red_op != LTB_R_DIV && !h.kahan))
+    return false;
+  *s = L0.coef[h.nout - 1];
+  *k = h.size[h.ndim - 1];
+  return true;
+}
+
 int ltb_nest_candidates(const LtbStage& h, LtbCfg* out, int cap) {
   int n = 0;
+  int64_t s = 0, k = 0;
+  const bool win = !h.linear && h.nout >= 1 && h.size[h.nout - 1] >= 4 && window_shape(h, &s, &k);
   for (int w : kWaves)
     for (int t : {128, 256})
-      if (n < cap) out[n++] = LtbCfg{w, t, 0};
+      for (int v : {0, 4})  // pooling: 2 or 4 work items per thread
+        if (n < cap && (v == 0 || win)) out[n++] = LtbCfg{w, t, v};
   return n;
 }
 
@@ -1187,19 +1207,17 @@ cudaError_t ltb_launch_nest(const LtbStage* d_stage, const LtbStage& h,
   while (l < 32 && (int64_t(1) << l) < nvec) ++l;
   const uint32_t mul =
       (uint32_t)((((uint64_t(1) << 32) * ((uint64_t(1) << l) - (uint64_t)nvec)) / (uint64_t)nvec) + 1);
-  // pooling-shaped reductions: one operand, unit-stride innermost window
-  const LtbLoad& L0 = h.loads[0];
-  if (vec && h.small && h.nout >= 1 && h.ndim > h.nout && h.nload == 1 && h.ninstr == 2 &&
-      h.code[0].op == LTB_V_LOAD && h.code[1].op == LTB_V_FOLD && L0.nq == 0 && L0.ng == 0 &&
-      h.out_coef[h.nout - 1] == 1 && L0.coef[h.ndim - 1] == 1 &&
-      h.red_total / h.size[h.ndim - 1] <= 64 && h.red_op != LTB_R_SUB && h.red_op != LTB_R_DIV &&
-      !h.kahan) {
-    const int64_t s = L0.coef[h.nout - 1], k = h.size[h.ndim - 1];
-#define LTB_WIN(SS, KK)                                                             \
-  if (s == SS && k == KK) {                                                         \
-    k_window<SS, KK><<<grid_of(k_window<SS, KK>, work, threads, sms, cfg), threads, 0, \
-                       st>>>(d_stage, bt, mul, l);                                  \
-    return cudaGetLastError();                                                      \
+  int64_t s = 0, k = 0;
+  if (vec && window_shape(h, &s, &k)) {
+#define LTB_WIN(SS, KK)                                                                   \
+  if (s == SS && k == KK) {                                                               \
+    if (cfg.variant == 4)                                                                 \
+      k_window<SS, KK, 4><<<grid_of(k_window<SS, KK, 4>, work, threads, sms, cfg), threads, \
+                            0, st>>>(d_stage, bt, mul, l);                                \
+    else                                                                                  \
+      k_window<SS, KK, 2><<<grid_of(k_window<SS, KK, 2>, work, threads, sms, cfg), threads, \
+                            0, st>>>(d_stage, bt, mul, l);                                \
+    return cudaGetLastError();                                                            \
   }
     LTB_WIN(2, 2) LTB_WIN(1, 2) LTB_WIN(1, 3) LTB_WIN(2, 3) LTB_WIN(3, 3) LTB_WIN(1, 1)
     LTB_WIN(2, 1)

@@ -531,7 +531,8 @@ void compile_device(ltb_compiled* c) {
       if (st.rows_from == i) launches++;
     } else if (st.family == ltb::Family::contraction) {
       const auto& t = c->gemms[c->gemm_of[i]];
-      launches += (int)t.nbatch * (t.tc ? 3 : 1);
+      // tensor cores: pack A, pack B, GEMM (image operands: one packing launch)
+      launches += (int)t.nbatch * (t.tc ? (t.img ? 2 : 3) : 1);
     } else {
       launches += c->split_of[i] > 1 ? 2 : 1;
     }
@@ -607,7 +608,7 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         p.N = s.con.N;
         p.K = s.con.K;
         if (!t.tc) {
-          e = ltb_launch_gemm_simt(p, c->sms, st);
+          e = ltb_launch_gemm_simt(p, c->sms, st, cfg.variant);
           continue;
         }
         void* ap = bt.p[t.a_slot];
@@ -882,8 +883,13 @@ std::string describe(ltb_compiled* c, int i) {
                          "read in place; weights resident in shared memory)"
             : t.img   ? " implicit_conv(A from NHWC image via 4-D TMA)"
                       : "");
-    else
-      o << "tile(128x128) cuda_cores";
+    else {
+      LtbGemmProblem q{};
+      q.M = s.con.M;
+      q.N = s.con.N;
+      const int tile = ltb_simt_tile(q, c->sms, f.variant);
+      o << "tile(" << tile << "x" << tile << ") cuda_cores";
+    }
     return o.str();
   }
   o << "parallel(grid=SMs x " << (f.cta_per_sm ? std::to_string(f.cta_per_sm) : "resident")
@@ -922,6 +928,9 @@ std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
         for (int v : {128, 129, 130, 256, 257})
           for (int gm : {0, 8, 32}) buf[n++] = LtbCfg{gm, 0, v};
         if (c->gemms[c->gemm_of[i]].halo_ok) buf[n++] = LtbCfg{0, 0, 131};
+      } else {  // CUDA-core tiles
+        buf[n++] = LtbCfg{0, 0, 64};
+        buf[n++] = LtbCfg{0, 0, 128};
       }
       break;
   }

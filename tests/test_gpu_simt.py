@@ -5,7 +5,9 @@ gather form (tables, guards, ragged or unaligned operands).  Every layout is
 checked against the FP64 oracle; and since every output is one FP32 FMA
 chain over k in order, the same product read through a vector form and
 through the gather form (an operand buffer offset by one element, which
-rules out 16-byte loads) must agree bit for bit."""
+rules out 16-byte loads) must agree bit for bit.  Problems with few
+128 x 128 tiles run 64 x 64 tiles by default; the large shapes below take
+the 128-wide loader forms."""
 import numpy as np
 import pytest
 
@@ -14,7 +16,8 @@ import pytest
 # include K, M, N not multiples of 4 (no vector form).
 LAYOUTS = [("nn", 130, 68, 20), ("nn", 65, 37, 50), ("nn", 200, 36, 132), ("nn", 1, 300, 8),
            ("tn", 132, 36, 68), ("tn", 67, 20, 30), ("nt", 130, 68, 20), ("nt", 33, 19, 129),
-           ("tt", 64, 40, 100), ("tt", 9, 7, 5), ("nn", 257, 1000, 260)]
+           ("tt", 64, 40, 100), ("tt", 9, 7, 5), ("nn", 257, 1000, 260),
+           ("nn", 1664, 36, 1540), ("tn", 1540, 20, 1664), ("nt", 1500, 37, 1500)]
 
 
 def _program(layout, M, K, N):
@@ -73,6 +76,34 @@ def test_fp32_layouts_vs_oracle_and_forms(case, cuda_dev):
     exact = _oracle(ir, [a[:-1].cpu().numpy(), b[:-1].cpu().numpy()]).ravel()
     err = float(np.linalg.norm(outs[0] - exact) / np.linalg.norm(exact))
     assert err <= 1e-6, f"normwise error {err:.3g}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [("nn", 130, 68, 20), ("nt", 33, 19, 129), ("tn", 67, 20, 30),
+                                  ("nn", 1500, 70, 1300), ("tt", 200, 33, 1400)],
+                         ids=lambda c: "%s_%dx%dx%d" % c)
+def test_fp32_tile_sizes_same_bits(case, cuda_dev):
+    """64 x 64 and 128 x 128 CUDA-core tiles (a tuned choice; small problems
+    default to 64) run the same FMA chain per output: identical bits."""
+    import torch
+
+    import loop_tool_b200 as ltb
+
+    layout, M, K, N = case
+    c = ltb.Compiled(_program(layout, M, K, N))
+    g = torch.Generator(device=cuda_dev).manual_seed(M + K + N)
+    a = torch.randn(M * K, device=cuda_dev, generator=g)
+    b = torch.randn(K * N, device=cuda_dev, generator=g)
+    outs = []
+    for tile in (64, 128):
+        c.set_schedule(0, variant=tile)
+        assert c.schedule(0)[2] == tile
+        out = torch.full((M * N,), float("nan"), device=cuda_dev)
+        c([a, b, out])
+        torch.cuda.synchronize()
+        outs.append(out)
+    assert torch.isfinite(outs[0]).all()
+    assert torch.equal(outs[0], outs[1])
 
 
 @pytest.mark.gpu

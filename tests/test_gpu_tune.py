@@ -81,6 +81,36 @@ def test_every_softmax_schedule_agrees(cols, cuda_dev):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("shape,k,st", [((3, 5, 112, 112), 2, 2), ((2, 3, 37, 42), 2, 2),
+                                        ((2, 4, 30, 30), 3, 3), ((1, 2, 17, 21), 3, 2)])
+def test_every_pool_schedule_exact(shape, k, st, cuda_dev):
+    """Max-pool through the window kernel with 2 and 4 work items per thread
+    (variant 0 / 4), every grid and CTA size: bit-identical to torch's
+    max_pool2d, ragged rows and partial vectors included."""
+    import torch
+
+    import loop_tool_b200 as ltb
+    from programs import maxpool
+
+    N, C, H, W = shape
+    T, _ = maxpool(N, C, H, W, k, st)
+    c = ltb.Compiled(T.ir)
+    g = torch.Generator(device=cuda_dev).manual_seed(H * W + k)
+    x = torch.randn(N * C * H * W, device=cuda_dev, generator=g)
+    ref = torch.nn.functional.max_pool2d(x.view(N, C, H, W), k, st).flatten()
+    y = torch.empty(c.io_sizes[-1], device=cuda_dev)
+    assert y.numel() == ref.numel()
+    for variant in (0, 4):
+        for w in (0, 1, 8):
+            for t in (128, 256):
+                c.set_schedule(0, cta_per_sm=w, threads=t, variant=variant)
+                y.fill_(float("nan"))
+                c([x, y])
+                torch.cuda.synchronize()
+                assert torch.equal(y, ref), (variant, w, t)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
 @pytest.mark.parametrize("name", ["mm_200x130x70", "conv_2x4x8x8_pad1", "bmm_3x16x8x24"])
 def test_tile_widths_agree(name, precision, cuda_dev):
