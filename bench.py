@@ -444,12 +444,19 @@ def extra_c1(dev):
         c = ltb.Compiled(ir, precision=prec)
         C = torch.empty(128 * 128, device=dev)
         us = timed(lambda: c.run([A, B, C], sync=False), 200) * 1e3
+        # device time per call: the same run captured once and replayed (no
+        # Python / ABI overhead between launches)
+        cap = c.capture([A, B, C])
+        graph_us = timed(lambda: cap.run(sync=False), 200) * 1e3
+        del cap
         ch = np.empty(128 * 128, np.float32)
         w0 = time.perf_counter()
         for _ in range(50):
             c([a, b, ch])
         e2e_us = (time.perf_counter() - w0) / 50 * 1e6
         res = {"device_us_per_call": us, "gflops": 2 * 128 ** 3 / (us * 1e-6) / 1e9,
+               "graph_replay_us_per_call": graph_us,
+               "gflops_graph_replay": 2 * 128 ** 3 / (graph_us * 1e-6) / 1e9,
                "e2e_us_per_call_host_buffers": e2e_us}
         # checked against the reference CPU backend on the same IR
         if os.path.exists(HARNESS):

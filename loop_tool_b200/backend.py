@@ -50,10 +50,21 @@ def device_count():
     return _lib.lib().ltb_device_count()
 
 
+_TORCH_F32 = []  # torch.float32, looked up once (torch is optional)
+
+
+def _is_f32(dtype):
+    if not _TORCH_F32:
+        import torch
+
+        _TORCH_F32.append(torch.float32)
+    return dtype is _TORCH_F32[0]
+
+
 def _ptr_and_keep(t):
     """Raw pointer of a buffer-like; returns (ptr, keepalive, host_array)."""
     if hasattr(t, "data_ptr"):  # torch.Tensor
-        if t.dtype.__repr__() != "torch.float32":
+        if not _is_f32(t.dtype):
             raise TypeError("loop_tool buffers are float32")
         if not t.is_contiguous():
             raise ValueError("buffers must be contiguous")
