@@ -217,14 +217,20 @@ class CapturedRun:
             self._h = None
 
 
-def _current_stream():
-    try:
-        import torch
+_TORCH = []  # the torch module, or None without torch (looked up once)
 
-        if torch.cuda.is_available() and torch.cuda.is_initialized():
-            return torch.cuda.current_stream().cuda_stream
-    except Exception:
-        pass
+
+def _current_stream():
+    if not _TORCH:
+        try:
+            import torch
+
+            _TORCH.append(torch)
+        except Exception:
+            _TORCH.append(None)
+    torch = _TORCH[0]
+    if torch is not None and torch.cuda.is_initialized():
+        return torch.cuda.current_stream().cuda_stream
     return None
 
 

@@ -21,6 +21,8 @@
 //            4 consecutive k, two rows per thread
 //   kVecR    dense with unit stride along rows (row-major B read by
 //            columns): 16-byte loads of 4 consecutive rows, two k per thread
+//   kGatherT the gather form of an A operand whose per-k entries (k offset,
+//            up to 3 guard partials, 32-bit) fit a shared table (K <= 768)
 #include <stdint.h>
 
 #include "kernels.h"
@@ -29,6 +31,11 @@ namespace {
 
 constexpr int BM = 128, BK = 16, NT = 256, LDS = BM + 4;
 constexpr int kHoistG = 4;  // guards whose row partials are kept in registers
+// Gathered operands with 32-bit k offsets, K <= kKtab and at most 3 guards:
+// the per-k entries {koff[k], gk[0][k], gk[1][k], gk[2][k]} are copied into
+// shared memory once per CTA, so an element costs one broadcast 16-byte
+// shared load instead of 1 + nguard global loads with 64-bit indexing.
+constexpr int kKtab = 768;
 
 struct Tile {
   float s[2][BK][LDS];
@@ -39,6 +46,22 @@ struct Tile {
 // bank for single launches), not copied into registers.
 template <int MODE>
 struct Loader;
+
+__host__ __device__ __forceinline__ bool ktab_ok(const LtbGemmOperand& op, int64_t K) {
+  return op.k32 && K <= kKtab && op.nguard <= 3;
+}
+
+// Fills kt[k] = {koff, gk0, gk1, gk2} for k < K (caller synchronises).
+__device__ __forceinline__ void ktab_fill(const LtbGemmOperand& op, int64_t K, int4* kt) {
+  for (int k = threadIdx.x; k < K; k += NT) {
+    int4 e;
+    e.x = (int)(op.dense ? k * op.ld_k : op.koff[k]);
+    e.y = op.nguard > 0 ? op.gk[k] : 0;
+    e.z = op.nguard > 1 ? op.gk[K + k] : 0;
+    e.w = op.nguard > 2 ? op.gk[2 * K + k] : 0;
+    kt[k] = e;
+  }
+}
 
 template <>
 struct Loader<kSimtGather> {
@@ -72,7 +95,8 @@ struct Loader<kSimtGather> {
         return 0.f;
     return __ldg(op.base + off + (op.dense ? k * op.ld_k : op.koff[k]));
   }
-  __device__ __forceinline__ void fetch(int k0) {
+  static constexpr bool kAsync = false;
+  __device__ __forceinline__ void fetch(int k0, float (*)[LDS]) {
     const int kk0 = threadIdx.x >> 7;
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = one(k0 + kk0 + 2 * q);
@@ -83,6 +107,60 @@ struct Loader<kSimtGather> {
     for (int q = 0; q < 8; ++q) s[kk0 + 2 * q][c] = v[q];
   }
 };
+
+// The gather form reading its per-k entries from the shared table kt
+// (ktab_ok operands): one broadcast 16-byte load per element.
+template <>
+struct Loader<kSimtGatherT> {
+  const LtbGemmOperand& op;
+  const int K;
+  const int4* kt;
+  int64_t off;  // element offset of this thread's row
+  int32_t g[3];
+  bool ok;
+  static constexpr bool kAsync = true;  // elements go global -> shared by cp.async
+
+  __device__ __forceinline__ Loader(const LtbGemmOperand& o, int64_t row0, int64_t rows,
+                                    int64_t K_)
+      : op(o), K((int)K_), kt(nullptr) {
+    const int64_t r = row0 + (threadIdx.x & (BM - 1));
+    ok = r < rows;
+    off = 0;
+    if (ok) off = op.dense ? r * op.ld_row : op.rowoff[r];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) g[q] = q < op.nguard && ok ? op.grow[(int64_t)q * rows + r] : 0;
+  }
+  // element k of this thread's row into s[kk][row]: a 4-byte cp.async, or
+  // zeros (source size 0) outside the operand or its guards
+  __device__ __forceinline__ void one(int k, float* dst) const {
+    bool in = ok && k < K;
+    const float* src = op.base;
+    if (in) {
+      const int4 e = kt[k];
+      const int ng = op.nguard;
+      in = !((ng > 0 && (uint32_t)(g[0] + e.y) >= (uint32_t)op.gub[0]) ||
+             (ng > 1 && (uint32_t)(g[1] + e.z) >= (uint32_t)op.gub[1]) ||
+             (ng > 2 && (uint32_t)(g[2] + e.w) >= (uint32_t)op.gub[2]));
+      if (in) src = op.base + off + e.x;
+    }
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(in ? 4 : 0)
+                 : "memory");
+  }
+  __device__ __forceinline__ void fetch(int k0, float (*s)[LDS]) {
+    const int c = threadIdx.x & (BM - 1), kk0 = threadIdx.x >> 7;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) one(k0 + kk0 + 2 * q, &s[kk0 + 2 * q][c]);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  __device__ __forceinline__ void stash(float (*)[LDS]) const {}
+};
+
+// Waits for this thread's cp.async copies (kAsync loaders).
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
 
 template <>
 struct Loader<kSimtVecK> {
@@ -99,7 +177,8 @@ struct Loader<kSimtVecK> {
       p[i] = r < rows ? op.base + r * op.ld_row + (threadIdx.x & 3) * 4 : nullptr;
     }
   }
-  __device__ __forceinline__ void fetch(int k0) {
+  static constexpr bool kAsync = false;
+  __device__ __forceinline__ void fetch(int k0, float (*)[LDS]) {
     const bool kin = k0 + (threadIdx.x & 3) * 4 < K;  // K % 4 == 0: all 4 or none
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -131,7 +210,8 @@ struct Loader<kSimtVecR> {
     const int64_t r = row0 + (threadIdx.x & 31) * 4;  // rows % 4 == 0: all 4 or none
     p = r < rows ? op.base + r : nullptr;
   }
-  __device__ __forceinline__ void fetch(int k0) {
+  static constexpr bool kAsync = false;
+  __device__ __forceinline__ void fetch(int k0, float (*)[LDS]) {
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       const int k = k0 + (threadIdx.x >> 5) + 8 * i;
@@ -149,12 +229,18 @@ struct Loader<kSimtVecR> {
 template <int AM, int BMODE>
 __device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, int64_t j0) {
   __shared__ __align__(16) Tile ta, tb;
+  __shared__ int4 kta[AM == kSimtGatherT ? kKtab : 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // warps 4 (rows) x 2 (columns), lanes 4 x 8: a warp's A reads touch 4
   // distinct 16-byte words and its B reads 8
   const int ty = (warp >> 1) * 4 + (lane >> 3), tx = (warp & 1) * 8 + (lane & 7);
   Loader<AM> la(p.a, i0, p.M, p.K);
   Loader<BMODE> lb(p.b, j0, p.N, p.K);
+  if constexpr (AM == kSimtGatherT) {
+    ktab_fill(p.a, p.K, kta);
+    __syncthreads();
+    la.kt = kta;
+  }
   float acc[8][8];
 #pragma unroll
   for (int a = 0; a < 8; ++a)
@@ -162,16 +248,18 @@ __device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, i
     for (int b = 0; b < 8; ++b) acc[a][b] = 0.f;
 
   const int nk = (int)((p.K + BK - 1) / BK);  // K <= kSimtMaxK (checked at launch)
-  la.fetch(0);
-  lb.fetch(0);
+  constexpr bool async = Loader<AM>::kAsync || Loader<BMODE>::kAsync;
+  la.fetch(0, ta.s[0]);
+  lb.fetch(0, tb.s[0]);
   la.stash(ta.s[0]);
   lb.stash(tb.s[0]);
+  if constexpr (async) cp_async_wait_all();
   __syncthreads();
   for (int t = 0; t < nk; ++t) {
     const int cur = t & 1;
-    if (t + 1 < nk) {
-      la.fetch((t + 1) * BK);
-      lb.fetch((t + 1) * BK);
+    if (t + 1 < nk) {  // buffer cur ^ 1 was last read before the previous barrier
+      la.fetch((t + 1) * BK, ta.s[cur ^ 1]);
+      lb.fetch((t + 1) * BK, tb.s[cur ^ 1]);
     }
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
@@ -190,6 +278,7 @@ __device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, i
       la.stash(ta.s[cur ^ 1]);
       lb.stash(tb.s[cur ^ 1]);
     }
+    if constexpr (async) cp_async_wait_all();
     __syncthreads();
   }
 
@@ -392,6 +481,8 @@ cudaError_t dispatch(int modes, const LtbGemmProblem* p, const LtbGemmProblem* d
                      const int64_t* d_tile_start, int nprob, int64_t tiles, cudaStream_t st) {
   const int am = modes & 15, bm = (modes >> 4) & 15;
   switch (am) {
+    case kSimtGatherT:
+      return dispatch_b<kSimtGatherT>(bm, p, d_probs, d_tile_start, nprob, tiles, st);
     case kSimtVecK:
       return dispatch_b<kSimtVecK>(bm, p, d_probs, d_tile_start, nprob, tiles, st);
     case kSimtVecR:
@@ -403,12 +494,13 @@ cudaError_t dispatch(int modes, const LtbGemmProblem* p, const LtbGemmProblem* d
 
 }  // namespace
 
-int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K) {
+int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K, bool a_side) {
+  const int gather = a_side && ktab_ok(op, K) ? kSimtGatherT : kSimtGather;
   if (!op.dense || op.nguard != 0 || (reinterpret_cast<uintptr_t>(op.base) & 15) != 0)
-    return kSimtGather;
+    return gather;
   if (op.ld_k == 1 && op.ld_row % 4 == 0 && K % 4 == 0) return kSimtVecK;
   if (op.ld_row == 1 && op.ld_k % 4 == 0 && rows % 4 == 0) return kSimtVecR;
-  return kSimtGather;
+  return gather;
 }
 
 int ltb_simt_tile(const LtbGemmProblem& p, int sms, int tile) {
@@ -428,7 +520,8 @@ cudaError_t ltb_launch_gemm_simt(const LtbGemmProblem& p, int sms, cudaStream_t 
     k_gemm_simt_mid<<<grid, NT, 0, st>>>(p);
     return cudaGetLastError();
   }
-  const int modes = ltb_simt_mode(p.a, p.M, p.K) | ltb_simt_mode(p.b, p.N, p.K) << 4;
+  const int modes =
+      ltb_simt_mode(p.a, p.M, p.K, true) | ltb_simt_mode(p.b, p.N, p.K, false) << 4;
   return dispatch(modes, &p, nullptr, nullptr, 0, 0, st);
 }
 

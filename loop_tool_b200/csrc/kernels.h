@@ -61,6 +61,7 @@ struct LtbGemmOperand {
   const int32_t* grow;    // [nguard][rows] guard partial from the row coords
   const int32_t* gk;      // [nguard][K]   guard partial from the k coords
   const int32_t* gub;     // [nguard]      valid iff 0 <= grow + gk < gub
+  int k32;                // every k offset (koff[k], or k * ld_k) fits in int32
 };
 
 struct LtbGemmProblem {
@@ -74,9 +75,10 @@ struct LtbGemmProblem {
 // FP32 CUDA-core path (exact fp32 FMA): the "plain FP32" baseline family.
 // Operand tile loader forms (gemm_simt.cu); ltb_simt_mode picks the fastest
 // one the operand's layout allows.
-enum { kSimtGather = 0, kSimtVecK = 1, kSimtVecR = 2 };
+enum { kSimtGather = 0, kSimtVecK = 1, kSimtVecR = 2, kSimtGatherT = 3 };
 constexpr int64_t kSimtMaxK = (int64_t(1) << 31) - 64;  // k indices are 32-bit
-int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K);
+// a_side: the A operand (the gather form may use a shared per-k table).
+int ltb_simt_mode(const LtbGemmOperand& op, int64_t rows, int64_t K, bool a_side);
 // tile: 128 (128 x 128 CTA tiles, the loader forms above), 64 (64 x 64
 // tiles for problems that 128-wide tiles leave SMs idle in), 0 = 64 when
 // there are at most SMs / 4 tiles of 128 x 128, else 128.  Same bits either

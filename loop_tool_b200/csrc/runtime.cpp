@@ -86,6 +86,7 @@ struct GemmTables {
   LtbTcProblem prob{};                // launch template (maps/c bound per run)
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
   bool a_off32 = false, b_off32 = false;  // operand offsets fit in int32
+  bool a_k32 = false, b_k32 = false;      // k offsets alone fit in int32
   // implicit-GEMM convolution: A packed as NHWC BF16 image(s) read by 4-D
   // TMA boxes (LtbTcProblem::img); B's K order permuted to (kh, kw, c)
   bool img = false;
@@ -336,6 +337,8 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     const int64_t lim = int64_t(1) << 31;
     t.a_off32 = maxabs(ra) + maxabs(ktab_a) < lim;
     t.b_off32 = maxabs(rb) + maxabs(ktab_b) < lim;
+    t.a_k32 = maxabs(ktab_a) < lim;
+    t.b_k32 = maxabs(ktab_b) < lim;
   }
   auto ctab = table(nd, d.out_coef, 0);
   t.unit_cols = true;
@@ -553,14 +556,16 @@ bool is_device_accessible(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-bool is_managed(const void* p) {
+// 0: host (pageable or pinned), 1: device, 2: managed.
+int mem_kind(const void* p) {
   cudaPointerAttributes a{};
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return 0;
   }
-  return a.type == cudaMemoryTypeManaged;
+  return a.type == cudaMemoryTypeManaged ? 2 : a.type == cudaMemoryTypeDevice ? 1 : 0;
 }
+
 
 // Launches of stage i (nothing for a row-chain member that is not the
 // chain's first stage: the chain launches as one kernel).
@@ -601,6 +606,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
                t.a_ng, t.ag_row, t.ag_k, t.ag_ub};
         p.b = {bt.p[B.buf] + t.b_boff[b], t.b_row, t.b_k, t.b_dense ? 1 : 0, t.b_ldr, t.b_ldk,
                t.b_ng, t.bg_row, t.bg_k, t.bg_ub};
+        p.a.k32 = t.a_k32 ? 1 : 0;
+        p.b.k32 = t.b_k32 ? 1 : 0;
         p.c = bt.p[s.dev.out_buf] + t.c_boff[b];
         p.crow = t.c_row;
         p.ccol = t.c_col;
@@ -712,10 +719,13 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
     // every buffer in host memory and a plain linear map: stage the copies
     // chunk by chunk on two streams, so each chunk's download overlaps the
     // next chunk's upload (the host link runs both directions at once)
+    // one pointer-attribute query per buffer per run
+    int kind[LTB_MAXBUF];
     bool all_host = true;
     for (int i = 0; i < n; ++i) {
       if (!memory[i]) return fail(LTB_ERR_INVALID, "null buffer " + std::to_string(i));
-      all_host = all_host && !is_device_accessible(memory[i]);
+      kind[i] = mem_kind(memory[i]);
+      all_host = all_host && kind[i] == 0;
     }
     constexpr int64_t kChunk = int64_t(1) << 24;  // elements per chunk (64 MB of FP32)
     const int64_t total = P.n_out ? P.io_elems[P.n_in] : 0;
@@ -764,14 +774,14 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
     // in bulk before the launch instead of page by page on first touch
     std::vector<int> managed;
     for (int i = 0; i < n; ++i)
-      if (is_managed(memory[i])) {
+      if (kind[i] == 2) {
         managed.push_back(i);
         const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[i], 1) * 4;
         if (cudaMemPrefetchAsync(memory[i], bytes, c->device, st) != cudaSuccess)
           cudaGetLastError();  // advisory only
       }
     for (int i = 0; i < n; ++i) {
-      if (is_device_accessible(memory[i])) {
+      if (kind[i] != 0) {
         bt.p[i] = static_cast<float*>(memory[i]);
         continue;
       }
@@ -1102,6 +1112,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
              t.ag_k, t.ag_ub};
       p.b = {ptr(B.buf), t.b_row, t.b_k, t.b_dense ? 1 : 0, t.b_ldr, t.b_ldk, t.b_ng, t.bg_row,
              t.bg_k, t.bg_ub};
+      p.a.k32 = t.a_k32 ? 1 : 0;
+      p.b.k32 = t.b_k32 ? 1 : 0;
       p.c = ptr(s.dev.out_buf);
       p.crow = t.c_row;
       p.ccol = t.c_col;
@@ -1190,7 +1202,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
       // form, else the gather form, which serves every operand
       int am = -1, bm = -1;
       for (const auto& q : sp) {
-        const int a = ltb_simt_mode(q.a, q.M, q.K), bb = ltb_simt_mode(q.b, q.N, q.K);
+        const int a = ltb_simt_mode(q.a, q.M, q.K, true), bb = ltb_simt_mode(q.b, q.N, q.K, false);
         am = am < 0 || am == a ? a : kSimtGather;
         bm = bm < 0 || bm == bb ? bb : kSimtGather;
       }

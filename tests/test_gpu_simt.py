@@ -108,10 +108,13 @@ def test_fp32_tile_sizes_same_bits(case, cuda_dev):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape", [(2, 4, 8, 8, 6, 3, 1), (1, 3, 7, 9, 5, 3, 0),
-                                   (2, 64, 16, 16, 40, 3, 1)])
+                                   (2, 64, 16, 16, 40, 3, 1), (4, 16, 33, 35, 24, 5, 2),
+                                   (1, 160, 12, 12, 8, 3, 1)])
 def test_fp32_conv_gather(shape, cuda_dev):
     """Padded convolution: the image operand is gathered with its guards
-    (zero outside the image), the weights through 16-byte loads along k."""
+    (zero outside the image), the weights through 16-byte loads along k; on
+    64-wide tiles element by element, on 128-wide tiles through the shared
+    per-k table.  Both give the same bits."""
     import torch
 
     import loop_tool_b200 as ltb
@@ -124,14 +127,19 @@ def test_fp32_conv_gather(shape, cuda_dev):
     x = torch.randn(N * C * H * W, device=cuda_dev, generator=g)
     w = torch.randn(CO * C * K * K, device=cuda_dev, generator=g)
     Ho, Wo = H + 2 * pad - K + 1, W + 2 * pad - K + 1
-    y = torch.full((N * Ho * Wo * CO,), float("nan"), device=cuda_dev)
-    c([x, w, y])
-    torch.cuda.synchronize()
     ref = torch.nn.functional.conv2d(x.view(N, C, H, W).double(),
                                      w.view(CO, C, K, K).double(), padding=pad)
-    got = y.view(N, Ho, Wo, CO).permute(0, 3, 1, 2).double()
-    err = float((got - ref).norm() / ref.norm())
-    assert err <= 1e-6, f"normwise error {err:.3g}"
+    outs = []
+    for tile in (64, 128):
+        c.set_schedule(0, variant=tile)
+        y = torch.full((N * Ho * Wo * CO,), float("nan"), device=cuda_dev)
+        c([x, w, y])
+        torch.cuda.synchronize()
+        got = y.view(N, Ho, Wo, CO).permute(0, 3, 1, 2).double()
+        err = float((got - ref).norm() / ref.norm())
+        assert err <= 1e-6, f"tile {tile}: normwise error {err:.3g}"
+        outs.append(y)
+    assert torch.equal(outs[0], outs[1])
 
 
 @pytest.mark.gpu
