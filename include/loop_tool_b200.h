@@ -194,7 +194,10 @@ int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps
  * epilogue, 129 / 257 shared-memory transposed epilogue, 130 two 128-wide
  * CTAs per SM, 131 halo image tiles with resident weights (single-segment
  * convolutions whose weights fit in shared memory; elsewhere it reads back
- * as 128); cta_per_sm is the raster group. */
+ * as 128); cta_per_sm is the raster group.  For a CUDA-core (FP32)
+ * contraction, variant = 64 or 128 is the CTA tile (0: 64 when the problem
+ * has at most SMs / 4 tiles of 128 x 128); both give the same bits.  For a
+ * pooling reduction, variant 4 runs 4 work items per thread (else 2). */
 int ltb_get_schedule(ltb_compiled* c, int stage, int* cta_per_sm, int* threads,
                      int* variant);
 int ltb_set_schedule(ltb_compiled* c, int stage, int cta_per_sm, int threads,
