@@ -964,12 +964,9 @@ bool ltb_tc_halo_geometry(LtbTcProblem& p, int wp) {
 cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st) {
   if (j.c % 64 || j.wp < 1 || j.wp > 1024) return cudaErrorInvalidValue;
   const size_t smem = (size_t)64 * (j.wp + 1) * sizeof(float);
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_pack_image,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = ltb_smem_optin((const void*)k_pack_image, smem);
     if (e != cudaSuccess) return e;
-    attr = smem;
   }
   dim3 grid((unsigned)(j.c / 64), (unsigned)j.hp, (unsigned)j.nimg);
   k_pack_image<<<grid, 256, smem, st>>>(j);
@@ -990,12 +987,9 @@ cudaError_t ltb_launch_pack_conv(const LtbImageJob& j, const LtbGemmOperand& bop
   if (img_ctas + nb > 0x7fffffff) return cudaErrorInvalidValue;
   size_t smem = (size_t)64 * (j.wp + 1) * sizeof(float);
   if (smem < (size_t)PKT * (PR + 1) * sizeof(float)) smem = (size_t)PKT * (PR + 1) * sizeof(float);
-  static size_t attr = 0;
-  if (smem > 40 * 1024 && smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_pack_conv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+  if (smem > 40 * 1024) {  // 48 KB less the static pack tables
+    const cudaError_t e = ltb_smem_optin((const void*)k_pack_conv, smem);
     if (e != cudaSuccess) return e;
-    attr = smem;
   }
   k_pack_conv<<<(unsigned)(img_ctas + nb), 256, smem, st>>>(j, JB, b_tiles, nb);
   return cudaGetLastError();
@@ -1068,19 +1062,16 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b,
                              const void* map_a2) {
-  static bool attr = false;
   size_t smem = Tile<BN, CTAS>::SMEM;
   if (HALO) {
     if (d_probs || !single || !single->img_halo) return cudaErrorInvalidValue;
     smem = halo_smem(*single);
     if (smem > kHaloSmemMax) return cudaErrorInvalidValue;
   }
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<BN, TE, CTAS, HALO>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(HALO ? kHaloSmemMax : smem));
+  {
+    const cudaError_t e = ltb_smem_optin((const void*)k_gemm_tc<BN, TE, CTAS, HALO>,
+                                         HALO ? kHaloSmemMax : smem);
     if (e != cudaSuccess) return e;
-    attr = true;
   }
   const int64_t slots = (int64_t)sms * CTAS;
   const int grid = (int)(total_tiles < slots ? total_tiles : slots);

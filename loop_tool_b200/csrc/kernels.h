@@ -5,6 +5,11 @@
 
 #include "stage.h"
 
+// Opts kernel fn into `bytes` of dynamic shared memory on the current
+// device (the attribute is per device), once per kernel, device and larger
+// size; thread-safe.
+cudaError_t ltb_smem_optin(const void* fn, size_t bytes);
+
 // Records `msg` as the calling thread's ltb_last_error() and returns code.
 int ltb_set_last_error(int code, const char* msg);
 

@@ -1112,6 +1112,20 @@ static int pick_threads(const LtbCfg& cfg, int dflt, int maxt) {
 
 static const int kWaves[] = {0, 1, 2, 4, 8, 16, 32};
 
+cudaError_t ltb_smem_optin(const void* fn, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;  // (kernel, device) -> bytes
+  std::lock_guard<std::mutex> g(mu);
+  size_t& have = done[{fn, dev}];
+  if (have >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
+}
+
 // Pooling-shaped reductions (k_window): one operand, unit-stride innermost
 // window, at most 64 outer window positions; *s = output stride, *k =
 // innermost window extent.
@@ -1383,13 +1397,10 @@ int ltb_row_chain_candidates(const LtbStage* const* h_stages, int nsteps, LtbCfg
 template <int EPT, int NT>
 static cudaError_t launch_softmax_bulk(const SoftmaxRows& P, int sms, const LtbCfg& cfg,
                                        int* err, cudaStream_t st) {
-  static size_t attr = 0;  // largest dynamic shared memory opted into so far
   const size_t smem = (size_t)kSmxRing * P.n * 4;
-  if (smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_softmax_bulk<EPT, NT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  {
+    const cudaError_t e = ltb_smem_optin((const void*)k_softmax_bulk<EPT, NT>, smem);
     if (e != cudaSuccess) return e;
-    attr = smem;
   }
   const int g = grid_of(k_softmax_bulk<EPT, NT>, P.rows * NT, NT, sms, cfg, smem);
   k_softmax_bulk<EPT, NT><<<g, NT, smem, st>>>(P, err);
