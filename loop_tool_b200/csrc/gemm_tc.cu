@@ -8,8 +8,9 @@
 // separable FP32 operand description, so the same kernel runs matmul,
 // batched matmul and gathered operands.  A convolution's input can instead
 // be an image operand: packed once as a zero-padded NHWC BF16 image
-// (k_pack_image) and loaded as 4-D TMA boxes per output image row (implicit
-// GEMM, no im2col matrix).  The split-BF16 modes pack A' = [Ah | Al | Ah
+// (k_pack_image, or k_pack_conv with the weights in the same launch) and
+// loaded as 4-D TMA boxes per output image row (implicit GEMM, no im2col
+// matrix).  The split-BF16 modes pack A' = [Ah | Al | Ah
 // (| Al)], B' = [Bh | Bh | Bl (| Bl)] along K, so one BF16 GEMM accumulates
 // Ah*Bh + Al*Bh + Ah*Bl (+ Al*Bl).
 //
@@ -25,8 +26,11 @@
 //
 // Tile forms (a tuned schedule): 128 x 256 or 128 x 128 output tiles, one CTA
 // per SM (4- or 6-stage ring), or two 128 x 128 CTAs per SM (3-stage rings);
-// epilogue by per-thread row stores or through a 32 x 32 shared-memory
-// transpose into whole-row stores.
+// epilogue by per-thread row stores (32-byte sector stores where aligned) or
+// through a 32 x 32 shared-memory transpose into whole-row stores.  Halo
+// image tiles (single-segment convolutions, N <= 128): the weights stay
+// resident in shared memory and one 4-D box of whole padded image rows per
+// (kh, channel block) serves every kw shift, read in place.
 //
 // Roles (320 threads per CTA):
 //   warp 0 lane 0 : TMA producer                  warp 0 : TMEM alloc/free
