@@ -75,7 +75,11 @@ int ltb_compile(const char* ir_text, const char* options, ltb_compiled** out);
  * copies chunk by chunk on two streams (uploads overlap downloads).
  * Managed buffers are prefetched to the device before the launch and, for
  * sync != 0, the outputs back to the host after it (bulk migration instead
- * of demand paging; the reference frontend reads results on the host). */
+ * of demand paging; the reference frontend reads results on the host).
+ * Runs of one compiled object on its own (default) scratch are ordered on
+ * the device: a run waits for the previous such run, whatever its stream,
+ * before its kernels touch the scratch.  With sync != 0 a bounded wait that
+ * gave up in a kernel on this stream is reported as LTB_ERR_TIMEOUT. */
 int ltb_run(ltb_compiled* c, void* const* memory, int n, int sync,
             void* stream);
 
@@ -84,6 +88,19 @@ int ltb_run(ltb_compiled* c, void* const* memory, int n, int sync,
  * of one compiled object on different streams do not share scratch. */
 int ltb_run_with_scratch(ltb_compiled* c, void* const* memory, int n,
                          int sync, void* stream, void* scratch);
+
+/* How ltb_run would treat each buffer, one line per buffer, decided on the
+ * host without launching anything: device memory of the compiled object's
+ * device and managed memory are read and written in place when 16-byte
+ * aligned (the kernels move 16-byte vectors and the tensor-core packers
+ * feed the TMA engine); host memory and device/managed memory off a 16-byte
+ * boundary (e.g. a view starting one element into a tensor) are staged
+ * through an aligned device copy; another GPU's memory is rejected
+ * (LTB_ERR_INVALID) rather than read as a peer.  Captured runs, batches and
+ * the autotuner take in-place buffers only.  No reference counterpart: the
+ * reference's Compiled::run (backend.h:20-21) passes pointers as given. */
+int ltb_run_plan(ltb_compiled* c, void* const* memory, int n, char* buf,
+                 size_t len);
 
 /* Compiled destructor. */
 int ltb_release(ltb_compiled* c);
@@ -213,8 +230,25 @@ int ltb_tune_clear(void);
 int64_t ltb_tune_entries(void);
 
 /* Stream synchronisation helper (cuCtxSynchronize in the reference,
- * src/backends/cuda/cuda.cpp:847-849, when stream is NULL). */
+ * src/backends/cuda/cuda.cpp:847-849, when stream is NULL).  Also reports
+ * (LTB_ERR_TIMEOUT, once) a bounded wait that gave up in a kernel launched
+ * on this stream of the current device since the stream's last
+ * synchronising call: every device wait in these kernels is bounded, and
+ * its timeout flag is kept per stream. */
 int ltb_synchronize(void* stream);
+
+/* Self-check of the bounded device waits, on the current device and
+ * `stream`: one CTA allocates TMEM, starts a bulk copy, then waits on an
+ * mbarrier that nothing ever arrives at for at most limit_cycles clock
+ * cycles (1 .. 4e9; the kernels' own waits allow about 2 s).  The wait
+ * gives up, raises the stream's timeout flag, lets its copy land, frees
+ * the TMEM and returns; the call then reports LTB_ERR_TIMEOUT with
+ * *completed = 0 and *drained = 1.  Exercises, on the GPU, the give-up path
+ * every wait in the tensor-core and bulk-copy kernels takes, without a
+ * fault or a hang.  No reference counterpart (the reference's kernels never
+ * wait on the device). */
+int ltb_check_bounded_wait(int64_t limit_cycles, void* stream, int* completed,
+                           int* drained);
 
 #ifdef __cplusplus
 }

@@ -29,6 +29,8 @@ SIGNATURES = {
     "ltb_run_with_scratch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                             ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                             ctypes.c_void_p]),
+    "ltb_run_plan": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                    ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
     "ltb_release": (ctypes.c_int, [ctypes.c_void_p]),
     "ltb_dump": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "ltb_int_property": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p,
@@ -39,6 +41,9 @@ SIGNATURES = {
     "ltb_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "ltb_free": (ctypes.c_int, [ctypes.c_void_p]),
     "ltb_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "ltb_check_bounded_wait": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int)]),
     "ltb_row_sum_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                                            ctypes.c_void_p, ctypes.c_void_p]),
     "ltb_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p),

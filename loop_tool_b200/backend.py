@@ -122,6 +122,19 @@ class Compiled:
     def __call__(self, tensors, sync=True):
         self.run(tensors, sync)
 
+    def run_plan(self, memory):
+        """How run() would treat each buffer (in place, staged, rejected),
+        decided on the host without launching anything."""
+        ptrs, keep = [], []
+        for t in memory:
+            p, k, _ = _ptr_and_keep(t)
+            ptrs.append(p)
+            keep.append(k)
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        buf = ctypes.create_string_buffer(1 << 16)
+        _lib.check(_lib.lib().ltb_run_plan(self._h, arr, len(ptrs), buf, len(buf)))
+        return buf.value.decode().splitlines()
+
     def int_property(self, name):
         v = ctypes.c_int64()
         _lib.check(_lib.lib().ltb_int_property(self._h, name.encode(), ctypes.byref(v)))

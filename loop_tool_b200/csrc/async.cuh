@@ -35,18 +35,26 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase of parity `parity` to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err) {
+// Wait at most `limit` cycles for the phase of parity `parity` to complete
+// (giving up early once another CTA has raised *err); on giving up, raise
+// *err and return false.
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, int* err,
+                                              long long limit) {
   if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try(bar, parity)) {
     const long long dt = clock64() - t0;
-    if (dt > kWaitCycles || (dt > kFlagCycles && *(volatile int*)err)) {
+    if (dt > limit || (dt > kFlagCycles && *(volatile int*)err)) {
       atomicExch(err, 1);
       return false;
     }
   }
   return true;
+}
+
+// Bounded wait for the phase of parity `parity` to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err) {
+  return mbar_wait_for(bar, parity, err, kWaitCycles);
 }
 
 // Bounded wait that ignores the error flag: used while winding down, to let

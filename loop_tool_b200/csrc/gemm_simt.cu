@@ -3,8 +3,11 @@
 //   A(i, k) = a.base[a.rowoff[i] + a.koff[k]]   (0 if a guard fails)
 // so the same kernel serves row-major matmul, transposed operands and padded
 // convolution as an implicit GEMM (the im2col gather happens in the tile
-// loader, never in HBM).  Every output is one FP32 FMA chain over k = 0..K-1
-// in order, whatever the tile loader's form.
+// loader, never in HBM).  Every output is one chain over k = 0..K-1 in
+// order of separately rounded FP32 multiplies and adds, whatever the tile
+// loader's form: the arithmetic of the reference's C path (cpp.cpp:467-471
+// compiles with cc -std=c99, which does not contract a*b+c into an FMA), so
+// plain FP32 contractions match the reference bit for bit.
 //
 // CTA tile 128 x 128, 16 k per step, 256 threads with 8 x 8 outputs each
 // (rows ty*4 + {0..3} and 64 + ty*4 + {0..3}, likewise columns); both
@@ -272,7 +275,7 @@ __device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, i
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 8; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+        for (int b = 0; b < 8; ++b) acc[a][b] = __fadd_rn(acc[a][b], __fmul_rn(av[a], bv[b]));
     }
     if (t + 1 < nk) {
       la.stash(ta.s[cur ^ 1]);
@@ -353,8 +356,8 @@ __global__ void __launch_bounds__(NT, 2)
 // threads with 4 x 4 outputs each (rows ty*4 + {0..3}, columns tx*4 +
 // {0..3}), 16 k per step, elements fetched one by one (dense offsets
 // computed, others from the tables, guards applied).  Each output is the
-// same FMA chain over k in order as in the 128 x 128 kernel, so both give
-// the same bits.
+// same chain of rounded multiplies and adds over k in order as in the
+// 128 x 128 kernel, so both give the same bits.
 constexpr int MBM = 64, MLD = MBM + 4;
 
 __device__ __forceinline__ float fetch_one(const LtbGemmOperand& op, int64_t r, int64_t k,
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(NT) k_gemm_simt_mid(LtbGemmProblem p) {
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+        for (int b = 0; b < 4; ++b) acc[a][b] = __fadd_rn(acc[a][b], __fmul_rn(av[a], bv[b]));
     }
     if (t + 1 < nk) {
       la.stash(sa[cur ^ 1], akf);

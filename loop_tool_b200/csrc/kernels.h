@@ -21,6 +21,9 @@ struct LtbCfg {
   int cta_per_sm;
   int threads;
   int variant;
+  // CTAs of the launch, fixed (a "parallel" loop annotation pins the
+  // stage's thread count); 0: from cta_per_sm and the work
+  int grid;
 };
 
 
@@ -98,3 +101,8 @@ int ltb_simt_tile(const LtbGemmProblem& p, int sms, int tile);
 cudaError_t ltb_launch_gemm_simt_grouped(const LtbGemmProblem* d_probs,
                                          const int64_t* d_tile_start, int nprob,
                                          int64_t total_tiles, int modes, cudaStream_t st);
+
+// Bounded-wait self-check (waitcheck.cu): one CTA whose mbarrier wait on a
+// barrier nothing arrives at gives up after `limit` cycles, raising *err;
+// status_host[2] = {wait completed, in-flight copy drained}.
+cudaError_t ltb_launch_wait_check(int* err, long long limit, int* status_host, cudaStream_t st);

@@ -137,6 +137,13 @@ struct Builder {
   Builder(const IRGraph& g_, const LowerOptions& o) : g(g_), opt(o) {}
 
   int64_t vsize(int v) const { return g.var_sizes.at(v); }
+  // position of var v's first loop in node N's order (after every loop
+  // when N has no loop over v)
+  static int order_pos(const Node& N, int v) {
+    for (size_t i = 0; i < N.order.size(); ++i)
+      if (N.order[i].first == v) return (int)i;
+    return 1 << 20;
+  }
 
   BufferInfo make_buf(int slot, const std::vector<int>& layout, bool scratch) {
     BufferInfo b;
@@ -491,6 +498,63 @@ struct Builder {
     if (d.red_op == LTB_R_ADD && R > opt.kahan_threshold) d.kahan = 1;
   }
 
+  // Loop annotations of the stage's node N: backend sub-tree annotations
+  // ("[cuda]": this backend; any other backend is rejected, there is no
+  // host path to hand a sub-tree to) and the launch pins (StagePins).
+  void read_pins(StageCtx& s, const Node& N) {
+    StagePins& p = s.ps.pins;
+    auto& d = s.ps.dev;
+    std::ostringstream notes;
+    std::vector<int64_t> par_out;  // iteration counts, outermost first
+    for (size_t i = 0; i < N.order.size() && i < N.loop_annotations.size(); ++i) {
+      const int v = N.order[i].first;
+      const int64_t iters = N.order[i].second.size + (N.order[i].second.tail > 0 ? 1 : 0);
+      const int k = dim_of(s, v);
+      std::istringstream words(N.loop_annotations[i]);
+      for (std::string w; words >> w;) {
+        if (w.size() > 2 && w.front() == '[' && w.back() == ']') {
+          const std::string be = w.substr(1, w.size() - 2);
+          LTB_CHECK(be == "cuda", "loop " << g.var_names[v] << " is annotated for backend '" << be
+                                          << "': this backend runs every loop on the device "
+                                             "and has no other backend to hand a sub-tree to");
+          notes << " [cuda] sub-tree at loop " << g.var_names[v]
+                << ": device launches with the rest of the tree, the loops around it in the "
+                   "grid (no host loop);";
+        } else if (w == "parallel") {
+          if (k >= 0 && k < d.nout) par_out.push_back(iters);
+          else if (k >= d.nout) p.parallel_red = (p.parallel_red ? p.parallel_red : 1) * iters;
+        } else if (w == "unroll") {
+          p.unroll = (int)std::min<int64_t>(iters, 1 << 20);
+        } else if (w == "vectorize") {
+          notes << " vectorize at " << g.var_names[v]
+                << ": 16-byte vectors are used wherever alignment allows (no change);";
+        } else {
+          notes << " annotation '" << w << "' at " << g.var_names[v] << " ignored;";
+        }
+      }
+    }
+    if (!par_out.empty()) {
+      p.parallel_out = 1;
+      for (auto x : par_out) p.parallel_out *= x;
+      if (par_out.size() >= 2) p.cta_threads = (int)std::min<int64_t>(par_out.back(), 1 << 20);
+    }
+    // a parallel loop over a reduced var asks for a parallel reduction: a
+    // tree per output up to 256 threads, split-K partials beyond that
+    const bool tree_ok = d.red_op == LTB_R_ADD || d.red_op == LTB_R_MUL ||
+                         d.red_op == LTB_R_MAX || d.red_op == LTB_R_MIN;
+    if (p.parallel_red > 1 && tree_ok && s.ps.family == Family::reduce_serial)
+      s.ps.family = Family::reduce_parallel;
+    if (p.parallel_red > 256 && s.ps.family == Family::reduce_parallel &&
+        (d.red_op == LTB_R_ADD || d.red_op == LTB_R_MUL))
+      s.ps.family = Family::reduce_split;
+    if (s.ps.family == Family::contraction && p.any()) {
+      notes << " parallel/unroll on a contraction: the tile kernel keeps its own mapping;";
+      p.parallel_out = p.parallel_red = 0;
+      p.cta_threads = p.unroll = 0;
+    }
+    p.text = notes.str();
+  }
+
   std::string stage_text(const StageCtx& s) {
     std::ostringstream ss;
     const auto& d = s.ps.dev;
@@ -508,6 +572,16 @@ struct Builder {
       ss << " gemm B=" << c.B << " M=" << c.M << " N=" << c.N << " K=" << c.K
          << (c.a_guarded ? " A-guarded" : "");
     }
+    const StagePins& p = s.ps.pins;
+    if (p.any()) {
+      ss << " pinned{";
+      if (p.parallel_out) ss << " parallel=" << p.parallel_out;
+      if (p.cta_threads) ss << " cta=" << p.cta_threads;
+      if (p.parallel_red) ss << " parallel_reduce=" << p.parallel_red;
+      if (p.unroll) ss << " unroll=" << p.unroll;
+      ss << " }";
+    }
+    if (!p.text.empty()) ss << " annotations:" << p.text;
     return ss.str();
   }
 
@@ -584,7 +658,14 @@ struct Builder {
         s.ps.family = Family::elementwise;
       } else {
         const BufferInfo& out = fused_elem ? bufs.at(fused_write[n]) : bufs.at(n);
+        // reduced vars in loop order (first appearance in the node's
+        // order): the reference folds them in its loop nest's order
+        // (compile.cpp:217-271 resets at the loops' LCA, then visits the
+        // reduced points lexicographically in that order)
         auto red = g.reduction_vars(n);
+        std::stable_sort(red.begin(), red.end(), [&](int a, int b) {
+          return order_pos(N, a) < order_pos(N, b);
+        });
         set_dims(s, out.layout, red);
         set_output(s, out);
         if (!red.empty()) {
@@ -603,6 +684,7 @@ struct Builder {
           s.ps.family = Family::elementwise;
         }
       }
+      read_pins(s, N);
       finalize(s.ps.dev);
       s.ps.text = stage_text(s);
       plan.stages.push_back(s.ps);
@@ -710,7 +792,13 @@ struct Builder {
       bool ends_elem = st[grp.back()].family == Family::elementwise;
       if (grp.size() >= 2 && ends_elem && inner_n <= 16384 && inner_n >= 256) {
         plan.row_groups.push_back(grp);
-        for (int k : grp) st[k].family = Family::row_chain;
+        for (int k : grp) {
+          st[k].family = Family::row_chain;
+          if (st[k].pins.any()) {  // the fused row kernel has its own mapping
+            st[k].pins = StagePins{};
+            st[k].text += " (parallel/unroll not applied: fused into a row chain)";
+          }
+        }
         for (size_t k = 0; k < grp.size(); ++k) st[grp[k]].rows_from = grp[0];
         if (is_softmax(grp))
           for (int k : grp) st[k].dev.pattern = LTB_P_SOFTMAX;

@@ -4,8 +4,9 @@
 // LoopTree over it computes too: element values follow the reference "cpp"
 // backend (cpp.cpp:172-270: left folds, ternary min/max, out-of-bounds reads
 // as 0), index equations follow Compiler::gen_index_equations
-// (compile.cpp:611-756).  The LoopTree schedule (orders, splits,
-// annotations) is a tuning hint here, not a semantic input.
+// (compile.cpp:611-756).  The LoopTree schedule does not change values
+// beyond what the reference's own order does (reductions fold in the
+// node's loop order); its loop annotations pin launch choices (StagePins).
 #pragma once
 
 #include <string>
@@ -47,8 +48,31 @@ struct Contraction {
   bool a_guarded = false, b_guarded = false;
 };
 
+// What the loop annotations of a stage's node ask for (LoopTree loop
+// annotations: IR::annotate_loop, ir.h:183-195, set by annotate(),
+// mutate.cpp:694-712; the reference's vocabulary is "parallel", "unroll",
+// "vectorize" and "[backend]").  A loop's iteration count is its size plus
+// one when it has a tail.
+struct StagePins {
+  // "parallel" loops over the stage's output vars: the product of their
+  // iteration counts is the number of device threads the stage runs with
+  // (CTAs x CTA size); the innermost such loop, when there are two or more,
+  // is the CTA size.  0: free.
+  int64_t parallel_out = 0;
+  int cta_threads = 0;
+  // "parallel" loops over reduced vars: the width of the parallel
+  // reduction (threads per output, or split-K partials).  0: free.
+  int64_t parallel_red = 0;
+  // "unroll": iteration count of the innermost unrolled loop (items per
+  // thread where the family has that choice).  0: free.
+  int unroll = 0;
+  bool any() const { return parallel_out || parallel_red || unroll; }
+  std::string text;  // what the plan made of the annotations
+};
+
 struct PlanStage {
   Family family = Family::elementwise;
+  StagePins pins;
   int node = -1;
   std::vector<int> dim_vars;  // stage iteration vars: outputs then reduced
   LtbStage dev{};             // device descriptor

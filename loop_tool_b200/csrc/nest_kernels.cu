@@ -8,6 +8,7 @@
 #include <tuple>
 
 #include "async.cuh"
+#include "compensated.cuh"
 #include "kernels.h"
 #include "vm.cuh"
 
@@ -169,12 +170,7 @@ __global__ void __launch_bounds__(256)
         } else if (op == LTB_V_FOLD) {
           if (S.kahan) {
 #pragma unroll
-            for (int j = 0; j < VEC; ++j) {  // Kahan-Babuska summation
-              const float y = s0.v[j] - comp[j];
-              const float t = acc[j] + y;
-              comp[j] = (t - acc[j]) - y;
-              acc[j] = t;
-            }
+            for (int j = 0; j < VEC; ++j) comp_add(acc[j], comp[j], s0.v[j]);
           } else {
 #pragma unroll
             for (int j = 0; j < VEC; ++j) acc[j] = fold(S.red_op, acc[j], s0.v[j]);
@@ -199,7 +195,8 @@ __global__ void __launch_bounds__(256)
     for (int k = 0; k < no; ++k) obase += S.out_coef[k] * x[k];
     float res[VEC];
 #pragma unroll
-    for (int j = 0; j < VEC; ++j) res[j] = has_red ? acc[j] : s0.v[j];
+    for (int j = 0; j < VEC; ++j)
+      res[j] = !has_red ? s0.v[j] : S.kahan ? comp_value(acc[j], comp[j]) : acc[j];
     if (VEC == 4 && ostep == 1 && nv == 4 && (obase & 3) == 0) {
       *reinterpret_cast<float4*>(out + obase) =
           make_float4(res[0], res[1 % VEC], res[2 % VEC], res[3 % VEC]);
@@ -238,10 +235,7 @@ __device__ __forceinline__ void part_add(Part& p, int op, int kahan, float x,
   switch (op) {
     case LTB_R_ADD:
       if (kahan) {
-        const float y = x - p.c;
-        const float t = p.v + y;
-        p.c = (t - p.v) - y;
-        p.v = t;
+        comp_add(p.v, p.c, x);
       } else {
         p.v += x;
       }
@@ -264,13 +258,8 @@ __device__ __forceinline__ Part part_combine(int op, Part a, Part b) {
   r.nan = a.nan | b.nan;
   switch (op) {
     case LTB_R_ADD: {
-      // TwoSum of the running values; their rounding error joins the
-      // compensation terms (true sum ~= v - c)
-      const float s = a.v + b.v;
-      const float bp = s - a.v;
-      const float e = (a.v - (s - bp)) + (b.v - bp);
-      r.c = a.c + b.c - e;
-      r.v = s;
+      // TwoSum of the running values (true sum ~= v - c)
+      comp_combine(r.v, r.c, b.v, b.c);
       break;
     }
     case LTB_R_MUL: r.v = a.v * b.v; break;
@@ -398,9 +387,9 @@ __global__ void __launch_bounds__(256)
         res = fold(S.red_op, S.red_init, p.v);
         if (p.i < 0) res = S.red_init;
       } else if (splits == 1) {
-        res = fold(S.red_op, S.red_init, p.v - p.c);
+        res = fold(S.red_op, S.red_init, comp_value(p.v, p.c));
       } else {
-        res = p.v - p.c;
+        res = comp_value(p.v, p.c);
       }
       if (splits == 1) {
         int64_t ob = S.out_off;
@@ -550,7 +539,7 @@ __global__ void __launch_bounds__(512)
           } else if (ordered) {
             res = p.i < 0 ? T.red_init : fold(T.red_op, T.red_init, p.v);
           } else {
-            res = fold(T.red_op, T.red_init, p.v - p.c);
+            res = fold(T.red_op, T.red_init, comp_value(p.v, p.c));
           }
           rs_slot[nrs] = T.out_buf;
           rs_val[nrs] = res;
@@ -1095,6 +1084,7 @@ static int resident(const void* kernel, int threads, size_t smem = 0) {
 template <typename K>
 static int grid_of(K kernel, int64_t work, int threads, int sms, const LtbCfg& cfg,
                    size_t smem = 0) {
+  if (cfg.grid > 0) return cfg.grid;  // pinned (grid-stride kernels cover any work)
   int64_t blocks = (work + threads - 1) / threads;
   const int per_sm = cfg.cta_per_sm > 0
                          ? cfg.cta_per_sm
@@ -1321,6 +1311,7 @@ cudaError_t ltb_launch_reduce(const LtbStage* d_stage, const LtbStage& h,
   // one CTA per output, up to a cap of CTAs per SM (block-stride over outputs)
   const int64_t per_sm = cfg.cta_per_sm > 0 ? cfg.cta_per_sm : 64;
   int64_t gx = outs < (int64_t)sms * per_sm ? outs : (int64_t)sms * per_sm;
+  if (cfg.grid > 0) gx = cfg.grid < outs ? cfg.grid : outs;  // pinned
   if (gx < 1) gx = 1;
   dim3 grid((unsigned)gx, (unsigned)splits);
   k_reduce_par<<<grid, threads, 0, st>>>(d_stage, bt, outs);

@@ -28,6 +28,7 @@
 #include <string>
 
 #include "../../include/loop_tool_b200.h"
+#include "compensated.cuh"
 #include "kernels.h"
 
 #define LTB_NOALLOC_SCRATCH_FLOATS (1 << 20)
@@ -41,10 +42,8 @@ struct KahanPart {
 };
 
 __device__ __forceinline__ KahanPart kp_combine(KahanPart a, KahanPart b) {
-  const float s = a.v + b.v;
-  const float bp = s - a.v;
-  const float e = (a.v - (s - bp)) + (b.v - bp);
-  return KahanPart{s, a.c + b.c - e};
+  ltbdev::comp_combine(a.v, a.c, b.v, b.c);
+  return a;
 }
 
 // block (row, split): compensated sum of one contiguous chunk of one row
@@ -59,10 +58,7 @@ __global__ void __launch_bounds__(256)
     const float* __restrict__ p = x + row * cols;
     KahanPart acc{0.f, 0.f};
     for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-      const float y = __ldg(p + c) - acc.c;
-      const float t = acc.v + y;
-      acc.c = (t - acc.v) - y;
-      acc.v = t;
+      ltbdev::comp_add(acc.v, acc.c, __ldg(p + c));
     }
     for (int off = 16; off > 0; off >>= 1) {
       KahanPart o{__shfl_down_sync(0xffffffffu, acc.v, off),
@@ -74,7 +70,7 @@ __global__ void __launch_bounds__(256)
     if (threadIdx.x == 0) {
       KahanPart r = sm[0];
       for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = kp_combine(r, sm[w]);
-      part[row * splits + blockIdx.y] = r.v - r.c;
+      part[row * splits + blockIdx.y] = ltbdev::comp_value(r.v, r.c);
     }
     __syncthreads();
   }
@@ -86,13 +82,8 @@ __global__ void k_rowsum_combine(const float* __restrict__ part, int64_t rows, i
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
        r += (int64_t)gridDim.x * blockDim.x) {
     float acc = 0.f, c = 0.f;
-    for (int s = 0; s < splits; ++s) {
-      const float y = part[r * splits + s] - c;
-      const float t = acc + y;
-      c = (t - acc) - y;
-      acc = t;
-    }
-    out[r] = acc;
+    for (int s = 0; s < splits; ++s) ltbdev::comp_add(acc, c, part[r * splits + s]);
+    out[r] = ltbdev::comp_value(acc, c);
   }
 }
 
@@ -103,13 +94,15 @@ int noalloc_fail(int code, const std::string& msg) {
   return ltb_set_last_error(code, msg.c_str());
 }
 
-bool on_device(const void* p) {
+// Memory the kernels on device `dev` can read: managed memory, or device
+// memory of `dev` itself (another GPU's memory would be a peer access).
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes a{};
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
 }
 
 }  // namespace
@@ -123,12 +116,13 @@ extern "C" int ltb_row_sum_noalloc(const float* x, int64_t rows, int64_t cols, f
     return noalloc_fail(LTB_ERR_INVALID,
                         "rows (" + std::to_string(rows) + ") exceed the no-alloc scratch (" +
                             std::to_string(LTB_NOALLOC_SCRATCH_FLOATS) + " partial sums)");
-  if (!on_device(x) || !on_device(out))
-    return noalloc_fail(LTB_ERR_INVALID,
-                        "device or managed buffers required: this entry point stages nothing");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return noalloc_fail(LTB_ERR_CUDA, "no current CUDA device");
+  if (!on_device(x, dev) || !on_device(out, dev))
+    return noalloc_fail(LTB_ERR_INVALID,
+                        "managed buffers or device buffers of the current device required: "
+                        "this entry point stages nothing");
   void* part = nullptr;
   {
     std::lock_guard<std::mutex> g(g_mu);

@@ -151,6 +151,65 @@ T* upload(const std::vector<T>& v, std::vector<void*>& owned) {
 
 int ltb_set_last_error(int code, const char* msg) { return fail(code, msg); }
 
+namespace {
+
+// Timeout flags of the bounded waits, one per (device, stream).  A kernel
+// whose wait gives up raises the flag of the stream it was launched on; the
+// next synchronising call on that stream (ltb_run / ltb_graph_run with
+// sync, ltb_synchronize, ltb_tune) reports LTB_ERR_TIMEOUT and clears it, so
+// an asynchronous run's timeout is charged to its own stream, not to
+// whichever run synchronises next.  Each device's table is one allocation,
+// made when the first loop tree is compiled on it (never in a run); with
+// more than kFlagSlots distinct streams on a device, later streams share
+// slots (a timeout is then reported on every stream of its slot).
+constexpr int kFlagSlots = 1024;
+struct FlagTable {
+  int* d = nullptr;
+  std::map<uintptr_t, int> slot;
+};
+std::mutex g_flag_mu;
+FlagTable g_flags[64];
+
+void ensure_flag_table(int dev) {
+  std::lock_guard<std::mutex> g(g_flag_mu);
+  FlagTable& t = g_flags[dev];
+  if (t.d) return;
+  CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&t.d), kFlagSlots * sizeof(int)));
+  CUDA_TRY(cudaMemset(t.d, 0, kFlagSlots * sizeof(int)));
+}
+
+// the flag of stream st on device dev (its table exists)
+int* timeout_flag(int dev, cudaStream_t st) {
+  std::lock_guard<std::mutex> g(g_flag_mu);
+  FlagTable& t = g_flags[dev];
+  const uintptr_t key = reinterpret_cast<uintptr_t>(st);
+  auto it = t.slot.find(key);
+  if (it != t.slot.end()) return t.d + it->second;
+  const int n = (int)t.slot.size();
+  const int s = n < kFlagSlots ? n : (int)(key % kFlagSlots);
+  t.slot[key] = s;
+  return t.d + s;
+}
+
+// After stream st has been synchronised: true (and the flag cleared) if a
+// bounded wait launched on it gave up.
+bool take_timeout(int dev, cudaStream_t st) {
+  {
+    std::lock_guard<std::mutex> g(g_flag_mu);
+    if (!g_flags[dev].d) return false;
+  }
+  int* f = timeout_flag(dev, st);
+  int flag = 0;
+  CUDA_TRY(cudaMemcpyAsync(&flag, f, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (!flag) return false;
+  CUDA_TRY(cudaMemsetAsync(f, 0, sizeof(int), st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return true;
+}
+
+}  // namespace
+
 struct ltb_compiled {
   std::string ir_text;
   ltb::IRGraph ir;
@@ -167,7 +226,7 @@ struct ltb_compiled {
   std::vector<int> gemm_of;           // stage -> index into gemms (or -1)
   std::vector<void*> owned;           // device allocations to free
   std::mutex mu;                      // guards the default scratch block
-  int* d_err = nullptr;               // device-side timeout flag
+  cudaEvent_t scratch_done = nullptr; // recorded after each run on the default scratch
   int64_t bandwidth_gbs = 0;
   int launches = 0;
   std::vector<LtbCfg> cfg;            // per stage launch schedule (autotuner)
@@ -480,6 +539,8 @@ const DeviceInfo& device_info(int dev) {
   return d;
 }
 
+void pin_cfg(ltb_compiled* c, int i);
+
 void compile_device(ltb_compiled* c) {
   CUDA_TRY(cudaGetDevice(&c->device));
   const DeviceInfo& di = device_info(c->device);
@@ -495,6 +556,9 @@ void compile_device(ltb_compiled* c) {
       const int64_t outs = stage_outs(st.dev);
       int64_t splits = (4LL * c->sms + outs - 1) / outs;
       splits = std::min<int64_t>(splits, std::max<int64_t>(1, st.dev.red_total / 4096));
+      // a "parallel" loop over the reduced var: that many threads in all,
+      // 256 per partial
+      if (st.pins.parallel_red > 256) splits = (st.pins.parallel_red + 255) / 256;
       splits = std::max<int64_t>(1, std::min<int64_t>(splits, 2048));
       c->split_of[i] = (int)splits;
       st.dev.split = (int)splits;
@@ -525,7 +589,6 @@ void compile_device(ltb_compiled* c) {
   std::vector<LtbStage> hs;
   for (auto& st : P.stages) hs.push_back(st.dev);
   ar.add(hs, &c->d_stages);
-  ar.add(std::vector<int>{0}, &c->d_err);
   ar.finalize(c->owned);
   int launches = 0;
   for (int i = 0; i < ns; ++i) {
@@ -542,28 +605,59 @@ void compile_device(ltb_compiled* c) {
   }
   c->launches = launches;
   c->cfg.assign(ns, LtbCfg{0, 0, 0});
-  for (int i = 0; i < ns; ++i)
+  for (int i = 0; i < ns; ++i) {
     if (c->gemm_of[i] >= 0 && c->gemms[c->gemm_of[i]].tc)
       c->cfg[i].variant = c->gemms[c->gemm_of[i]].bn;
+    pin_cfg(c, i);
+  }
 }
 
-bool is_device_accessible(const void* p) {
+// How a run treats one caller buffer (ltb_run_plan reports it).  The
+// kernels read and write a buffer in place only when it is device memory
+// of the compiled object's device, or managed memory, and 16-byte aligned:
+// the elementwise, window and softmax kernels move 16-byte vectors wherever
+// a row's offsets allow, and the tensor-core operand packers and the TMA
+// engine need 16-byte aligned addresses.  Every other buffer a run accepts
+// is staged through an aligned device copy.
+enum BufKind {
+  kBufHost = 0,        // pageable or pinned host memory: staged
+  kBufDevice = 1,      // device memory of this device, aligned: in place
+  kBufManaged = 2,     // managed memory, aligned: in place (prefetched)
+  kBufMisaligned = 3,  // device/managed memory off a 16-byte boundary: staged
+  kBufForeign = -1,    // another GPU's memory: rejected (a peer access)
+};
+
+int buffer_kind(const void* p, int dev) {
   cudaPointerAttributes a{};
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return kBufHost;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeDevice && a.device != dev) return kBufForeign;
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return kBufHost;
+  if (reinterpret_cast<uintptr_t>(p) & 15) return kBufMisaligned;
+  return a.type == cudaMemoryTypeManaged ? kBufManaged : kBufDevice;
 }
 
-// 0: host (pageable or pinned), 1: device, 2: managed.
-int mem_kind(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return 0;
+const char* buffer_kind_text(int k) {
+  switch (k) {
+    case kBufHost: return "host memory: staged through device memory";
+    case kBufDevice: return "device memory: read/written in place";
+    case kBufManaged: return "managed memory: prefetched, read/written in place";
+    case kBufMisaligned: return "device/managed memory off a 16-byte boundary: staged "
+                                "through an aligned device copy";
+    default: return "another device's memory: rejected";
   }
-  return a.type == cudaMemoryTypeManaged ? 2 : a.type == cudaMemoryTypeDevice ? 1 : 0;
+}
+
+// Entry points that run kernels on caller buffers without staging
+// (captured runs, batches, the autotuner) accept in-place buffers only.
+void require_in_place(const void* p, int dev, const char* what) {
+  if (!p) throw ltb::Error(std::string(what) + ": null buffer");
+  const int k = buffer_kind(p, dev);
+  if (k != kBufDevice && k != kBufManaged)
+    throw ltb::Error(std::string(what) + " need 16-byte aligned device or managed buffers of the "
+                     "compiled object's device; got " + buffer_kind_text(k));
 }
 
 
@@ -593,7 +687,9 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         n++;
       const LtbStage* hs[16];
       for (int k = 0; k < n && k < 16; ++k) hs[k] = &P.stages[i + k].dev;
-      e = n <= 16 ? ltb_launch_row_chain(d, hs, n, bt, c->sms, st, cfg, c->d_err) : cudaErrorInvalidValue;
+      e = n <= 16 ? ltb_launch_row_chain(d, hs, n, bt, c->sms, st, cfg,
+                                        timeout_flag(c->device, st))
+                   : cudaErrorInvalidValue;
       break;
     }
     case ltb::Family::contraction: {
@@ -651,7 +747,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           one.c = p.c;
           one.crow = t.c_row;
           one.ccol = t.c_col;
-          e = ltb_launch_gemm_tc(t.bn | t.epi, nullptr, 1, t.tiles, nullptr, c->sms, c->d_err, st,
+          e = ltb_launch_gemm_tc(t.bn | t.epi, nullptr, 1, t.tiles, nullptr, c->sms,
+                                 timeout_flag(c->device, st), st,
                                  &one, maps, maps + 128, t.img ? maps + 256 : nullptr);
         }
       }
@@ -673,8 +770,44 @@ void launch_plan(ltb_compiled* c, const LtbBufTable& bt, cudaStream_t st) {
 
 // Apply a schedule to stage i (the tile width of a tensor-core contraction
 // changes its tile count).
+// The launch choices a stage's loop annotations pin (StagePins), on top of
+// whatever schedule it has: "parallel" over output vars fixes threads x
+// CTAs of the grid-stride families (and the CTA count of the per-output
+// reduction), "parallel" over reduced vars the threads per output of the
+// tree reduction (split-K counts are fixed when the object is compiled),
+// "unroll" 4 (or 2) the work items per thread of the pooling window kernel.
+void pin_cfg(ltb_compiled* c, int i) {
+  const auto& s = c->plan.stages[i];
+  const ltb::StagePins& pn = s.pins;
+  if (!pn.any()) return;
+  LtbCfg& cf = c->cfg[i];
+  auto warp_round = [](int64_t t) {
+    t = std::max<int64_t>(32, std::min<int64_t>(t, 256));
+    return (int)(t / 32 * 32);
+  };
+  switch (s.family) {
+    case ltb::Family::elementwise:
+    case ltb::Family::reduce_serial:
+      if (pn.parallel_out) {
+        const int t = warp_round(pn.cta_threads ? pn.cta_threads : pn.parallel_out);
+        cf.threads = t;
+        cf.grid = (int)std::min<int64_t>((pn.parallel_out + t - 1) / t, 1 << 30);
+      }
+      if (pn.unroll) cf.variant = pn.unroll >= 4 ? 4 : 2;
+      break;
+    case ltb::Family::reduce_parallel:
+    case ltb::Family::reduce_split:
+      if (pn.parallel_red) cf.threads = warp_round(pn.parallel_red);
+      if (pn.parallel_out) cf.grid = (int)std::min<int64_t>(pn.parallel_out, 1 << 30);
+      break;
+    default:
+      break;
+  }
+}
+
 void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
   c->cfg[i] = cfg;
+  pin_cfg(c, i);
   const int g = c->gemm_of[i];
   if (g >= 0 && c->gemms[g].tc) {
     // variant: tile width | form, form 0: row-store epilogue, 1: transposed
@@ -698,6 +831,7 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
                                      " buffers, got " + std::to_string(n));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   std::unique_lock<std::mutex> lock(c->mu, std::defer_lock);
+  const bool default_scratch = !scratch;
   if (!scratch) {
     lock.lock();
     if (!c->scratch && c->scratch_bytes) {
@@ -724,9 +858,14 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
     bool all_host = true;
     for (int i = 0; i < n; ++i) {
       if (!memory[i]) return fail(LTB_ERR_INVALID, "null buffer " + std::to_string(i));
-      kind[i] = mem_kind(memory[i]);
-      all_host = all_host && kind[i] == 0;
+      kind[i] = buffer_kind(memory[i], c->device);
+      if (kind[i] == kBufForeign)
+        return fail(LTB_ERR_INVALID, "buffer " + std::to_string(i) + ": " +
+                                         buffer_kind_text(kind[i]));
+      all_host = all_host && kind[i] == kBufHost;
     }
+    if (scratch && (reinterpret_cast<uintptr_t>(scratch) & 255))
+      return fail(LTB_ERR_INVALID, "caller scratch must be 256-byte aligned");
     constexpr int64_t kChunk = int64_t(1) << 24;  // elements per chunk (64 MB of FP32)
     const int64_t total = P.n_out ? P.io_elems[P.n_in] : 0;
     bool same = true;
@@ -774,23 +913,25 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
     // in bulk before the launch instead of page by page on first touch
     std::vector<int> managed;
     for (int i = 0; i < n; ++i)
-      if (kind[i] == 2) {
+      if (kind[i] == kBufManaged) {
         managed.push_back(i);
         const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[i], 1) * 4;
         if (cudaMemPrefetchAsync(memory[i], bytes, c->device, st) != cudaSuccess)
           cudaGetLastError();  // advisory only
       }
     for (int i = 0; i < n; ++i) {
-      if (kind[i] != 0) {
+      if (kind[i] == kBufDevice || kind[i] == kBufManaged) {
         bt.p[i] = static_cast<float*>(memory[i]);
         continue;
       }
+      // host memory, or device/managed memory off a 16-byte boundary:
+      // an aligned device copy (cudaMallocAsync blocks are 256-byte aligned)
       const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[i], 1) * 4;
       void* d = nullptr;
       CUDA_TRY(cudaMallocAsync(&d, bytes, st));
       temps.push_back(d);
       if (i < P.n_in)
-        CUDA_TRY(cudaMemcpyAsync(d, memory[i], bytes, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(d, memory[i], bytes, cudaMemcpyDefault, st));
       else
         staged.push_back({i, memory[i]});
       bt.p[i] = static_cast<float*>(d);
@@ -798,10 +939,25 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
     for (size_t k = 0; k < P.scratch_elems.size(); ++k)
       bt.p[P.n_in + P.n_out + k] =
           reinterpret_cast<float*>(static_cast<char*>(scratch) + c->scratch_off[k]);
+    // The default scratch is shared by every run of this object that brings
+    // none: this run's kernels wait (on the device) for the previous such
+    // run, which may still be executing on another stream.  Skipped while
+    // the stream is being captured (an event recorded outside a capture
+    // cannot be waited on inside it).
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    const bool order = default_scratch && c->scratch_bytes && cap == cudaStreamCaptureStatusNone;
+    if (order) {
+      if (!c->scratch_done)
+        CUDA_TRY(cudaEventCreateWithFlags(&c->scratch_done, cudaEventDisableTiming));
+      else
+        CUDA_TRY(cudaStreamWaitEvent(st, c->scratch_done, 0));
+    }
     launch_plan(c, bt, st);
+    if (order) CUDA_TRY(cudaEventRecord(c->scratch_done, st));
     for (auto& s : staged) {
       const size_t bytes = (size_t)std::max<int64_t>(P.io_elems[s.first], 1) * 4;
-      CUDA_TRY(cudaMemcpyAsync(s.second, bt.p[s.first], bytes, cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaMemcpyAsync(s.second, bt.p[s.first], bytes, cudaMemcpyDefault, st));
     }
     for (void* d : temps) CUDA_TRY(cudaFreeAsync(d, st));
     // a synchronous run's managed outputs go back to the host in bulk: the
@@ -817,12 +973,8 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
     // are complete once the stream is (Compiled::async)
     if (sync) {
       CUDA_TRY(cudaStreamSynchronize(st));
-      int flag = 0;
-      CUDA_TRY(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-      if (flag) {
-        CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
-        return fail(LTB_ERR_TIMEOUT, "a bounded wait in a tensor-core kernel gave up");
-      }
+      if (take_timeout(c->device, st))
+        return fail(LTB_ERR_TIMEOUT, "a bounded wait in a kernel on this stream gave up");
     }
   } catch (const CudaFailure& e) {
     return fail(LTB_ERR_CUDA, e.what());
@@ -982,6 +1134,147 @@ void record_schedule(ltb_compiled* c, const std::vector<double>& us) {
 }
 
 // Schedules from the cache, if this IR + options were tuned before.
+// ---------------------------------------------------- schedule as IR text
+// The launch schedule of the grid-stride and tree-reduction stages written
+// back into the loop tree as the reference's own vocabulary: the stage's
+// outermost unsplit output loop v of size S becomes
+//   v (S / (G*T), S % (G*T)), v (G) "parallel", v (T) "parallel"
+// (G CTAs of T threads), and the innermost unsplit reduced loop r of size
+// R of a tree reduction becomes r (R / T, R % T), r (T) "parallel" (T
+// threads per output).  Splits keep every loop's visiting order, so values
+// are unchanged (reductions still fold in ascending index order).  Stages
+// whose choices the vocabulary cannot express (fused row kernels, tile
+// kernels) keep their schedule in the schedule cache only.
+std::vector<std::string> split_keep(const std::string& s, char sep) {
+  std::vector<std::string> out;
+  size_t a = 0;
+  while (true) {
+    size_t b = s.find(sep, a);
+    out.push_back(s.substr(a, b == std::string::npos ? std::string::npos : b - a));
+    if (b == std::string::npos) break;
+    a = b + 1;
+  }
+  return out;
+}
+
+struct OrderEdit {
+  std::vector<std::pair<int, ltb::LoopSize>> order;
+  std::vector<std::string> annots;
+};
+
+OrderEdit node_order(const ltb::Node& N) {
+  OrderEdit e;
+  e.order = N.order;
+  e.annots.assign(N.order.size(), "");
+  for (size_t i = 0; i < N.order.size() && i < N.loop_annotations.size(); ++i)
+    e.annots[i] = N.loop_annotations[i];
+  return e;
+}
+
+// replace entry i by the given loops (same var), keeping annotations elsewhere
+void split_entry(OrderEdit& e, size_t i, const std::vector<std::pair<ltb::LoopSize, std::string>>& parts) {
+  const int v = e.order[i].first;
+  std::vector<std::pair<int, ltb::LoopSize>> o(e.order.begin(), e.order.begin() + i);
+  std::vector<std::string> a(e.annots.begin(), e.annots.begin() + i);
+  for (auto& p : parts) {
+    o.push_back({v, p.first});
+    a.push_back(p.second);
+  }
+  o.insert(o.end(), e.order.begin() + i + 1, e.order.end());
+  a.insert(a.end(), e.annots.begin() + i + 1, e.annots.end());
+  e.order = o;
+  e.annots = a;
+}
+
+// the unsplit entry of a var in `vars`: outermost (first) or innermost (last)
+int unsplit_entry(const OrderEdit& e, const std::vector<int>& vars, bool innermost) {
+  int found = -1;
+  for (size_t i = 0; i < e.order.size(); ++i) {
+    const int v = e.order[i].first;
+    if (std::find(vars.begin(), vars.end(), v) == vars.end()) continue;
+    int n = 0;
+    for (auto& o : e.order) n += o.first == v;
+    if (n != 1 || e.order[i].second.tail != 0) continue;
+    if (!innermost) return (int)i;
+    found = (int)i;
+  }
+  return found;
+}
+
+std::string schedule_ir(ltb_compiled* c) {
+  auto lines = split_keep(c->ir_text, '\n');
+  std::vector<size_t> node_line;
+  for (size_t l = 0; l < lines.size(); ++l)
+    if (lines[l].rfind("n:", 0) == 0) node_line.push_back(l);
+  const auto& P = c->plan;
+  std::map<int, OrderEdit> edits;
+  for (size_t i = 0; i < P.stages.size(); ++i) {
+    const auto& s = P.stages[i];
+    const LtbCfg& cf = c->cfg[i];
+    if (s.pins.any() || s.node < 0 || s.node >= (int)node_line.size()) continue;
+    const bool grid_stride = s.family == ltb::Family::elementwise ||
+                             s.family == ltb::Family::reduce_serial;
+    const bool tree = s.family == ltb::Family::reduce_parallel;
+    if (!grid_stride && !tree) continue;
+    const ltb::Node& N = c->ir.nodes[s.node];
+    OrderEdit e = edits.count(s.node) ? edits[s.node] : node_order(N);
+    const int nout = s.dev.nout;
+    std::vector<int> outv(s.dim_vars.begin(), s.dim_vars.begin() + nout);
+    std::vector<int> redv(s.dim_vars.begin() + nout, s.dim_vars.end());
+    const int T = cf.threads > 0 ? cf.threads
+                                 : grid_stride ? 256 : (s.dev.red_total >= 256 ? 256 : 128);
+    const int64_t G = cf.grid > 0 ? cf.grid : cf.cta_per_sm > 0 ? (int64_t)c->sms * cf.cta_per_sm : 0;
+    if (tree) {
+      const int k = unsplit_entry(e, redv, true);
+      if (k >= 0 && e.order[k].second.size >= T) {
+        const int64_t R = e.order[k].second.size;
+        split_entry(e, (size_t)k, {{{R / T, R % T}, e.annots[k]}, {{T, 0}, "parallel"}});
+      }
+    }
+    if (G > 0) {
+      const int k = unsplit_entry(e, outv, false);
+      const int64_t GT = G * (grid_stride ? T : 1);
+      if (k >= 0 && e.order[k].second.size >= GT) {
+        const int64_t S = e.order[k].second.size;
+        if (grid_stride)
+          split_entry(e, (size_t)k, {{{S / GT, S % GT}, e.annots[k]}, {{G, 0}, "parallel"},
+                                     {{T, 0}, "parallel"}});
+        else
+          split_entry(e, (size_t)k, {{{S / G, S % G}, e.annots[k]}, {{G, 0}, "parallel"}});
+      }
+    }
+    edits[s.node] = e;
+  }
+  for (auto& kv : edits) {
+    auto f = split_keep(lines[node_line[kv.first]], ':');
+    if (f.size() != 11) continue;
+    std::ostringstream o, a;
+    for (auto& x : kv.second.order) o << x.first << ";" << x.second.size << ";" << x.second.tail << ",";
+    for (auto& x : kv.second.annots) a << x << ",";
+    const std::string old_order = f[7];
+    f[7] = o.str();
+    f[9] = a.str();
+    std::string ln;
+    for (size_t j = 0; j < f.size(); ++j) ln += (j ? ":" : "") + f[j];
+    lines[node_line[kv.first]] = ln;
+    // a write fused into this node shares its loops in the reference's tree
+    for (int w : c->ir.outputs) {
+      const auto& W = c->ir.nodes[w];
+      if (W.inputs.size() != 1 || W.inputs[0] != kv.first || edits.count(w)) continue;
+      auto fw = split_keep(lines[node_line[w]], ':');
+      if (fw.size() != 11 || fw[7] != old_order) continue;
+      fw[7] = f[7];
+      fw[9] = f[9];
+      std::string lw;
+      for (size_t j = 0; j < fw.size(); ++j) lw += (j ? ":" : "") + fw[j];
+      lines[node_line[w]] = lw;
+    }
+  }
+  std::string out;
+  for (size_t l = 0; l < lines.size(); ++l) out += (l ? "\n" : "") + lines[l];
+  return out;
+}
+
 void lookup_schedule(ltb_compiled* c) {
   c->key = fnv1a(c->ir_text, canon_options(c->opt));
   std::lock_guard<std::mutex> g(g_tune_mu);
@@ -1101,9 +1394,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
       if (t.tc != b->tc || (t.tc && t.nseg != cs[0]->gemms[0].nseg))
         throw ltb::Error("batch members must share one precision");
       const int nio = c->plan.n_in + c->plan.n_out;
-      for (int k = 0; k < nio; ++k)
-        if (!memories[i] || !memories[i][k] || !is_device_accessible(memories[i][k]))
-          throw ltb::Error("batch buffers must be device or managed memory");
+      if (!memories[i]) throw ltb::Error("batch member without buffers");
+      for (int k = 0; k < nio; ++k) require_in_place(memories[i][k], b->device, "batches");
       auto ptr = [&](int slot) { return static_cast<float*>(memories[i][slot]); };
       const LtbLoad& A = s.dev.loads[s.con.a_load];
       const LtbLoad& B = s.dev.loads[s.con.b_load];
@@ -1404,6 +1696,7 @@ int ltb_compile(const char* ir_text, const char* options, ltb_compiled** out) {
     return fail(LTB_ERR_NO_DEVICE, "no sm_100 CUDA device visible");
   }
   try {
+    ensure_flag_table(c->device);
     compile_device(c);
     lookup_schedule(c);
   } catch (const std::exception& e) {
@@ -1426,9 +1719,34 @@ int ltb_run_with_scratch(ltb_compiled* c, void* const* memory, int n, int sync,
   return run_impl(c, memory, n, sync, stream, scratch);
 }
 
+int ltb_schedule_ir(ltb_compiled* c, char* buf, size_t len) {
+  if (!c) return fail(LTB_ERR_INVALID, "null compiled object");
+  try {
+    return copy_out(schedule_ir(c), buf, len);
+  } catch (const std::exception& e) {
+    return fail(LTB_ERR_INVALID, e.what());
+  }
+}
+
+int ltb_run_plan(ltb_compiled* c, void* const* memory, int n, char* buf, size_t len) {
+  if (!c || !memory) return fail(LTB_ERR_INVALID, "null argument");
+  const auto& P = c->plan;
+  if (n != P.n_in + P.n_out)
+    return fail(LTB_ERR_INVALID, "expected " + std::to_string(P.n_in + P.n_out) +
+                                     " buffers, got " + std::to_string(n));
+  std::ostringstream ss;
+  for (int i = 0; i < n; ++i) {
+    if (!memory[i]) return fail(LTB_ERR_INVALID, "null buffer " + std::to_string(i));
+    ss << (i < P.n_in ? "input " : "output ") << (i < P.n_in ? i : i - P.n_in) << ": "
+       << buffer_kind_text(buffer_kind(memory[i], c->device)) << "\n";
+  }
+  return copy_out(ss.str(), buf, len);
+}
+
 int ltb_release(ltb_compiled* c) {
   if (!c) return LTB_OK;
   if (c->aux) cudaStreamDestroy(c->aux);
+  if (c->scratch_done) cudaEventDestroy(c->scratch_done);
   for (void* p : c->owned) cudaFree(p);
   delete c;
   return LTB_OK;
@@ -1504,6 +1822,7 @@ int ltb_free(void* ptr) {
 // ------------------------------------------------------- captured runs
 struct ltb_graph {
   ltb_compiled* c = nullptr;
+  int* flag = nullptr;  // timeout flag of the capture stream
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -1524,8 +1843,7 @@ int ltb_graph_create(ltb_compiled* c, void* const* memory, int n, void* scratch,
     CUDA_TRY(cudaSetDevice(c->device));
     LtbBufTable bt{};
     for (int i = 0; i < n; ++i) {
-      if (!memory[i] || !is_device_accessible(memory[i]))
-        throw ltb::Error("captured runs need device or managed buffers");
+      require_in_place(memory[i], c->device, "captured runs");
       bt.p[i] = static_cast<float*>(memory[i]);
     }
     if (!scratch) {
@@ -1543,6 +1861,7 @@ int ltb_graph_create(ltb_compiled* c, void* const* memory, int n, void* scratch,
       CUDA_TRY(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
       st = own;
     }
+    g->flag = timeout_flag(c->device, st);
     CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     try {
       launch_plan(c, bt, st);
@@ -1576,11 +1895,12 @@ int ltb_graph_run(ltb_graph* g, int sync, void* stream) {
     CUDA_TRY(cudaGraphLaunch(g->exec, st));
     if (sync) {
       CUDA_TRY(cudaStreamSynchronize(st));
+      // the graph's kernels raise the flag of the stream it was captured on
       int flag = 0;
-      CUDA_TRY(cudaMemcpy(&flag, g->c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+      CUDA_TRY(cudaMemcpy(&flag, g->flag, sizeof(int), cudaMemcpyDeviceToHost));
       if (flag) {
-        CUDA_TRY(cudaMemset(g->c->d_err, 0, sizeof(int)));
-        return fail(LTB_ERR_TIMEOUT, "a bounded wait in a tensor-core kernel gave up");
+        CUDA_TRY(cudaMemset(g->flag, 0, sizeof(int)));
+        return fail(LTB_ERR_TIMEOUT, "a bounded wait in a kernel of this captured run gave up");
       }
     }
   } catch (const std::exception& e) {
@@ -1613,8 +1933,11 @@ int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps
     CUDA_TRY(cudaSetDevice(c->device));
     LtbBufTable bt{};
     for (int i = 0; i < n; ++i) {
-      if (!memory[i] || !is_device_accessible(memory[i]))
-        return fail(LTB_ERR_INVALID, "tuning needs device or managed buffers");
+      try {
+        require_in_place(memory[i], c->device, "tuning runs");
+      } catch (const std::exception& e) {
+        return fail(LTB_ERR_INVALID, e.what());
+      }
       bt.p[i] = static_cast<float*>(memory[i]);
     }
     {
@@ -1656,12 +1979,8 @@ int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps
     }
     launch_plan(c, bt, st);  // outputs from the chosen schedules
     CUDA_TRY(cudaStreamSynchronize(st));
-    int flag = 0;
-    CUDA_TRY(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) {
-      CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
-      throw ltb::Error("a bounded wait in a tensor-core kernel gave up while tuning");
-    }
+    if (take_timeout(c->device, st))
+      throw ltb::Error("a bounded wait in a kernel gave up while tuning");
     c->tuned = true;
     record_schedule(c, best_us);
   } catch (const CudaFailure& e) {
@@ -1783,9 +2102,43 @@ int ltb_tune_load(const char* path) {
   return LTB_OK;
 }
 
+int ltb_check_bounded_wait(int64_t limit_cycles, void* stream, int* completed, int* drained) {
+  if (limit_cycles < 1 || limit_cycles > 4000000000LL)
+    return fail(LTB_ERR_INVALID, "limit_cycles must be in [1, 4e9]");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  try {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(LTB_ERR_INVALID, "device index out of range");
+    ensure_flag_table(dev);
+    int status[2] = {-1, -1};
+    CUDA_TRY(ltb_launch_wait_check(timeout_flag(dev, st), limit_cycles, status, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (completed) *completed = status[0];
+    if (drained) *drained = status[1];
+    if (take_timeout(dev, st))
+      return fail(LTB_ERR_TIMEOUT, "the bounded wait gave up (the self-check's expected outcome)");
+  } catch (const std::exception& e) {
+    return fail(LTB_ERR_CUDA, e.what());
+  }
+  return LTB_OK;
+}
+
 int ltb_synchronize(void* stream) {
-  cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return fail(LTB_ERR_CUDA, cudaGetErrorString(e));
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return LTB_OK;
+  }
+  try {
+    if (take_timeout(dev, st))
+      return fail(LTB_ERR_TIMEOUT, "a bounded wait in a kernel on this stream gave up");
+  } catch (const std::exception& ex) {
+    return fail(LTB_ERR_CUDA, ex.what());
+  }
   return LTB_OK;
 }
 

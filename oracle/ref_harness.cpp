@@ -19,13 +19,29 @@
 //       Annotates the first loop at <depth> with "[cuda]" (or "[backend]") and runs the tree
 //       through the "cpu_interpreted" backend, which compiles that subtree
 //       with the "cuda" backend and calls it per enclosing iteration.
+//   lt_ref_harness fuzz <out_dir> <in_dir> <seed> <permute> <backend> <program> <params...>
+//       Gives every non-view node of <program>'s IR a random schedule the
+//       way the reference's own randomized test does (test/test.py:56-96
+//       rand_split / rand_sched: each loop var split into up to 3 loops
+//       with random factors and tails), and with <permute> = 1 also
+//       shuffles the order of the var groups (the schedule is a function
+//       of the seed).  Writes the scheduled IR (serialize) to out_dir/ir.txt
+//       and, unless <backend> is "none", that backend's outputs on the
+//       in-memory loop tree to out_dir/<backend><j>.f32.
+//   lt_ref_harness annotate <depth> <annotation> <program> <params...>
+//       Annotates the first loop at <depth> of <program>'s loop tree with
+//       <annotation> through the reference's own annotate()
+//       (mutate.cpp:694-712) and prints serialize() of the result.
 //   lt_ref_harness tree <ir_file>      LoopTree::dump of the IR
 //   lt_ref_harness code <ir_file>      the C the "cpp" backend generates
 //   lt_ref_harness sizes <ir_file>     element counts of every I/O buffer
 #include <loop_tool/cpp.h>
 #include <loop_tool/loop_tool.h>
 
+#include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <random>
 #include <cstdio>
 #include <fstream>
 #include <thread>
@@ -248,6 +264,36 @@ static Tensor build(const std::string& prog, const std::vector<int64_t>& p) {
   std::exit(2);
 }
 
+// test/test.py:56-82: the total size of a split list, one split, and up
+// to `attempts` random splits of a (size, tail) loop list
+using Splits = std::vector<std::pair<int64_t, int64_t>>;
+static int64_t split_total(const Splits& s) {
+  int64_t running = 1;
+  for (auto it = s.rbegin(); it != s.rend(); ++it) running = it->first * running + it->second;
+  return running;
+}
+static Splits do_split(const Splits& s, size_t idx, std::pair<int64_t, int64_t> ns) {
+  Splits inner(s.begin() + idx + 1, s.end());
+  const int64_t inner_size = split_total(inner);
+  const int64_t outer_size = s[idx].first * inner_size + s[idx].second;
+  const int64_t new_total = ns.first * inner_size + ns.second;
+  Splits out(s.begin(), s.begin() + idx);
+  out.push_back({outer_size / new_total, outer_size % new_total});
+  out.push_back(ns);
+  out.insert(out.end(), inner.begin(), inner.end());
+  return out;
+}
+static Splits rand_split(Splits s, int attempts, std::mt19937_64& rng) {
+  for (int a = 0; a < attempts; ++a) {
+    const size_t idx = std::uniform_int_distribution<size_t>(0, s.size() - 1)(rng);
+    const int64_t hi = (int64_t)std::sqrt((double)s[idx].first);
+    if (hi < 2) continue;
+    const int64_t f = std::uniform_int_distribution<int64_t>(2, hi)(rng);
+    s = do_split(s, idx, {f, 0});
+  }
+  return s;
+}
+
 static std::string read_file(const std::string& path) {
   std::ifstream f(path);
   std::stringstream ss;
@@ -311,6 +357,85 @@ int main(int argc, char** argv) {
       std::ofstream f(out_dir + "/out0.f32", std::ios::binary);
       f.write(reinterpret_cast<const char*>(out),
               tsizes[tir.inputs().size()] * sizeof(float));
+      return 0;
+    }
+    if (mode == "annotate") {
+      const int depth = std::stoi(argv[2]);
+      const std::string annot = argv[3];
+      std::vector<int64_t> params;
+      for (int i = 5; i < argc; ++i) params.emplace_back(std::stoll(argv[i]));
+      auto T = build(argv[4], params);
+      loop_tool::LoopTree base(T.ir());
+      loop_tool::LoopTree::TreeRef target = -1;
+      base.walk([&](loop_tool::LoopTree::TreeRef r, int d) {
+        if (target < 0 && d == depth && base.kind(r) == loop_tool::LoopTree::LOOP) target = r;
+      });
+      if (target < 0) {
+        std::cerr << "no loop at depth " << depth << "\n";
+        return 3;
+      }
+      std::cout << loop_tool::serialize(loop_tool::annotate(base, target, annot).ir);
+      return 0;
+    }
+    if (mode == "fuzz") {
+      std::string out_dir = argv[2], in_dir = argv[3];
+      std::mt19937_64 rng(std::stoull(argv[4]));
+      const bool permute = std::atoi(argv[5]) != 0;
+      const std::string fbe = argv[6];
+      std::vector<int64_t> params;
+      for (int i = 8; i < argc; ++i) params.emplace_back(std::stoll(argv[i]));
+      auto T = build(argv[7], params);
+      auto ir = T.ir();
+      for (auto n : ir.nodes()) {
+        if (ir.node(n).op() == loop_tool::Operation::view) continue;
+        // the default order holds each loop var once at its full size
+        std::vector<std::pair<int, loop_tool::IR::LoopSize>> order;
+        std::vector<std::vector<std::pair<int, loop_tool::IR::LoopSize>>> groups;
+        for (auto& o : ir.order(n)) {
+          const int attempts = std::uniform_int_distribution<int>(1, 3)(rng);
+          Splits sp = rand_split({{o.second.size, o.second.tail}}, attempts, rng);
+          if (split_total(sp) != split_total({{o.second.size, o.second.tail}})) {
+            std::cerr << "split bookkeeping error\n";
+            return 3;
+          }
+          std::vector<std::pair<int, loop_tool::IR::LoopSize>> g;
+          for (auto& p : sp) g.push_back({o.first, loop_tool::IR::LoopSize{p.first, p.second}});
+          groups.push_back(g);
+        }
+        if (permute) std::shuffle(groups.begin(), groups.end(), rng);
+        for (auto& g : groups) order.insert(order.end(), g.begin(), g.end());
+        ir.set_order(n, order);
+      }
+      std::ofstream(out_dir + "/ir.txt") << loop_tool::serialize(ir);
+      if (fbe == "none") return 0;
+      loop_tool::LoopTree flt(ir);
+      loop_tool::Compiler fc(flt);
+      auto fsizes = fc.memory_sizes(true);
+      const size_t n_in = ir.inputs().size(), n_out = ir.outputs().size();
+      {
+        const std::string be = fbe;
+        std::vector<std::vector<float>> bufs(n_in + n_out);
+        std::vector<void*> mem;
+        for (size_t i = 0; i < n_in + n_out; ++i) {
+          bufs[i].assign(std::max<int64_t>(fsizes[i], 1), 0.f);
+          if (i < n_in) {
+            std::ifstream f(in_dir + "/in" + std::to_string(i) + ".f32", std::ios::binary);
+            f.read(reinterpret_cast<char*>(bufs[i].data()), bufs[i].size() * sizeof(float));
+            if ((size_t)f.gcount() != bufs[i].size() * sizeof(float)) {
+              std::cerr << "short input " << i << "\n";
+              return 3;
+            }
+          }
+          mem.emplace_back(bufs[i].data());
+        }
+        auto cc = loop_tool::getBackends().at(be)->compile(flt);
+        cc->run(mem, true);
+        for (size_t j = 0; j < n_out; ++j) {
+          std::ofstream f(out_dir + "/" + be + std::to_string(j) + ".f32", std::ios::binary);
+          f.write(reinterpret_cast<const char*>(bufs[n_in + j].data()),
+                  bufs[n_in + j].size() * sizeof(float));
+        }
+      }
       return 0;
     }
     if (mode == "subtree") {

@@ -12,7 +12,7 @@ the reference's Compiler then misses some view constraints, e.g. the first
 operand of a concatenation reads index 0).
 
 Run from the repository root after `make -C oracle`:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case names...]
 """
 import json
 import os
@@ -37,6 +37,10 @@ CASES = [
     ("min_specials", "min", [1024], 206, "specials"),
     ("max_specials", "max", [1024], 207, "specials"),
     ("exp_1000", "exp", [1000], 208, "randn"),
+    # log (compile.cpp:1036-1081, op 11): the lazy frontend has no log
+    # (lazy.cpp:221-270), so its IR is the reference's exp IR with the op
+    # replaced, run by both CPU backends
+    ("log_1000", "log", [1000], 233, "log"),
     ("sqrt_1000", "sqrt", [1000], 209, "abs"),
     ("neg_specials", "neg", [512], 210, "specials"),
     ("recip_1000", "recip", [1000], 211, "randn"),
@@ -96,6 +100,9 @@ def make_inputs(kind, sizes, seed):
             a = rng.standard_normal(n)
         elif kind == "abs":
             a = np.abs(rng.standard_normal(n))
+        elif kind == "log":  # positive values, plus log's special arguments
+            a = np.abs(rng.standard_normal(n)) * 10.0 ** rng.integers(-30, 30, n)
+            a[:6] = [0.0, -0.0, 1.0, np.inf, -1.0, np.nan]
         elif kind == "softmax":
             a = 4.0 * rng.standard_normal(n)
         elif kind == "specials":
@@ -136,9 +143,20 @@ def make_inputs(kind, sizes, seed):
 def main():
     if not os.path.exists(HARNESS):
         sys.exit("build the oracle first: make -C oracle")
+    only = set(sys.argv[1:])  # case names to (re)generate; default all
     manifest = []
+    if only:
+        manifest = [m for m in json.load(open(os.path.join(OUT, "manifest.json")))
+                    if m["name"] not in only]
     for name, prog, params, seed, kind in CASES:
-        ir = harness("ir", prog, *params).stdout
+        if only and name not in only:
+            continue
+        if prog == "log":
+            ir = harness("ir", "exp", *params).stdout
+            assert "\nn:12:" in ir
+            ir = ir.replace("\nn:12:", "\nn:11:")
+        else:
+            ir = harness("ir", prog, *params).stdout
         with tempfile.TemporaryDirectory() as td:
             irf = os.path.join(td, "ir.txt")
             open(irf, "w").write(ir)
@@ -163,10 +181,13 @@ def main():
             # the lazy frontend's own run (no serialize round trip): the
             # expected values -- deserialize() gives every node fresh
             # symbols, which changes some view index equations
-            ld = os.path.join(td, "lazy")
-            os.makedirs(ld)
-            harness("lazyrun", ld, td, prog, *params)
-            outs["lazy"] = [np.fromfile(os.path.join(ld, "out0.f32"), dtype=np.float32)]
+            if prog == "log":  # no view in the tree: the C path's output
+                outs["lazy"] = outs["cpp"]
+            else:
+                ld = os.path.join(td, "lazy")
+                os.makedirs(ld)
+                harness("lazyrun", ld, td, prog, *params)
+                outs["lazy"] = [np.fromfile(os.path.join(ld, "out0.f32"), dtype=np.float32)]
             tree = harness("tree", irf).stdout
         arrays = {f"in{i}": a for i, a in enumerate(inputs)}
         arrays["out0_lazy"] = outs["lazy"][0]
@@ -188,6 +209,8 @@ def main():
                          "seed": seed, "kind": kind,
                          "n_in": len(inputs), "n_out": len(sizes["outputs"])})
         print(f"{name}: {len(inputs)} in, {len(sizes['outputs'])} out")
+    order = [c[0] for c in CASES]
+    manifest.sort(key=lambda m: order.index(m["name"]))
     json.dump(manifest, open(os.path.join(OUT, "manifest.json"), "w"), indent=1)
 
 

@@ -15,7 +15,7 @@ import np_oracle  # noqa: E402
 
 # the oracle evaluates exp/log/sqrt in double like the generated C, so it is
 # bit-exact even where the B200 path is within tolerance
-ORACLE_EXACT = EXACT_PROGRAMS | {"exp", "softmax", "rowsum", "colsum", "mm", "bmm",
+ORACLE_EXACT = EXACT_PROGRAMS | {"exp", "log", "softmax", "rowsum", "colsum", "mm", "bmm",
                                  "conv", "padconv1d", "mean_rows", "layernorm", "fullsum"}
 
 
