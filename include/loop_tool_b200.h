@@ -221,6 +221,22 @@ int ltb_set_schedule(ltb_compiled* c, int stage, int cta_per_sm, int threads,
                      int variant);
 /* Store the compiled object's current schedules in the cache. */
 int ltb_tune_record(ltb_compiled* c);
+
+/* The compiled object's current launch schedule written into its loop tree
+ * in the reference's annotation vocabulary (serialize() text that the
+ * reference's deserialize reads, serialization.cpp:239-332; the portable
+ * schedule record of the reference's IR-text format, :175-237).  For each
+ * grid-stride elementwise / serial-reduction stage the outermost unsplit
+ * output loop v of size S is split into v(S / (G*T), S % (G*T)),
+ * v(G) "parallel", v(T) "parallel" -- G CTAs of T threads; for a tree
+ * reduction the innermost unsplit reduced loop r of size R into
+ * r(R / T, R % T), r(T) "parallel" -- T threads per output.  Splits keep
+ * each var's visiting order, so values do not change.  ltb_compile of the
+ * text pins the same choices (a "parallel" loop's iteration counts fix the
+ * thread count; the autotuner leaves pinned choices alone).  Stages whose
+ * choices the vocabulary cannot express (fused row kernels, tensor-core
+ * tiles) keep theirs in the schedule cache (ltb_tune_save). */
+int ltb_schedule_ir(ltb_compiled* c, char* buf, size_t len);
 /* Cache persistence: a text file holding, per entry, the serialized IR
  * (src/core/serialization.cpp:175-237 format), the options and one
  * schedule line per stage.  Loading merges into the cache. */

@@ -65,6 +65,7 @@ SIGNATURES = {
     "ltb_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int]),
     "ltb_tune_record": (ctypes.c_int, [ctypes.c_void_p]),
+    "ltb_schedule_ir": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "ltb_batch_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "ltb_graph_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

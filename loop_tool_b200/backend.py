@@ -122,6 +122,13 @@ class Compiled:
     def __call__(self, tensors, sync=True):
         self.run(tensors, sync)
 
+    def schedule_ir(self):
+        """The current launch schedule as an annotated loop tree (IR text
+        the reference's deserialize reads; ltb_schedule_ir)."""
+        buf = ctypes.create_string_buffer(1 << 22)
+        _lib.check(_lib.lib().ltb_schedule_ir(self._h, buf, len(buf)))
+        return buf.value.decode()
+
     def run_plan(self, memory):
         """How run() would treat each buffer (in place, staged, rejected),
         decided on the host without launching anything."""
