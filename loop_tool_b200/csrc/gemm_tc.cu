@@ -12,7 +12,8 @@
 // loaded as 4-D TMA boxes per output image row (implicit GEMM, no im2col
 // matrix).  The split-BF16 modes pack A' = [Ah | Al | Ah
 // (| Al)], B' = [Bh | Bh | Bl (| Bl)] along K, so one BF16 GEMM accumulates
-// Ah*Bh + Al*Bh + Ah*Bl (+ Al*Bl).
+// Ah*Bh + Al*Bh + Ah*Bl (+ Al*Bl); the six-product mode splits each value
+// into three pieces (hi + lo + lo2 == x) and adds Al*Bl + Al2*Bh + Ah*Bl2.
 //
 // Chunked accumulation.  The tensor core's FP32 accumulation truncates, so
 // its error grows linearly with the number of K steps summed into one TMEM
@@ -529,7 +530,7 @@ __global__ void __launch_bounds__(NT, CTAS)
 // Gathers an operand through its separable description and writes the BF16
 // split of every element into nseg K-segments of a K-major matrix: bit s of
 // seg_mask selects the hi part (1) or the lo part (0, x - hi rounded to
-// BF16) for segment s.  Columns [nseg*K, Kp) of every row are zeroed (the
+// BF16) for segment s, bit 8 + s the third part (x - hi - lo).  Columns [nseg*K, Kp) of every row are zeroed (the
 // packed buffers live in reused scratch).
 //
 // Work unit: a 64-row x 64-k tile.  Each CTA takes a contiguous range of
@@ -544,23 +545,37 @@ __global__ void __launch_bounds__(NT, CTAS)
 constexpr int PR = 64, PKT = 64, PACK_THREADS = 256;
 
 // 8 consecutive k of row r (k < K) split and stored into every segment.
+// The pieces of x: hi = bf16(x), lo = bf16(x - hi), lo2 = bf16(x - hi - lo);
+// each difference is exact in FP32, and lo2 holds the last bits, so
+// hi + lo + lo2 == x for normal x.  Segment s takes lo2 when bit 8 + s of
+// seg_mask is set, else hi (bit s set) or lo.
 __device__ __forceinline__ void pack_store8(const LtbPackJob& J, int64_t r, int64_t k,
                                             const float (&x)[8]) {
-  uint32_t hi[4], lo[4];
+  uint32_t hi[4], lo[4], lo2[4];
+  const bool third = (J.seg_mask >> 8) != 0;
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * e], x[2 * e + 1]);
     const float2 hf = __bfloat1622float2(h);
-    const __nv_bfloat162 l = __floats2bfloat162_rn(x[2 * e] - hf.x, x[2 * e + 1] - hf.y);
+    const float r0 = x[2 * e] - hf.x, r1 = x[2 * e + 1] - hf.y;
+    const __nv_bfloat162 l = __floats2bfloat162_rn(r0, r1);
     hi[e] = *reinterpret_cast<const uint32_t*>(&h);
     lo[e] = *reinterpret_cast<const uint32_t*>(&l);
+    if (third) {
+      const float2 lf = __bfloat1622float2(l);
+      const __nv_bfloat162 l2 = __floats2bfloat162_rn(r0 - lf.x, r1 - lf.y);
+      lo2[e] = *reinterpret_cast<const uint32_t*>(&l2);
+    } else {
+      lo2[e] = 0;
+    }
   }
   __nv_bfloat16* out = static_cast<__nv_bfloat16*>(J.out);
   const int nv = J.K - k < 8 ? (int)(J.K - k) : 8;
   const uint4 H = make_uint4(hi[0], hi[1], hi[2], hi[3]);
   const uint4 L = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  const uint4 L2 = make_uint4(lo2[0], lo2[1], lo2[2], lo2[3]);
   for (int s = 0; s < J.nseg; ++s) {
-    const uint4 v = (J.seg_mask >> s) & 1 ? H : L;
+    const uint4 v = (J.seg_mask >> (8 + s)) & 1 ? L2 : (J.seg_mask >> s) & 1 ? H : L;
     const int64_t off = r * J.Kp + s * J.K + k;
     if (nv == 8 && (off & 7) == 0) {
       *reinterpret_cast<uint4*>(out + off) = v;

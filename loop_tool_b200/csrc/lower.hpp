@@ -27,7 +27,7 @@ enum class Family : int {
 };
 const char* family_name(Family f);
 
-enum class Precision : int { fp32 = 0, bf16 = 1, bf16x3 = 2, bf16x4 = 3 };
+enum class Precision : int { fp32 = 0, bf16 = 1, bf16x3 = 2, bf16x4 = 3, bf16x6 = 4 };
 
 struct BufferInfo {
   int slot = -1;

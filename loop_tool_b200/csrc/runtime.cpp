@@ -53,6 +53,7 @@ ltb::LowerOptions parse_options(const char* s) {
       else if (v == "bf16") o.precision = ltb::Precision::bf16;
       else if (v == "bf16x3") o.precision = ltb::Precision::bf16x3;
       else if (v == "bf16x4") o.precision = ltb::Precision::bf16x4;
+      else if (v == "bf16x6") o.precision = ltb::Precision::bf16x6;
       else throw ltb::Error("unknown precision '" + v + "'");
     } else if (k == "fuse_rows") {
       o.fuse_rows = v != "0";
@@ -406,11 +407,18 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
       con.M < (1LL << 31) && con.N < (1LL << 31)) {
     t.tc = true;
     // split-BF16 along K: bit s of a mask selects hi (1) or lo (0) for
-    // segment s.  bf16x3: A' = [Ah|Al|Ah], B' = [Bh|Bh|Bl] (Al*Bl dropped);
-    // bf16x4 adds Al*Bl: A' = [Ah|Al|Ah|Al], B' = [Bh|Bh|Bl|Bl].
+    // segment s, bit 8 + s the third piece lo2.  bf16x3: A' = [Ah|Al|Ah],
+    // B' = [Bh|Bh|Bl] (Al*Bl dropped); bf16x4 adds Al*Bl: A' = [Ah|Al|Ah|Al],
+    // B' = [Bh|Bh|Bl|Bl]; bf16x6 (three pieces, FP32's whole significand):
+    // A' = [Ah|Al|Ah|Al|Al2|Ah], B' = [Bh|Bh|Bl|Bl|Bh|Bl2].
     switch (c->opt.precision) {
       case ltb::Precision::bf16x3: t.nseg = 3; t.a_mask = 0x5; t.b_mask = 0x3; break;
       case ltb::Precision::bf16x4: t.nseg = 4; t.a_mask = 0x5; t.b_mask = 0x3; break;
+      case ltb::Precision::bf16x6:
+        t.nseg = 6;
+        t.a_mask = 0x25 | (0x10 << 8);
+        t.b_mask = 0x13 | (0x20 << 8);
+        break;
       default: t.nseg = 1; t.a_mask = 0x1; t.b_mask = 0x1; break;
     }
     t.Kp = (t.nseg * con.K + 7) / 8 * 8;
@@ -434,7 +442,10 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     e.tiles_m = tm;
     e.unit_cols = t.unit_cols ? 1 : 0;
     ImageGeom ig;
-    if (t.nbatch == 1 && t.Kp == t.nseg * con.K && detect_image(d, A, md, kd, ig)) {
+    // (the image repack writes hi and lo images only: three-piece splits
+    // take the gathered packing)
+    if (t.nbatch == 1 && t.Kp == t.nseg * con.K && (t.a_mask >> 8) == 0 &&
+        detect_image(d, A, md, kd, ig)) {
       // implicit GEMM: A' never materialises; the A slot holds the padded
       // NHWC image(s), hi (+ lo for split modes)
       t.img = true;

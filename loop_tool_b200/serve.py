@@ -91,6 +91,47 @@ def _program(kind, params):
     return e / e.sum(n)
 
 
+# Shape buckets (the reference keys its compile cache by exact sizes,
+# lazy.h:82-115, so every new size is a new compile): a bucketed server
+# compiles one loop tree per bucket and runs each request in it, its inputs
+# zero-padded into the bucket's layout and its output read back at the
+# request's own size.  Zero padding only adds exact zeros to sums (and
+# computes rows / columns / images that are dropped), so values stay within
+# the contraction's tolerance.  Ladder: multiples of 16, about 1.25x apart.
+LADDER = sorted({16 * round(16 * 1.25 ** i / 16) for i in range(0, 40)
+                 if 16 * 1.25 ** i <= 1 << 15} | {1, 2, 4, 8})
+
+
+def _bucket(x):
+    for b in LADDER:
+        if b >= x:
+            return b
+    return x
+
+
+def bucket_params(kind, params):
+    """The bucket a request runs in: matmul M, K, N and softmax rows up the
+    ladder, convolution batch to the next power of two."""
+    if kind == "matmul":
+        return tuple(_bucket(v) for v in params)
+    if kind == "conv":
+        (b,) = params
+        return (1 << (b - 1).bit_length(),)
+    (rows,) = params
+    return (_bucket(rows),)
+
+
+def work_of(kind, params):
+    """FLOP (contractions) or bytes (softmax) of a request, for the padding
+    overhead of buckets."""
+    if kind == "matmul":
+        M, K, N = params
+        return 2.0 * M * K * N
+    if kind == "conv":
+        return 2.0 * params[0] * 128 * 56 * 56 * 64 * 9
+    return 8.0 * params[0] * 4096
+
+
 _ALIGN = 64  # floats (256 bytes) between the regions of a slot workspace
 
 
@@ -108,7 +149,7 @@ class Server:
     workspaces of idle slots when the sum would pass the budget."""
 
     def __init__(self, slots=8, hbm_budget=16 << 30, precision="bf16x3", device=0,
-                 keep_outputs=False):
+                 keep_outputs=False, buckets=False):
         import torch
 
         self.torch = torch
@@ -124,15 +165,23 @@ class Server:
         self.keep = keep_outputs
         self._kernels = {}
         self.compiles = 0
+        self.compile_s = 0.0
+        self.buckets = buckets
+
+    def _shape(self, req):
+        return bucket_params(req.kind, req.params) if self.buckets else req.params
 
     def _compiled(self, req):
         """The request's compiled loop tree from the server's own kernel
-        cache: one entry per distinct program and sizes, never evicted (a
-        trace of 20,000 requests holds ~14,000 distinct programs)."""
-        key = (req.kind, req.params)
+        cache: one entry per distinct program and sizes (or per bucket),
+        never evicted (a trace of 20,000 requests holds ~14,000 distinct
+        programs, ~1,800 buckets)."""
+        key = (req.kind, self._shape(req))
         c = self._kernels.get(key)
         if c is None:
-            c = Compiled(_program(req.kind, req.params).ir, precision=self.precision)
+            t0 = time.perf_counter()
+            c = Compiled(_program(req.kind, key[1]).ir, precision=self.precision)
+            self.compile_s += time.perf_counter() - t0
             self._kernels[key] = c
             self.compiles += 1
         return c
@@ -187,18 +236,41 @@ class Server:
             gen.manual_seed(req.seed)
             views = [ws[a:a + n] for a, n in zip(offs, sizes)]
             for i, x in enumerate(views[:c.n_inputs]):
-                torch.randn(x.numel(), generator=gen, device=self.dev, out=x)
+                dst = self._true_view(req, x, i)
+                if dst is not x:
+                    x.zero_()  # bucket padding
+                v = torch.randn(dst.numel(), generator=gen, device=self.dev).view(dst.shape)
                 if req.kind == "matmul":
-                    x /= math.sqrt(req.params[1])  # N(0,1)/sqrt(K)
+                    v /= math.sqrt(req.params[1])  # N(0,1)/sqrt(K)
                 elif req.kind == "conv" and i == 1:
-                    x *= math.sqrt(6.0 / 576) / math.sqrt(3.0)  # Kaiming-uniform scale
+                    v *= math.sqrt(6.0 / 576) / math.sqrt(3.0)  # Kaiming-uniform scale
                 elif req.kind == "softmax":
-                    x *= 4.0
+                    v *= 4.0
+                dst.copy_(v)
             c.run(views, sync=False, stream=st.cuda_stream,
                   scratch=ws[o:].data_ptr() if sb else None)
             ev = self.events[slot]
             ev.record(st)
-        req.event, req.hold, req.admitted = ev, views[-1], now
+        req.event, req.hold, req.admitted = ev, self._true_view(req, views[-1], -1), now
+
+    def _true_view(self, req, buf, i):
+        """The request's own part of one of its (possibly bucket-padded)
+        buffers: input i, or the output for i = -1."""
+        if not self.buckets:
+            return buf
+        p, q = req.params, self._shape(req)
+        if p == q:
+            return buf
+        if req.kind == "matmul":
+            (M, K, N), (Mp, Kp, Np) = p, q
+            shape, want = {0: ((Mp, Kp), (M, K)), 1: ((Kp, Np), (K, N)),
+                           -1: ((Mp, Np), (M, N))}[i]
+            return buf.view(shape)[:want[0], :want[1]]
+        if req.kind == "conv":
+            if i == 1:  # weights: no batch dim
+                return buf
+            return buf.view(q[0], -1)[:p[0]]
+        return buf.view(q[0], 4096)[:p[0]]
 
     def bytes_of(self, req):
         c = self._compiled(req)
@@ -226,7 +298,7 @@ class Server:
                 if r.event.query():
                     r.done = time.perf_counter() - t0
                     if self.keep:
-                        r.out = r.hold.cpu().numpy()
+                        r.out = r.hold.cpu().numpy().ravel()
                     r.hold = None
                     self.used -= r.bytes
                     self.free.append(slot)
@@ -257,6 +329,7 @@ class Server:
             "mean_ms": float(lat.mean() * 1e3),
             "span_s": span,
             "compiles": self.compiles,
+            "compile_s": self.compile_s,
             "peak_inflight": self.peak_inflight,
             "peak_bytes": self.peak_used,
             "slots": len(self.streams),
@@ -264,10 +337,16 @@ class Server:
         }, done
 
 
-def run_alone(req, precision="bf16x3", device=0):
+def padding_overhead(trace):
+    """Work of the trace run in its buckets over its own work."""
+    own = sum(work_of(r.kind, r.params) for r in trace)
+    return sum(work_of(r.kind, bucket_params(r.kind, r.params)) for r in trace) / own
+
+
+def run_alone(req, precision="bf16x3", device=0, buckets=False):
     """One request by itself on a fresh stream: the reference point for
     "same result alone and in the mix"."""
-    s = Server(slots=1, precision=precision, device=device, keep_outputs=True)
+    s = Server(slots=1, precision=precision, device=device, keep_outputs=True, buckets=buckets)
     r = Request(req.rid, req.kind, req.params, 0.0, req.seed)
     s.serve([r])
     return r.out

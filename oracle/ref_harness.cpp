@@ -32,6 +32,15 @@
 //       Annotates the first loop at <depth> of <program>'s loop tree with
 //       <annotation> through the reference's own annotate()
 //       (mutate.cpp:694-712) and prints serialize() of the result.
+//   lt_ref_harness lazytime <reps> <program> <params...>
+//       Times the reference lazy frontend itself on <program>: leaves are
+//       filled with seeded uniform values, one untimed T.data() compiles and
+//       runs, then <reps> times force_recompute() + data() (lazy.h:219-260:
+//       a fresh output allocation on the default hardware, Compiled::run
+//       with sync, the result readable on the host) with the first and last
+//       output element read on the host; prints {"seconds": [...]} (steady
+//       clock, per call).  With LT_PLUGIN the default backend and hardware
+//       are the plugin's "cuda".
 //   lt_ref_harness tree <ir_file>      LoopTree::dump of the IR
 //   lt_ref_harness code <ir_file>      the C the "cpp" backend generates
 //   lt_ref_harness sizes <ir_file>     element counts of every I/O buffer
@@ -45,6 +54,7 @@
 #include <cstdio>
 #include <fstream>
 #include <thread>
+#include <unordered_set>
 #include <iostream>
 #include <sstream>
 #include <string>
@@ -357,6 +367,42 @@ int main(int argc, char** argv) {
       std::ofstream f(out_dir + "/out0.f32", std::ios::binary);
       f.write(reinterpret_cast<const char*>(out),
               tsizes[tir.inputs().size()] * sizeof(float));
+      return 0;
+    }
+    if (mode == "lazytime") {
+      const int reps = std::stoi(argv[2]);
+      std::vector<int64_t> params;
+      for (int i = 4; i < argc; ++i) params.emplace_back(std::stoll(argv[i]));
+      auto T = build(argv[3], params);
+      auto tir = T.ir();
+      loop_tool::LoopTree tlt(tir);
+      loop_tool::Compiler tc(tlt);
+      auto tsizes = tc.memory_sizes(true);
+      std::unordered_set<const loop_tool::lazy::TensorImpl*> seen;
+      auto leaves = T.impl()->getInputBuffers(seen);
+      uint64_t st = 0x9E3779B97F4A7C15ull;  // xorshift64: seeded uniform [-1, 1)
+      for (size_t i = 0; i < leaves.size(); ++i) {
+        float* f = static_cast<float*>(leaves[i]);
+        for (int64_t e = 0; e < tsizes[i]; ++e) {
+          st ^= st << 13;
+          st ^= st >> 7;
+          st ^= st << 17;
+          f[e] = (float)((int64_t)(st >> 40) - (1 << 23)) * (1.0f / (1 << 23));
+        }
+      }
+      const int64_t nout = tsizes[tir.inputs().size()];
+      volatile float sink = T.data<float>()[0];
+      std::cout << "{\"seconds\": [";
+      for (int r = 0; r < reps; ++r) {
+        auto t0 = std::chrono::steady_clock::now();
+        T.force_recompute();
+        const float* out = T.data<float>();
+        sink = out[0] + out[nout - 1];
+        auto t1 = std::chrono::steady_clock::now();
+        std::cout << (r ? ", " : "") << std::chrono::duration<double>(t1 - t0).count();
+      }
+      (void)sink;
+      std::cout << "]}\n";
       return 0;
     }
     if (mode == "annotate") {

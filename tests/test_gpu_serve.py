@@ -66,3 +66,33 @@ def test_reserved_workspaces_serve_without_growth(cuda_dev):
     by_id = {r.rid: r.out for r in base}
     for r in done:
         assert same(r.out, by_id[r.rid]), f"request {r.rid} differs"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x3", "fp32"])
+def test_bucketed_server(precision, cuda_dev):
+    """Shape-bucketed keys: fewer compiled programs than distinct shapes;
+    each result equals the same request alone in the same bucket (bit for
+    bit) and the exact-size server's result (bit for bit in FP32, whose sums
+    only gain trailing zero terms; within the split-BF16 tolerance, whose
+    K segments shift with the padded K)."""
+    from loop_tool_b200.serve import Server, bucket_params, run_alone
+
+    trace = small_trace(30, seed=14)
+    exact = Server(slots=4, precision=precision, keep_outputs=True)
+    _, base = exact.serve(small_trace(30, seed=14))
+    srv = Server(slots=6, precision=precision, keep_outputs=True, buckets=True)
+    stats, done = srv.serve(trace)
+    assert stats["requests"] == len(trace)
+    assert srv.compiles == len({(r.kind, bucket_params(r.kind, r.params)) for r in trace})
+    assert srv.compiles < exact.compiles
+    by_id = {r.rid: r.out for r in base}
+    for r in done:
+        alone = run_alone(r, precision=precision, buckets=True)
+        assert same(r.out, alone), f"request {r.rid} differs alone vs mix"
+        ref = by_id[r.rid]
+        if precision == "fp32":
+            assert np.array_equal(r.out, ref), f"request {r.rid} ({r.kind} {r.params})"
+        else:
+            d = np.linalg.norm(r.out.astype(np.float64) - ref) / np.linalg.norm(ref)
+            assert d <= 2e-5, f"request {r.rid} ({r.kind} {r.params}): {d:.3g}"
