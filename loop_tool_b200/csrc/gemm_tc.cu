@@ -18,7 +18,8 @@
 // Chunked accumulation.  The tensor core's FP32 accumulation truncates, so
 // its error grows linearly with the number of K steps summed into one TMEM
 // accumulator (measured: ~1.9e-5 relative at K = 16384 with BF16-exact
-// inputs).  The K loop is therefore cut into chunks of 512 elements, each
+// inputs).  The K loop is therefore cut into chunks (512 elements, fewer
+// for the six-product split mode: LtbTcProblem::chunk_blocks), each
 // accumulated from zero in one of two TMEM buffers; drain warps read a
 // finished chunk back (16 columns per tcgen05.ld) and add it into FP32
 // registers with round-to-nearest adds while the tensor core fills the other
@@ -52,7 +53,7 @@ namespace {
 
 constexpr int BM = 128, BK = 64;
 constexpr int NT = 320;
-constexpr int kChunkBlocks = 8;  // 8 x 64 = 512 K elements per accumulator
+constexpr int kChunkBlocks = 8;  // default: 8 x 64 = 512 K elements per accumulator
 constexpr int A_BYTES = BM * BK * 2;
 // epilogue: each drain warp transposes 32 x 32 blocks through a padded
 // shared buffer so global stores are whole 128-byte row segments
@@ -399,7 +400,8 @@ __global__ void __launch_bounds__(NT, CTAS)
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const int nk = (int)((p.Kp + BK - 1) / BK);
-      for (int c0 = 0; c0 < nk && alive; c0 += kChunkBlocks, ++q) {
+      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
+      for (int c0 = 0; c0 < nk && alive; c0 += cbk, ++q) {
         const int buf = q & 1;
         if (!mbar_wait(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
           alive = false;
@@ -407,7 +409,7 @@ __global__ void __launch_bounds__(NT, CTAS)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t acc = tmem + (uint32_t)(buf * BN);
-        const int c1 = c0 + kChunkBlocks < nk ? c0 + kChunkBlocks : nk;
+        const int c1 = c0 + cbk < nk ? c0 + cbk : nk;
         for (int kb = c0; kb < c1; ++kb, ++g) {
           const int s = g % STAGES;
           if (!mbar_wait(smem_u32(&full[s]), (g / STAGES) & 1u, err)) {
@@ -444,7 +446,8 @@ __global__ void __launch_bounds__(NT, CTAS)
       float run[T::HALF];
 #pragma unroll
       for (int i = 0; i < T::HALF; ++i) run[i] = 0.f;
-      for (int c0 = 0; c0 < nk; c0 += kChunkBlocks, ++q) {
+      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
+      for (int c0 = 0; c0 < nk; c0 += cbk, ++q) {
         const int buf = q & 1;
         const bool ok = mbar_wait(smem_u32(&chunk_full[buf]), (q >> 1) & 1u, err);
         if (!__all_sync(0xffffffffu, ok)) {

@@ -441,6 +441,10 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     e.N = (int)con.N;
     e.tiles_m = tm;
     e.unit_cols = t.unit_cols ? 1 : 0;
+    // the six-product mode drains every 2 k blocks (128 K): its pieces
+    // carry FP32's whole significand, so the accumulation's truncation is
+    // what is left to bound
+    e.chunk_blocks = t.nseg >= 6 ? 2 : 0;
     ImageGeom ig;
     // (the image repack writes hi and lo images only: three-piece splits
     // take the gathered packing)

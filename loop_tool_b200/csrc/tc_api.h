@@ -39,7 +39,11 @@ struct LtbTcProblem {
   int img_halo;
   int img_stages;        // halo ring depth
   int img_slot_bytes;    // bytes per halo ring slot (1024-aligned)
-  int img_pad_;
+  // 64-wide k blocks accumulated into one TMEM buffer before the drain
+  // warps add it into FP32 registers (0: 8).  The tensor core's FP32
+  // accumulation truncates, so its error grows with the MMA steps of a
+  // chunk: the FP32-accurate split modes drain shorter chunks.
+  int chunk_blocks;
 };
 
 // Repacks an image operand x(n, c, h + off_h, w + off_w) (FP32 at

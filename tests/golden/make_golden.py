@@ -64,6 +64,9 @@ CASES = [
     ("colsum_300x37", "colsum", [300, 37], 222, "randn"),
     ("colmax_specials", "colmax", [300, 37], 223, "specials"),
     ("fullsum_2x40000", "fullsum", [2, 40000], 224, "randn"),
+    # compensated row sums (rows above 65536) meeting inf, -inf, inf + -inf
+    # and overflow: the plain sequential loop's inf / -inf / NaN
+    ("rowsum_specials_5x70000", "rowsum", [5, 70000], 234, "sum_specials"),
     ("softmax_16x32", "softmax", [16, 32], 225, "softmax"),
     ("softmax_16x4096", "softmax", [16, 4096], 226, "softmax"),
     ("mean_rows_4x8", "mean_rows", [4, 8], 227, "ones_last"),
@@ -100,6 +103,14 @@ def make_inputs(kind, sizes, seed):
             a = rng.standard_normal(n)
         elif kind == "abs":
             a = np.abs(rng.standard_normal(n))
+        elif kind == "sum_specials":  # rows: +inf, -inf, both, overflow, plain
+            a = rng.standard_normal(n).reshape(5, -1)
+            a[0, 1234] = np.inf
+            a[1, 40000] = -np.inf
+            a[2, 10] = np.inf
+            a[2, 69000] = -np.inf
+            a[3, :] = 3e38
+            a = a.ravel()
         elif kind == "log":  # positive values, plus log's special arguments
             a = np.abs(rng.standard_normal(n)) * 10.0 ** rng.integers(-30, 30, n)
             a[:6] = [0.0, -0.0, 1.0, np.inf, -1.0, np.nan]

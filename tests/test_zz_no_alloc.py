@@ -5,15 +5,19 @@ serving loop with its HBM budget already committed, a host framework that
 owns all device allocations): the split-K partials live in a static device
 array instead of a compiled object's scratch.  Checked through the C ABI
 against the existing entry point (ltb_compile + ltb_run on the same row-sum
-loop tree), on two calls in a row.  This file is collected last so that a
-run stopping at the first failure has already run every other test.
+loop tree) and against FP64, on two calls in a row: each row's error
+against the FP64 sum is within 1e-5 of that row's value or no larger than
+the existing entry point's own error there (the parity bar of the golden
+tests), and rows that meet inf, -inf, both, or overflow give exactly the
+reference's inf / -inf / NaN.  This file is collected last so that a run
+stopping at the first failure has already run every other test.
 """
 import ctypes
 
 import numpy as np
 import pytest
 
-RTOL = 1e-5
+from golden_util import assert_accuracy, bits_equal, load
 
 
 def rowsum_ir(rows, cols):
@@ -36,19 +40,47 @@ def test_no_alloc_matches_existing_entry_point(rows, cols, cuda_dev):
     ref = torch.empty(rows, device=cuda_dev)
     lt.cuda(rowsum_ir(rows, cols))([x, ref])
     torch.cuda.synchronize()
+    existing = ref.cpu().numpy()
+    exact = x.view(rows, cols).double().sum(1).cpu().numpy()  # FP64, the oracle
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    expected = ref.cpu().numpy().astype(np.float64)
-    scale = float(np.sqrt(np.mean(expected ** 2)))
     for call in range(2):
         out = torch.full((rows,), float("nan"), device=cuda_dev)
         rc = _lib.lib().ltb_row_sum_noalloc(ctypes.c_void_p(x.data_ptr()), rows, cols,
                                             ctypes.c_void_p(out.data_ptr()), stream)
         assert rc == 0, _lib.lib().ltb_last_error().decode()
         torch.cuda.synchronize()
-        got = out.cpu().numpy().astype(np.float64)
-        err = np.abs(got - expected)
-        assert (err <= RTOL * (np.abs(expected) + scale)).all(), \
-            f"call {call}: max error {err.max():.3g} (scale {scale:.3g})"
+        assert_accuracy(out.cpu().numpy(), existing, exact, what=f"call {call}")
+
+
+@pytest.mark.gpu
+def test_no_alloc_non_finite_rows(cuda_dev):
+    """Rows holding +inf, -inf, both, or summing past FLT_MAX: inf, -inf,
+    NaN and inf as the reference's sequential loop gives them (golden
+    fixture rowsum_specials_5x70000), from the scratch-free entry point and
+    from ltb_run, on two calls in a row."""
+    import torch
+
+    import loop_tool_b200 as lt
+    from loop_tool_b200 import _lib
+
+    case = load("rowsum_specials_5x70000")
+    x = torch.from_numpy(case["inputs"][0]).to(cuda_dev)
+    expected = case["expected"]
+    ref = torch.empty(5, device=cuda_dev)
+    lt.cuda(case["ir"])([x, ref])
+    torch.cuda.synchronize()
+    assert bits_equal(ref.cpu().numpy()[:4], expected[:4])
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for call in range(2):
+        out = torch.full((5,), 7.0, device=cuda_dev)
+        rc = _lib.lib().ltb_row_sum_noalloc(ctypes.c_void_p(x.data_ptr()), 5, 70000,
+                                            ctypes.c_void_p(out.data_ptr()), stream)
+        assert rc == 0, _lib.lib().ltb_last_error().decode()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert bits_equal(got[:4], expected[:4]), f"call {call}: {got[:4]}"
+        exact = case["inputs"][0].reshape(5, -1)[4].astype(np.float64).sum()
+        assert_accuracy(got[4:], ref.cpu().numpy()[4:], np.array([exact]), what=f"call {call}")
 
 
 @pytest.mark.gpu
