@@ -778,7 +778,7 @@ def extra_c5(dev, n_requests, rates):
 
 
 # ------------------------------------------------------- profiling cases
-NCU_CASES = ("add", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "mm_fp32", "conv_bf16",
+NCU_CASES = ("add", "add_2p28", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "mm_fp32", "conv_bf16",
              "conv_fp32", "batch_bf16", "mm_bf16_batch")
 
 
@@ -802,6 +802,8 @@ def ncu_case(name, reps, tune=True, schedules=None):
     opts = {}
     if name in ("add", "softmax", "maxpool"):
         ir = {n.split("_")[0]: t for n, t, _ in nests(add_log2=26)}[name]
+    elif name == "add_2p28":  # the headline's add at its own size (3.2 GB per launch)
+        ir = reference_ir("add_2p28")
     elif name == "mm_bf16_batch":  # 8192^3 through the grouped (batch) launch path
         n = 8192
         c = ltb.Compiled(mm_ir(n, n, n), precision="bf16")

@@ -266,8 +266,11 @@ __global__ void __launch_bounds__(NT, CTAS)
 
   if (kHalo && warp == 0 && lane == 0) {
     // ------------------------------------------------- producer (halo tiles)
+    // one box per (tile, channel block): the tile's img_rows image rows and
+    // the kh - 1 halo rows below them, every padded column; all kh x kw
+    // shifts of the tile are read from it in place
     const LtbTcProblem& p = single;
-    const uint32_t box_bytes = (uint32_t)(p.img_rows * p.img_slot * 128);
+    const uint32_t box_bytes = (uint32_t)((p.img_rows + p.img_kh - 1) * p.img_slot * 128);
     bool first = true;  // the first tile also loads the resident B' blocks, in first-use order
     uint32_t g = 0;  // stages issued
     bool alive = true;
@@ -276,25 +279,25 @@ __global__ void __launch_bounds__(NT, CTAS)
       tile_coords<BN>(p, t, &m0, &n0);
       const int mt = m0 / BM, n_img = mt / p.img_hgroups;
       const int ho0 = (mt - n_img * p.img_hgroups) * p.img_rows;
-      for (int kh = 0; kh < p.img_kh && alive; ++kh)
-        for (int cb = 0; cb < p.img_cblocks; ++cb, ++g) {
-          const int s = (int)(g % (uint32_t)nst);
-          if (!mbar_wait(smem_u32(&empty[s]), ((g / (uint32_t)nst) & 1u) ^ 1u, err)) {
-            alive = false;
-            break;
-          }
-          if (first)
+      for (int cb = 0; cb < p.img_cblocks; ++cb, ++g) {
+        const int s = (int)(g % (uint32_t)nst);
+        if (!mbar_wait(smem_u32(&empty[s]), ((g / (uint32_t)nst) & 1u) ^ 1u, err)) {
+          alive = false;
+          break;
+        }
+        if (first)
+          for (int kh = 0; kh < p.img_kh; ++kh)
             for (int kw = 0; kw < p.img_kw; ++kw) {
               const int kb = (kh * p.img_kw + kw) * p.img_cblocks + cb;
               const uint32_t bb = smem_u32(&b_full[kb]);
               mbar_expect_tx(bb, (uint32_t)T::B_BYTES);
               tma_load_2d(smem_u32(bres + (size_t)kb * T::B_BYTES), &single_b, bb, kb * BK, 0);
             }
-          const uint32_t fb = smem_u32(&full[s]);
-          mbar_expect_tx(fb, box_bytes);
-          tma_load_4d(smem_u32(ring + (size_t)s * slot_bytes), &single_a, fb, cb * 64, 0,
-                      ho0 + kh, n_img);
-        }
+        const uint32_t fb = smem_u32(&full[s]);
+        mbar_expect_tx(fb, box_bytes);
+        tma_load_4d(smem_u32(ring + (size_t)s * slot_bytes), &single_a, fb, cb * 64, 0, ho0,
+                    n_img);
+      }
       first = false;
     }
   } else if (kHalo && warp == 1 && lane == 0) {
@@ -307,15 +310,15 @@ __global__ void __launch_bounds__(NT, CTAS)
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       int issued = 0, buf = 0;
       uint32_t acc = tmem;
-      for (int kh = 0; kh < p.img_kh && alive; ++kh)
-        for (int cb = 0; cb < p.img_cblocks && alive; ++cb, ++g) {
-          const int s = (int)(g % (uint32_t)nst);
-          if (!mbar_wait(smem_u32(&full[s]), (g / (uint32_t)nst) & 1u, err)) {
-            alive = false;
-            break;
-          }
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t a_slot = smem_u32(ring + (size_t)s * slot_bytes);
+      for (int cb = 0; cb < p.img_cblocks && alive; ++cb, ++g) {
+        const int s = (int)(g % (uint32_t)nst);
+        if (!mbar_wait(smem_u32(&full[s]), (g / (uint32_t)nst) & 1u, err)) {
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a_slot = smem_u32(ring + (size_t)s * slot_bytes);
+        for (int kh = 0; kh < p.img_kh && alive; ++kh)
           for (int kw = 0; kw < p.img_kw; ++kw) {
             if (issued % kChunkBlocks == 0) {  // a new accumulation chunk
               buf = (int)(q & 1u);
@@ -331,7 +334,9 @@ __global__ void __launch_bounds__(NT, CTAS)
               alive = false;
               break;
             }
-            const uint64_t ad = sw128_desc(a_slot + (uint32_t)kw * 128u);
+            // shift (kh, kw): tile row i * wp + w reads box row
+            // (i + kh) * wp + (w + kw)
+            const uint64_t ad = sw128_desc(a_slot + (uint32_t)(kh * p.img_slot + kw) * 128u);
             const uint64_t bd = sw128_desc(smem_u32(bres + (size_t)kb * T::B_BYTES));
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk)
@@ -343,8 +348,8 @@ __global__ void __launch_bounds__(NT, CTAS)
               ++q;
             }
           }
-          mma_commit(smem_u32(&empty[s]));  // slot reusable once these finish
-        }
+        mma_commit(smem_u32(&empty[s]));  // slot reusable once these finish
+      }
       first = false;
     }
   } else if (!kHalo && warp == 0 && lane == 0) {
@@ -965,8 +970,8 @@ cudaError_t ltb_make_tmap_image(void* map, const void* base, int n, int hp, int 
 
 bool ltb_tc_halo_geometry(LtbTcProblem& p, int wp) {
   if (!p.img || p.N > 128 || p.Kp % BK || wp > 128 || p.Kp / BK > kMaxHaloKb) return false;
-  // a kw-shifted operand reads halo rows kw .. kw + 127
-  const int slot_bytes = ((127 + p.img_kw) * 128 + 1023) / 1024 * 1024;
+  // the (kh, kw)-shifted operand reads box rows kh * wp + kw .. + 127
+  const int slot_bytes = (((p.img_kh - 1) * wp + 127 + p.img_kw) * 128 + 1023) / 1024 * 1024;
   const size_t fixed = (size_t)(p.Kp / BK) * kHaloBBytes + 1024 + kHaloBarBytes;
   if (fixed + 2 * (size_t)slot_bytes > kHaloSmemMax) return false;
   int stages = (int)((kHaloSmemMax - fixed) / slot_bytes);

@@ -739,9 +739,9 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           j.lo = t.img_kinds == 2 ? static_cast<char*>(ap) + t.img_elems * 2 : nullptr;
           e = ltb_launch_pack_conv(j, p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig,
                                    t.b_off32, st);
-          if (e == cudaSuccess && t.epi == 3)  // halo boxes: img_rows padded rows, full width
+          if (e == cudaSuccess && t.epi == 3)  // halo boxes: the tile's rows + kh - 1, full width
             e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.halo.img_slot,
-                                    t.halo.img_rows);
+                                    t.halo.img_rows + t.halo.img_kh - 1);
           else if (e == cudaSuccess)
             e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.prob.img_wo);
           if (e == cudaSuccess)
