@@ -547,6 +547,14 @@ struct Builder {
     if (p.parallel_red > 256 && s.ps.family == Family::reduce_parallel &&
         (d.red_op == LTB_R_ADD || d.red_op == LTB_R_MUL))
       s.ps.family = Family::reduce_split;
+    // Sums: a sequential fold (reduce_serial) is the reference's own
+    // order, bit for bit; a tree or split-K sum reassociates, so it is
+    // compensated (TwoSum partials, error ~2u|sum|): plain trees have errors
+    // of the reference's size in other places, which entry by entry exceed
+    // the reference's on some cancelling sums.
+    if (d.red_op == LTB_R_ADD &&
+        (s.ps.family == Family::reduce_parallel || s.ps.family == Family::reduce_split))
+      d.kahan = 1;
     if (s.ps.family == Family::contraction && p.any()) {
       notes << " parallel/unroll on a contraction: the tile kernel keeps its own mapping;";
       p.parallel_out = p.parallel_red = 0;
@@ -794,6 +802,13 @@ struct Builder {
         plan.row_groups.push_back(grp);
         for (int k : grp) {
           st[k].family = Family::row_chain;
+          // fused row chains compensate only long rows
+          if (st[k].dev.red_op == LTB_R_ADD && st[k].dev.red_total <= opt.kahan_threshold &&
+              st[k].dev.kahan) {
+            st[k].dev.kahan = 0;
+            const size_t at = st[k].text.find("(kahan)");
+            if (at != std::string::npos) st[k].text.erase(at, 7);
+          }
           if (st[k].pins.any()) {  // the fused row kernel has its own mapping
             st[k].pins = StagePins{};
             st[k].text += " (parallel/unroll not applied: fused into a row chain)";

@@ -414,15 +414,10 @@ __global__ void k_reduce_combine(const LtbStage* __restrict__ gst,
     const float* part = bt.p[S.partial_buf] + o * splits;
     float acc = S.red_init, c = 0.f;
     for (int s = 0; s < splits; ++s) {
-      if (S.red_op == LTB_R_ADD) {
-        const float y = part[s] - c;
-        const float t = acc + y;
-        c = (t - acc) - y;
-        acc = t;
-      } else {
-        acc = fold(S.red_op, acc, part[s]);
-      }
+      if (S.red_op == LTB_R_ADD) comp_add(acc, c, part[s]);
+      else acc = fold(S.red_op, acc, part[s]);
     }
+    if (S.red_op == LTB_R_ADD) acc = comp_value(acc, c);
     int64_t x[LTB_MAXD];
     set_out_coords(S, o, x);
     int64_t ob = S.out_off;
