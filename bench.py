@@ -752,6 +752,9 @@ def extra_c5(dev, n_requests, rates):
             srv.bytes_of(r)
         srv.reserve(trace0)  # slot workspaces sized before the clock starts
         warm_s = time.perf_counter() - w0
+        # untimed: the first launch of each kernel loads its module (CUDA
+        # lazy loading), which must not land in the first sweep point
+        srv.serve(make_trace(2000, rate=1e9, seed=777))
         sweep, capacity = {}, None
         for rate in rates:
             stats, _ = srv.serve(make_trace(n_requests, rate=rate, seed=501))

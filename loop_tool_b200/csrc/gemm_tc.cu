@@ -31,8 +31,9 @@
 // epilogue by per-thread row stores (32-byte sector stores where aligned) or
 // through a 32 x 32 shared-memory transpose into whole-row stores.  Halo
 // image tiles (single-segment convolutions, N <= 128): the weights stay
-// resident in shared memory and one 4-D box of whole padded image rows per
-// (kh, channel block) serves every kw shift, read in place.
+// resident in shared memory and one 4-D box per (tile, channel block) -- the
+// tile's padded image rows and the kh - 1 rows below them -- serves every
+// (kh, kw) shift, read in place.
 //
 // Roles (320 threads per CTA):
 //   warp 0 lane 0 : TMA producer                  warp 0 : TMEM alloc/free

@@ -1056,8 +1056,8 @@ std::string describe(ltb_compiled* c, int i) {
         << " row blocks) epilogue("
         << (t.epi == 1 ? "smem transpose" : t.epi == 2 ? "row stores, 2 CTAs/SM" : "row stores")
         << ")"
-        << (t.epi == 3 ? " implicit_conv(halo tiles: one 4-D TMA box per kernel row, kw shifts "
-                         "read in place; weights resident in shared memory)"
+        << (t.epi == 3 ? " implicit_conv(halo tiles: one 4-D TMA box per tile and channel block, "
+                         "every (kh, kw) shift read in place; weights resident in shared memory)"
             : t.img   ? " implicit_conv(A from NHWC image via 4-D TMA)"
                       : "");
     else {
