@@ -1148,7 +1148,6 @@ void record_schedule(ltb_compiled* c, const std::vector<double>& us) {
   g_tune[c->key] = std::move(e);
 }
 
-// Schedules from the cache, if this IR + options were tuned before.
 // ---------------------------------------------------- schedule as IR text
 // The launch schedule of the grid-stride and tree-reduction stages written
 // back into the loop tree as the reference's own vocabulary: the stage's
@@ -1290,6 +1289,7 @@ std::string schedule_ir(ltb_compiled* c) {
   return out;
 }
 
+// Schedules from the cache, if this IR + options were tuned before.
 void lookup_schedule(ltb_compiled* c) {
   c->key = fnv1a(c->ir_text, canon_options(c->opt));
   std::lock_guard<std::mutex> g(g_tune_mu);
