@@ -396,7 +396,8 @@ def headline(args, world, rank, dev):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "bandwidth nests: add 2^28, softmax 8192x4096, maxpool "
-                               "64x128x112x112 (FP32 lazy-frontend loop trees)",
+                               "64x128x112x112 (FP32 loop trees emitted by the reference's lazy "
+                               "frontend)",
                    "l2": "two buffer sets per nest used in turn (each set's inputs and "
                          "outputs exceed L2, 126 MB): no launch finds its data in L2",
                    "issue": "each step's three independent nests on three streams; per-nest "
