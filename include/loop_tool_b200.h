@@ -266,6 +266,56 @@ int ltb_synchronize(void* stream);
 int ltb_check_bounded_wait(int64_t limit_cycles, void* stream, int* completed,
                            int* drained);
 
+/* ------------------------------------------------------------- serving
+ * A native continuous-batching request loop.  The reference has none: its
+ * lazy frontend runs one program at a time, synchronously, allocating each
+ * output (include/loop_tool/lazy.h:249-258).  The server keeps one CUDA
+ * stream ("slot") per concurrent request and one device workspace per slot
+ * (inputs, output and run scratch of its request, grown stream-ordered only
+ * when a request needs more), admits requests in arrival order while a slot
+ * is free and their bytes (ltb_io_sizes + scratch_bytes) fit the HBM budget,
+ * compiles each distinct loop tree once (kernel cache keyed by IR text),
+ * generates each request's inputs on the device from its seed, and runs it
+ * with caller scratch (ltb_run_with_scratch), so concurrent requests share
+ * nothing.  Latency is arrival to completion (the slot's event), on the
+ * host's steady clock. */
+#define LTB_SERVE_MAX_IO 8
+typedef struct {
+  int64_t rows, cols;           /* the buffer: rows x cols floats, row-major */
+  int64_t true_rows, true_cols; /* the request's own top-left block; the rest
+                                   is shape-bucket padding, zero in inputs */
+  float scale;                  /* inputs: seeded N(0, 1) values times scale */
+} ltb_block;
+typedef struct {
+  const char* ir_text;          /* the request's loop tree (serialize text) */
+  double arrival_s;             /* arrival time from the start of the trace */
+  uint64_t seed;                /* seed of its inputs */
+  int n_io;                     /* inputs + outputs of the loop tree */
+  ltb_block io[LTB_SERVE_MAX_IO];
+  float* host_out;              /* NULL, or host memory receiving the first
+                                   output's true block when the request ends */
+} ltb_request;
+typedef struct {
+  int64_t requests, compiles, peak_inflight, peak_bytes;
+  double span_s, req_per_s, p50_ms, p99_ms, mean_ms, compile_s;
+} ltb_serve_stats;
+typedef struct ltb_server ltb_server;
+/* slots >= 1 concurrent requests, hbm_budget bytes of request buffers at
+ * once, options as for ltb_compile (e.g. "precision=bf16x3"). */
+int ltb_server_create(int slots, int64_t hbm_budget, const char* options, ltb_server** out);
+/* Compiles every distinct loop tree of reqs[0..n) and sizes every slot's
+ * workspace for the largest request (within the budget), so that serving
+ * them compiles and allocates nothing; *reserved_bytes (optional) = the
+ * workspace bytes held. */
+int ltb_server_prepare(ltb_server* s, const ltb_request* reqs, int n, int64_t* reserved_bytes);
+/* Serves reqs[0..n) against the wall clock (arrival times scaled by
+ * time_scale); latency_s (optional) receives each request's latency, in
+ * request order.  A request larger than the budget is an error
+ * (LTB_ERR_INVALID) before anything runs. */
+int ltb_server_serve(ltb_server* s, const ltb_request* reqs, int n, double time_scale,
+                     ltb_serve_stats* stats, double* latency_s);
+int ltb_server_release(ltb_server* s);
+
 #ifdef __cplusplus
 }
 #endif

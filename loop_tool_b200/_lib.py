@@ -17,6 +17,30 @@ ERR_CUDA = 3
 ERR_NO_DEVICE = 4
 ERR_TIMEOUT = 5
 
+# The serving structures of include/loop_tool_b200.h ("serving").
+LTB_SERVE_MAX_IO = 8
+
+
+class LtbBlock(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_int64), ("cols", ctypes.c_int64),
+                ("true_rows", ctypes.c_int64), ("true_cols", ctypes.c_int64),
+                ("scale", ctypes.c_float)]
+
+
+class LtbRequest(ctypes.Structure):
+    _fields_ = [("ir_text", ctypes.c_char_p), ("arrival_s", ctypes.c_double),
+                ("seed", ctypes.c_uint64), ("n_io", ctypes.c_int),
+                ("io", LtbBlock * LTB_SERVE_MAX_IO), ("host_out", ctypes.POINTER(ctypes.c_float))]
+
+
+class LtbServeStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_int64), ("compiles", ctypes.c_int64),
+                ("peak_inflight", ctypes.c_int64), ("peak_bytes", ctypes.c_int64),
+                ("span_s", ctypes.c_double), ("req_per_s", ctypes.c_double),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("compile_s", ctypes.c_double)]
+
+
 # every symbol include/loop_tool_b200.h declares, with its ctypes signature
 SIGNATURES = {
     "ltb_abi_version": (ctypes.c_int, []),
@@ -76,6 +100,14 @@ SIGNATURES = {
     "ltb_tune_load": (ctypes.c_int, [ctypes.c_char_p]),
     "ltb_tune_clear": (ctypes.c_int, []),
     "ltb_tune_entries": (ctypes.c_int64, []),
+    "ltb_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_char_p,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "ltb_server_prepare": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LtbRequest), ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int64)]),
+    "ltb_server_serve": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LtbRequest), ctypes.c_int,
+                                        ctypes.c_double, ctypes.POINTER(LtbServeStats),
+                                        ctypes.POINTER(ctypes.c_double)]),
+    "ltb_server_release": (ctypes.c_int, [ctypes.c_void_p]),
 }
 
 

@@ -337,6 +337,107 @@ class Server:
         }, done
 
 
+_IR_TEXT = {}  # (kind, shape) -> IR bytes, built once per distinct program
+
+
+def _ir_bytes(kind, shape):
+    key = (kind, shape)
+    t = _IR_TEXT.get(key)
+    if t is None:
+        t = _IR_TEXT[key] = _program(kind, shape).ir.encode()
+    return t
+
+
+def _blocks(kind, params, shape):
+    """(rows, cols, true_rows, true_cols, scale) of each buffer of a request
+    whose program runs at `shape` (its bucket, or its own sizes): inputs
+    first, then the output; the true block holds the request's own data."""
+    if kind == "matmul":
+        (M, K, N), (Mp, Kp, Np) = params, shape
+        return [(Mp, Kp, M, K, 1.0 / math.sqrt(K)), (Kp, Np, K, N, 1.0), (Mp, Np, M, N, 0.0)]
+    if kind == "conv":
+        (b,), (bp,) = params, shape
+        img, out = 64 * 56 * 56, 56 * 56 * 128
+        return [(bp, img, b, img, 1.0), (128, 64 * 9, 128, 64 * 9, math.sqrt(6.0 / 576) / math.sqrt(3.0)),
+                (bp, out, b, out, 0.0)]
+    (rows,), (rp,) = params, shape
+    return [(rp, 4096, rows, 4096, 4.0), (rp, 4096, rows, 4096, 0.0)]
+
+
+class NativeServer:
+    """The same request loop in C++ (ltb_server_*, csrc/serve.cpp): slots
+    as streams, HBM budget admission, a kernel cache per distinct loop tree,
+    inputs generated on the device from each request's seed (zero-padded
+    into its bucket's layout when `buckets`), per-slot workspaces.  The
+    Python side only describes the trace; no Python runs per request."""
+
+    def __init__(self, slots=8, hbm_budget=16 << 30, precision="bf16x3", buckets=False):
+        import ctypes
+
+        from . import _lib
+
+        self._c, self._L = ctypes, _lib
+        self.buckets = buckets
+        self.precision = precision
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().ltb_server_create(int(slots), int(hbm_budget),
+                                                f"precision={precision}".encode(),
+                                                ctypes.byref(h)))
+        self._h = h
+        self.slots = slots
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and self._L._lib is not None:
+            self._L.lib().ltb_server_release(h)
+            self._h = None
+
+    def _requests(self, trace, keep_outputs=False):
+        c, L = self._c, self._L
+        arr = (L.LtbRequest * len(trace))()
+        outs = []
+        for i, r in enumerate(trace):
+            shape = bucket_params(r.kind, r.params) if self.buckets else r.params
+            q = arr[i]
+            q.ir_text = _ir_bytes(r.kind, shape)
+            q.arrival_s = r.arrival
+            q.seed = r.seed
+            bl = _blocks(r.kind, r.params, shape)
+            q.n_io = len(bl)
+            for j, (R, C, tr, tc, sc) in enumerate(bl):
+                q.io[j] = L.LtbBlock(R, C, tr, tc, sc)
+            if keep_outputs:
+                R, C, tr, tc, _ = bl[-1]
+                o = np.empty(tr * tc, np.float32)
+                outs.append(o)
+                q.host_out = o.ctypes.data_as(c.POINTER(c.c_float))
+            else:
+                outs.append(None)
+        return arr, outs
+
+    def prepare(self, trace):
+        """Compile every distinct program of the trace and size the slot
+        workspaces for its largest request; returns the bytes reserved."""
+        arr, _ = self._requests(trace)
+        got = self._c.c_int64()
+        self._L.check(self._L.lib().ltb_server_prepare(self._h, arr, len(trace),
+                                                       self._c.byref(got)))
+        return got.value
+
+    def serve(self, trace, time_scale=1.0, keep_outputs=False):
+        """Serve the trace against the wall clock; returns (stats, outputs),
+        outputs[i] the true output of trace[i] when keep_outputs."""
+        c, L = self._c, self._L
+        arr, outs = self._requests(trace, keep_outputs)
+        st = L.LtbServeStats()
+        lat = (c.c_double * len(trace))()
+        L.check(L.lib().ltb_server_serve(self._h, arr, len(trace), float(time_scale),
+                                         c.byref(st), lat))
+        stats = {k: getattr(st, k) for k, _ in L.LtbServeStats._fields_}
+        stats.update(slots=self.slots, precision=self.precision, buckets=self.buckets)
+        return stats, outs
+
+
 def padding_overhead(trace):
     """Work of the trace run in its buckets over its own work."""
     own = sum(work_of(r.kind, r.params) for r in trace)

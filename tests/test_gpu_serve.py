@@ -96,3 +96,45 @@ def test_bucketed_server(precision, cuda_dev):
         else:
             d = np.linalg.norm(r.out.astype(np.float64) - ref) / np.linalg.norm(ref)
             assert d <= 2e-5, f"request {r.rid} ({r.kind} {r.params}): {d:.3g}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x3", "fp32"])
+def test_native_server_mix_equals_alone(precision, cuda_dev):
+    """The C++ request loop (ltb_server_*): every result in the concurrent
+    mix equals the same request served alone, bit for bit; requests
+    overlapped; softmax rows sum to one."""
+    from loop_tool_b200.serve import NativeServer
+
+    trace = small_trace(30, seed=21)
+    srv = NativeServer(slots=6, precision=precision)
+    srv.prepare(trace)
+    stats, outs = srv.serve(trace, keep_outputs=True)
+    assert stats["requests"] == len(trace) and stats["peak_inflight"] > 1
+    alone = NativeServer(slots=1, precision=precision)
+    for r, o in zip(trace, outs):
+        _, (a,) = alone.serve([r], keep_outputs=True)
+        assert same(o, a), f"request {r.rid} ({r.kind} {r.params}) differs alone vs mix"
+        assert np.isfinite(o).all()
+        if r.kind == "softmax":
+            assert np.abs(o.reshape(-1, 4096).astype(np.float64).sum(1) - 1).max() < 1e-5
+
+
+@pytest.mark.gpu
+def test_native_server_budget_and_buckets(cuda_dev):
+    """Admission keeps the bytes in flight within the budget; a bucketed
+    native server compiles fewer programs and, in FP32, gives the exact-key
+    server's results bit for bit (inputs are seeded per element of the true
+    block, so padding does not change them)."""
+    from loop_tool_b200.serve import NativeServer, bucket_params
+
+    trace = small_trace(24, seed=22)
+    exact = NativeServer(slots=4, precision="fp32")
+    _, base = exact.serve(trace, keep_outputs=True)
+    need = max(4 * sum(r.params[0] * 4096 for r in trace if r.kind == "softmax"), 1)
+    srv = NativeServer(slots=8, hbm_budget=64 << 20, precision="fp32", buckets=True)
+    stats, outs = srv.serve(trace, keep_outputs=True)
+    assert stats["peak_bytes"] <= 64 << 20 and need > 0
+    assert stats["compiles"] == len({(r.kind, bucket_params(r.kind, r.params)) for r in trace})
+    for r, o, b in zip(trace, outs, base):
+        assert np.array_equal(o, b), f"request {r.rid} ({r.kind} {r.params})"
