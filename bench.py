@@ -727,17 +727,22 @@ P99_BOUND_MS = 20.0  # capacity = the highest served rate with p99 under this
 
 
 def extra_c5(dev, n_requests, rates):
-    """Serving the seeded trace.  Warm: each server compiles the trace's
+    """Serving the seeded trace with the native request loop (ltb_server_*,
+    C++: no Python per request).  Warm: each server compiles the trace's
     distinct programs (or buckets) once, untimed, reserves its slot
-    workspaces, then serves the trace at every offered rate of the sweep.
-    Cold: a fresh server serves the trace at one rate with its kernel cache
-    empty (every first use of a program compiles inside that request's
-    latency), exact-size keys and shape buckets."""
-    from loop_tool_b200.serve import Server, make_trace, padding_overhead
+    workspaces and serves an untimed warm-up trace (first launches load
+    kernel modules), then serves the trace at every offered rate of the
+    sweep.  Cold: a fresh server serves the trace at one rate with its
+    kernel cache empty (every first use of a program compiles inside that
+    request's latency), exact-size keys and shape buckets.  One arm of the
+    Python loop (serve.Server) at one rate shows the host loop's share."""
+    from loop_tool_b200.serve import NativeServer, Server, make_trace, padding_overhead
 
     trace0 = make_trace(n_requests, rate=1e9, seed=501)
+    warmup = make_trace(2000, rate=1e9, seed=777)
     out = {"workload": f"{n_requests} requests, Poisson arrivals, 50% matmul (c4 shapes), "
                        f"30% conv (batch U[1,64]), 20% softmax (rows U[1,8192] x 4096)",
+           "loop": "native (C++ ltb_server): admission, slots, kernel cache, device-side inputs",
            "workspaces": "reserved per slot before serving",
            "distinct_programs": len({(r.kind, r.params) for r in trace0}),
            "bucket_padding_work_ratio": padding_overhead(trace0),
@@ -747,15 +752,11 @@ def extra_c5(dev, n_requests, rates):
                ("plain_fp32_1slot", dict(slots=1, precision="fp32"))]
     keys = ("req_per_s", "p50_ms", "p99_ms", "mean_ms", "peak_inflight", "compiles", "compile_s")
     for name, kw in configs:
-        srv = Server(hbm_budget=24 << 30, **kw)
+        srv = NativeServer(hbm_budget=24 << 30, **kw)
         w0 = time.perf_counter()
-        for r in trace0:  # populate the kernel cache (one compile per program / bucket)
-            srv.bytes_of(r)
-        srv.reserve(trace0)  # slot workspaces sized before the clock starts
+        srv.prepare(trace0)  # every program compiled, workspaces sized, before the clock
         warm_s = time.perf_counter() - w0
-        # untimed: the first launch of each kernel loads its module (CUDA
-        # lazy loading), which must not land in the first sweep point
-        srv.serve(make_trace(2000, rate=1e9, seed=777))
+        srv.serve(warmup)
         sweep, capacity = {}, None
         for rate in rates:
             stats, _ = srv.serve(make_trace(n_requests, rate=rate, seed=501))
@@ -763,21 +764,27 @@ def extra_c5(dev, n_requests, rates):
             if stats["req_per_s"] >= 0.95 * rate and stats["p99_ms"] <= P99_BOUND_MS:
                 capacity = max(capacity or 0, rate)
         out[name] = {"kernel_cache": "warm", "warm_compile_s": warm_s,
-                     "compiled_programs": srv.compiles, "sweep": sweep,
+                     "compiled_programs": stats["compiles"], "sweep": sweep,
                      "capacity_req_per_s": capacity,
                      "saturation_req_per_s": max(v["req_per_s"] for v in sweep.values())}
         del srv
-        import torch
-
-        torch.cuda.empty_cache()
     cold_rate = 4000.0
     for name, kw in configs[:2]:
-        srv = Server(hbm_budget=24 << 30, **kw)
-        srv.reserve(trace0[:1])
+        srv = NativeServer(hbm_budget=24 << 30, **kw)
         stats, _ = srv.serve(make_trace(n_requests, rate=cold_rate, seed=501))
         out[name + "_cold"] = dict({k: stats[k] for k in keys}, offered_req_per_s=cold_rate,
                                    kernel_cache="cold (compiles inside latency)")
         del srv
+    # the Python request loop, same configuration, warm, at the native arm's
+    # saturation point (offered 16k req/s)
+    py = Server(slots=8, hbm_budget=24 << 30, precision="bf16x3")
+    for r in trace0:
+        py.bytes_of(r)
+    py.reserve(trace0)
+    py.serve(make_trace(2000, rate=1e9, seed=777))
+    stats, _ = py.serve(make_trace(n_requests, rate=16000.0, seed=501))
+    out["python_loop_bf16x3_8slots_rate_16000"] = {k: stats[k] for k in keys}
+    del py
     return out
 
 
