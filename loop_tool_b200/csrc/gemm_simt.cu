@@ -7,8 +7,7 @@
 // order of separately rounded FP32 multiplies and adds, whatever the tile
 // loader's form: the arithmetic of the reference's C path (cpp.cpp:467-471
 // compiles with cc -std=c99, which does not contract a*b+c into an FMA), so
-// plain FP32 contractions match the reference bit for bit.  The multiplies
-// and adds run as paired FP32 instructions (two output columns each).
+// plain FP32 contractions match the reference bit for bit.
 //
 // CTA tile 128 x 128, 16 k per step, 256 threads with 8 x 8 outputs each
 // (rows ty*4 + {0..3} and 64 + ty*4 + {0..3}, likewise columns); both
@@ -32,26 +31,6 @@
 #include "kernels.h"
 
 namespace {
-
-// Paired FP32 arithmetic (sm_100: two lanes per instruction, each lane
-// rounded exactly as the scalar mul.rn / add.rn): an output pair (j, j + 1)
-// of one row accumulates acc = acc + a * (b_j, b_j+1) in one multiply and
-// one add instruction, the reference's separately rounded multiply-add.
-typedef unsigned long long f32x2;
-__device__ __forceinline__ f32x2 pack2(float x, float y) {
-  f32x2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
-  return r;
-}
-__device__ __forceinline__ void unpack2(f32x2 v, float& x, float& y) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
-}
-__device__ __forceinline__ f32x2 madd2(f32x2 acc, f32x2 a, f32x2 b) {
-  f32x2 p, d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(p) : "l"(a), "l"(b));
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(acc), "l"(p));
-  return d;
-}
 
 constexpr int BM = 128, BK = 16, NT = 256, LDS = BM + 4;
 constexpr int kHoistG = 4;  // guards whose row partials are kept in registers
@@ -265,11 +244,11 @@ __device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, i
     __syncthreads();
     la.kt = kta;
   }
-  f32x2 acc2[8][4];  // output pairs (columns 2j, 2j + 1 of this thread's 8)
+  float acc[8][8];
 #pragma unroll
   for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc2[a][b] = pack2(0.f, 0.f);
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.f;
 
   const int nk = (int)((p.K + BK - 1) / BK);  // K <= kSimtMaxK (checked at launch)
   constexpr bool async = Loader<AM>::kAsync || Loader<BMODE>::kAsync;
@@ -292,14 +271,11 @@ __device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, i
       const float4 b0 = *reinterpret_cast<const float4*>(&tb.s[cur][kk][tx * 4]);
       const float4 b1 = *reinterpret_cast<const float4*>(&tb.s[cur][kk][64 + tx * 4]);
       const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const f32x2 bv[4] = {pack2(b0.x, b0.y), pack2(b0.z, b0.w), pack2(b1.x, b1.y),
-                           pack2(b1.z, b1.w)};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-      for (int a = 0; a < 8; ++a) {
-        const f32x2 aa = pack2(av[a], av[a]);
+      for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc2[a][b] = madd2(acc2[a][b], aa, bv[b]);
-      }
+        for (int b = 0; b < 8; ++b) acc[a][b] = __fadd_rn(acc[a][b], __fmul_rn(av[a], bv[b]));
     }
     if (t + 1 < nk) {
       la.stash(ta.s[cur ^ 1]);
@@ -309,11 +285,6 @@ __device__ __forceinline__ void gemm_tile(const LtbGemmProblem& p, int64_t i0, i
     __syncthreads();
   }
 
-  float acc[8][8];
-#pragma unroll
-  for (int a = 0; a < 8; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) unpack2(acc2[a][b], acc[a][2 * b], acc[a][2 * b + 1]);
   // epilogue: 16-byte stores where four neighbouring columns are adjacent
   // and aligned in the output, scalar stores otherwise
   int64_t c0[2];
@@ -430,11 +401,11 @@ __global__ void __launch_bounds__(NT) k_gemm_simt_mid(LtbGemmProblem p) {
   const int64_t i0 = (int64_t)blockIdx.y * MBM, j0 = (int64_t)blockIdx.x * MBM;
   const bool akf = p.a.dense && p.a.ld_k == 1, bkf = p.b.dense && p.b.ld_k == 1;
   MidLoader la, lb;
-  f32x2 acc2[4][2];  // output pairs (columns 2j, 2j + 1 of this thread's 4)
+  float acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 2; ++b) acc2[a][b] = pack2(0.f, 0.f);
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
   const int nk = (int)((p.K + BK - 1) / BK);  // K <= kSimtMaxK (checked at launch)
   la.fetch(p.a, i0, p.M, p.K, 0, akf);
   lb.fetch(p.b, j0, p.N, p.K, 0, bkf);
@@ -452,13 +423,11 @@ __global__ void __launch_bounds__(NT) k_gemm_simt_mid(LtbGemmProblem p) {
       const float4 a4 = *reinterpret_cast<const float4*>(&sa[cur][kk][ty * 4]);
       const float4 b4 = *reinterpret_cast<const float4*>(&sb[cur][kk][tx * 4]);
       const float av[4] = {a4.x, a4.y, a4.z, a4.w};
-      const f32x2 bv[2] = {pack2(b4.x, b4.y), pack2(b4.z, b4.w)};
+      const float bv[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const f32x2 aa = pack2(av[a], av[a]);
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 2; ++b) acc2[a][b] = madd2(acc2[a][b], aa, bv[b]);
-      }
+        for (int b = 0; b < 4; ++b) acc[a][b] = __fadd_rn(acc[a][b], __fmul_rn(av[a], bv[b]));
     }
     if (t + 1 < nk) {
       la.stash(sa[cur ^ 1], akf);
@@ -466,11 +435,6 @@ __global__ void __launch_bounds__(NT) k_gemm_simt_mid(LtbGemmProblem p) {
     }
     __syncthreads();
   }
-  float acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b) unpack2(acc2[a][b], acc[a][2 * b], acc[a][2 * b + 1]);
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const int64_t i = i0 + ty * 4 + a;
