@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(NT, CTAS)
               float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
               const __grid_constant__ CUtensorMap single_a,
               const __grid_constant__ CUtensorMap single_b,
-              const __grid_constant__ CUtensorMap single_a2) {
+              const __grid_constant__ CUtensorMap single_a2,
+              const __grid_constant__ CUtensorMap single_a3) {
   // probs == nullptr: one problem passed by value with its tensor maps as
   // kernel parameters (encoded at launch over per-run scratch)
   using T = Tile<BN, CTAS>;
@@ -365,6 +366,8 @@ __global__ void __launch_bounds__(NT, CTAS)
           probs ? static_cast<const CUtensorMap*>(p.map_b) : &single_b;
       const CUtensorMap* ma2 =
           probs ? static_cast<const CUtensorMap*>(p.map_a2) : &single_a2;
+      const CUtensorMap* ma3 =
+          probs ? static_cast<const CUtensorMap*>(p.map_a3) : &single_a3;
       int m0, n0;
       tile_coords<BN>(p, t - p.tile_start, &m0, &n0);
       const int nk = (int)((p.Kp + BK - 1) / BK);
@@ -387,7 +390,9 @@ __global__ void __launch_bounds__(NT, CTAS)
           const int seg = kb / kseg, r = kb - seg * kseg;
           const int cb = r % p.img_cblocks, r2 = r / p.img_cblocks;
           const int kw = r2 % p.img_kw, kh = r2 / p.img_kw;
-          const CUtensorMap* m = (p.img_a_mask >> seg) & 1 ? ma : ma2;
+          const CUtensorMap* m = (p.img_a_mask >> (8 + seg)) & 1 ? ma3
+                                 : (p.img_a_mask >> seg) & 1    ? ma
+                                                                : ma2;
           mbar_expect_tx(fb, (uint32_t)(p.img_rows * p.img_wo * 128 + T::B_BYTES));
           for (int i = 0; i < p.img_rows; ++i)
             tma_load_4d(smem_u32(sa + i * p.img_slot * 128), m, fb, cb * 64, kw, ho0 + i + kh,
@@ -539,8 +544,9 @@ __global__ void __launch_bounds__(NT, CTAS)
 // Gathers an operand through its separable description and writes the BF16
 // split of every element into nseg K-segments of a K-major matrix: bit s of
 // seg_mask selects the hi part (1) or the lo part (0, x - hi rounded to
-// BF16) for segment s, bit 8 + s the third part (x - hi - lo).  Columns [nseg*K, Kp) of every row are zeroed (the
-// packed buffers live in reused scratch).
+// BF16) for segment s, bit 8 + s the third part (x - hi - lo).  Columns
+// [nseg*K, Kp) of every row are zeroed (the packed buffers live in reused
+// scratch).
 //
 // Work unit: a 64-row x 64-k tile.  Each CTA takes a contiguous range of
 // tiles (one job search per CTA, sequential addresses).  Four load modes:
@@ -849,7 +855,8 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
 
 // Image operand repack: one CTA per (channel block of 64, padded row, image)
 // reads the 64 channel rows of x (coalesced along w) into shared memory and
-// writes the padded row [wp, 64] of BF16 channel pairs (coalesced along c).
+// writes the padded row [wp, 64] of BF16 channel pairs (coalesced along c)
+// into the hi image, and into the lo and lo2 images when the job has them.
 // The reads of a 160-column chunk are all issued before any is stored, so
 // each thread has up to 40 loads in flight.
 constexpr int kImgChunkJ = 5;  // 32-column slices per chunk
@@ -885,17 +892,24 @@ __device__ __forceinline__ void pack_image_row(const LtbImageJob& J, int cb, int
   // warp per padded column, lanes over channel pairs (coalesced 128-byte rows)
   __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(J.hi) +
                       (((int64_t)n * J.hp + h) * J.wp) * J.c + cb * 64 + 2 * lane;
-  __nv_bfloat16* lo = J.lo ? static_cast<__nv_bfloat16*>(J.lo) +
-                                 (((int64_t)n * J.hp + h) * J.wp) * J.c + cb * 64 + 2 * lane
-                           : nullptr;
+  const int64_t at = (((int64_t)n * J.hp + h) * J.wp) * J.c + cb * 64 + 2 * lane;
+  __nv_bfloat16* lo = J.lo ? static_cast<__nv_bfloat16*>(J.lo) + at : nullptr;
+  __nv_bfloat16* lo2 = J.lo && J.lo2 ? static_cast<__nv_bfloat16*>(J.lo2) + at : nullptr;
   for (int w = warp; w < J.wp; w += 8) {
     const float x0 = tile[2 * lane * pitch + w], x1 = tile[(2 * lane + 1) * pitch + w];
     const __nv_bfloat162 hv = __floats2bfloat162_rn(x0, x1);
     *reinterpret_cast<__nv_bfloat162*>(hi + (int64_t)w * J.c) = hv;
     if (lo) {
+      // the pieces of pack_store8: both differences are exact in FP32
       const float2 hf = __bfloat1622float2(hv);
-      *reinterpret_cast<__nv_bfloat162*>(lo + (int64_t)w * J.c) =
-          __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+      const float r0 = x0 - hf.x, r1 = x1 - hf.y;
+      const __nv_bfloat162 lv = __floats2bfloat162_rn(r0, r1);
+      *reinterpret_cast<__nv_bfloat162*>(lo + (int64_t)w * J.c) = lv;
+      if (lo2) {
+        const float2 lf = __bfloat1622float2(lv);
+        *reinterpret_cast<__nv_bfloat162*>(lo2 + (int64_t)w * J.c) =
+            __floats2bfloat162_rn(r0 - lf.x, r1 - lf.y);
+      }
     }
   }
 }
@@ -1089,7 +1103,7 @@ template <int BN, bool TE, int CTAS = 1, bool HALO = false>
 static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b,
-                             const void* map_a2) {
+                             const void* map_a2, const void* map_a3) {
   size_t smem = Tile<BN, CTAS>::SMEM;
   if (HALO) {
     if (d_probs || !single || !single->img_halo) return cudaErrorInvalidValue;
@@ -1104,27 +1118,28 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
   const int64_t slots = (int64_t)sms * CTAS;
   const int grid = (int)(total_tiles < slots ? total_tiles : slots);
   LtbTcProblem one{};
-  CUtensorMap ma{}, mb{}, ma2{};
+  CUtensorMap ma{}, mb{}, ma2{}, ma3{};
   if (!d_probs) {
     if (!single || !map_a || !map_b) return cudaErrorInvalidValue;
     one = *single;
     ma = *static_cast<const CUtensorMap*>(map_a);
     mb = *static_cast<const CUtensorMap*>(map_b);
     ma2 = map_a2 ? *static_cast<const CUtensorMap*>(map_a2) : ma;
+    ma3 = map_a3 ? *static_cast<const CUtensorMap*>(map_a3) : ma2;
   }
   k_gemm_tc<BN, TE, CTAS, HALO><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override,
-                                                        err, one, ma, mb, ma2);
+                                                        err, one, ma, mb, ma2, ma3);
   return cudaGetLastError();
 }
 
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single, const void* map_a,
-                               const void* map_b, const void* map_a2) {
+                               const void* map_b, const void* map_a2, const void* map_a3) {
   if (total_tiles == 0) return cudaSuccess;
 #define LTB_TC(BN, TE)                                                                      \
   return launch_tc<BN, TE>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a, \
-                           map_b, map_a2)
+                           map_b, map_a2, map_a3)
   switch (bn) {
     case 128: LTB_TC(128, false);
     case 129: LTB_TC(128, true);
@@ -1132,10 +1147,10 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
     case 257: LTB_TC(256, true);
     case 130:  // 128 wide, two CTAs per SM
       return launch_tc<128, false, 2>(d_probs, nprob, total_tiles, c_override, sms, err, st,
-                                      single, map_a, map_b, map_a2);
+                                      single, map_a, map_b, map_a2, map_a3);
     case 131:  // 128 wide halo image tiles, resident weights
       return launch_tc<128, false, 1, true>(d_probs, nprob, total_tiles, c_override, sms, err,
-                                            st, single, map_a, map_b, map_a2);
+                                            st, single, map_a, map_b, map_a2, map_a3);
   }
 #undef LTB_TC
   return cudaErrorInvalidValue;

@@ -91,9 +91,9 @@ struct GemmTables {
   // implicit-GEMM convolution: A packed as NHWC BF16 image(s) read by 4-D
   // TMA boxes (LtbTcProblem::img); B's K order permuted to (kh, kw, c)
   bool img = false;
-  int img_kinds = 1;                  // images in the A slot: hi (+ lo)
+  int img_kinds = 1;                  // images in the A slot: hi (+ lo (+ lo2))
   int64_t img_elems = 0;              // elements of one image
-  LtbImageJob ijob{};                 // base / hi / lo bound at launch
+  LtbImageJob ijob{};                 // base / hi / lo / lo2 bound at launch
   int bn = 256;                       // tensor-core tile width (128 or 256)
   int epi = 0;                        // 1: shared-memory transposed epilogue,
                                       // 2: two CTAs per SM, 3: halo image tiles
@@ -111,6 +111,18 @@ void set_tile_n(GemmTables& t, int bn, int epi) {
   const int64_t tn = (t.prob.N + bn - 1) / bn;
   t.prob.tiles_n = (int)tn;
   t.tiles = epi == 3 ? (int64_t)t.halo.tiles_m : (int64_t)t.prob.tiles_m * tn;
+}
+
+// The image repack job of a run: the operand's buffer and the A slot, which
+// holds the hi image, then the lo and lo2 images when the split has them.
+LtbImageJob image_job(const GemmTables& t, const float* base, void* a_slot) {
+  LtbImageJob j = t.ijob;
+  j.base = base;
+  j.hi = a_slot;
+  char* const at = static_cast<char*>(a_slot);
+  j.lo = t.img_kinds >= 2 ? at + t.img_elems * 2 : nullptr;
+  j.lo2 = t.img_kinds == 3 ? at + t.img_elems * 4 : nullptr;
+  return j;
 }
 
 // All of a compiled object's constant device data (stage descriptors,
@@ -446,15 +458,12 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     // what is left to bound
     e.chunk_blocks = t.nseg >= 6 ? 2 : 0;
     ImageGeom ig;
-    // (the image repack writes hi and lo images only: three-piece splits
-    // take the gathered packing)
-    if (t.nbatch == 1 && t.Kp == t.nseg * con.K && (t.a_mask >> 8) == 0 &&
-        detect_image(d, A, md, kd, ig)) {
+    if (t.nbatch == 1 && t.Kp == t.nseg * con.K && detect_image(d, A, md, kd, ig)) {
       // implicit GEMM: A' never materialises; the A slot holds the padded
-      // NHWC image(s), hi (+ lo for split modes)
+      // NHWC image(s), hi (+ lo for split modes, + lo2 for three-piece ones)
       t.img = true;
       const int segs = (1 << t.nseg) - 1;
-      t.img_kinds = (~t.a_mask & segs) ? 2 : 1;
+      t.img_kinds = ((t.a_mask >> 8) & segs) ? 3 : (~t.a_mask & segs) ? 2 : 1;
       const int64_t hp = ig.ho + ig.kh - 1, wp = ig.wo + ig.kw - 1;
       t.img_elems = ig.nimg * hp * wp * ig.c;
       P.scratch_elems[t.a_slot - (P.n_in + P.n_out)] = (t.img_kinds * t.img_elems + 1) / 2;
@@ -731,12 +740,9 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         }
         void* ap = bt.p[t.a_slot];
         void* bp = bt.p[t.b_slot];
-        alignas(64) unsigned char maps[384];  // A (hi image), B, A lo image
+        alignas(64) unsigned char maps[512];  // A (hi image), B, A lo image, A lo2 image
         if (t.img) {
-          LtbImageJob j = t.ijob;
-          j.base = p.a.base;
-          j.hi = ap;
-          j.lo = t.img_kinds == 2 ? static_cast<char*>(ap) + t.img_elems * 2 : nullptr;
+          LtbImageJob j = image_job(t, p.a.base, ap);
           e = ltb_launch_pack_conv(j, p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig,
                                    t.b_off32, st);
           if (e == cudaSuccess && t.epi == 3)  // halo boxes: the tile's rows + kh - 1, full width
@@ -747,6 +753,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           if (e == cudaSuccess)
             e = ltb_make_tmap_image(maps + 256, j.lo ? j.lo : j.hi, j.nimg, j.hp, j.wp, j.c,
                                     t.prob.img_wo);
+          if (e == cudaSuccess && j.lo2)
+            e = ltb_make_tmap_image(maps + 384, j.lo2, j.nimg, j.hp, j.wp, j.c, t.prob.img_wo);
         } else {
           e = ltb_launch_pack(p.a, p.M, p.K, ap, t.Kp, t.nseg, t.a_mask, t.a_kcontig, t.a_off32,
                               c->sms, st);
@@ -764,7 +772,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           one.ccol = t.c_col;
           e = ltb_launch_gemm_tc(t.bn | t.epi, nullptr, 1, t.tiles, nullptr, c->sms,
                                  timeout_flag(c->device, st), st,
-                                 &one, maps, maps + 128, t.img ? maps + 256 : nullptr);
+                                 &one, maps, maps + 128, t.img ? maps + 256 : nullptr,
+                                 t.img_kinds == 3 ? maps + 384 : nullptr);
         }
       }
       break;
@@ -1457,17 +1466,16 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         job(p.b, p.N, bp, t.b_mask, t.b_kcontig, t.b_off32);
         const int grp = group_of(t);
         auto& mv = maps[grp];
-        mv.resize(mv.size() + 384);  // A (hi image), B, A lo image
-        unsigned char* m = mv.data() + mv.size() - 384;
+        mv.resize(mv.size() + 512);  // A (hi image), B, A lo image, A lo2 image
+        unsigned char* m = mv.data() + mv.size() - 512;
         if (t.img) {
-          LtbImageJob j = t.ijob;
-          j.base = p.a.base;
-          j.hi = ap;
-          j.lo = t.img_kinds == 2 ? static_cast<char*>(ap) + t.img_elems * 2 : nullptr;
+          const LtbImageJob j = image_job(t, p.a.base, ap);
           b->img_jobs.push_back(j);
           CUDA_TRY(ltb_make_tmap_image(m, j.hi, j.nimg, j.hp, j.wp, j.c, t.prob.img_wo));
           CUDA_TRY(ltb_make_tmap_image(m + 256, j.lo ? j.lo : j.hi, j.nimg, j.hp, j.wp, j.c,
                                        t.prob.img_wo));
+          CUDA_TRY(ltb_make_tmap_image(m + 384, j.lo2 ? j.lo2 : j.lo ? j.lo : j.hi, j.nimg, j.hp,
+                                       j.wp, j.c, t.prob.img_wo));
         } else {
           CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
         }
@@ -1495,9 +1503,10 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         // tensor maps in device memory (cudaMalloc is 256-byte aligned)
         unsigned char* d_maps = upload(maps[g], b->owned);
         for (size_t i = 0; i < tcp[g].size(); ++i) {
-          tcp[g][i].map_a = d_maps + 384 * i;
-          tcp[g][i].map_b = d_maps + 384 * i + 128;
-          tcp[g][i].map_a2 = d_maps + 384 * i + 256;
+          tcp[g][i].map_a = d_maps + 512 * i;
+          tcp[g][i].map_b = d_maps + 512 * i + 128;
+          tcp[g][i].map_a2 = d_maps + 512 * i + 256;
+          tcp[g][i].map_a3 = d_maps + 512 * i + 384;
         }
         b->ntc[g] = (int)tcp[g].size();
         b->d_tc[g] = upload(tcp[g], b->owned);

@@ -28,8 +28,10 @@ struct LtbTcProblem {
   int img;               // 0: A' [M, Kp] dense as above
   int img_rows, img_slot, img_wo, img_ho, img_hgroups;
   int img_kh, img_kw, img_cblocks;
-  int img_a_mask;        // bit s: segment s reads the hi image (1) or lo (0)
+  int img_a_mask;        // bit s: segment s reads the hi image (1) or lo (0);
+                         // bit 8 + s: segment s reads the lo2 image
   const void* map_a2;    // image mode: CUtensorMap over the lo image
+  const void* map_a3;    // image mode: CUtensorMap over the lo2 image
   // Halo image tiles (single-segment image operands, N <= 128, single
   // launches): img_slot = the padded width wp, so tile row i * wp + w is
   // output column w of image row i; one 4-D box of img_rows padded rows per
@@ -57,7 +59,8 @@ struct LtbImageJob {
   int nimg, c, hp, wp;
   int off_h, ub_h, off_w, ub_w;
   void* hi;
-  void* lo;
+  void* lo;   // x - hi, rounded (null: hi only)
+  void* lo2;  // (x - hi) - lo, rounded (null: no third piece; needs lo)
 };
 cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st);
 // The image repack and the B' packing of the same contraction (arguments
@@ -125,5 +128,5 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single = nullptr,
                                const void* map_a = nullptr, const void* map_b = nullptr,
-                               const void* map_a2 = nullptr);
+                               const void* map_a2 = nullptr, const void* map_a3 = nullptr);
 int ltb_tc_tile_m();
