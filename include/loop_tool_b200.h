@@ -114,7 +114,9 @@ int ltb_dump(ltb_compiled* c, char* buf, size_t len);
  * computes it), plus "stages", "launches", "scratch_bytes", "inputs",
  * "outputs", "algorithmic_bytes", "flops", "tuned" (schedules from the
  * autotuner or its cache), "implicit_conv" (contractions whose A operand is
- * read as an image: convolution as implicit GEMM). */
+ * read as an image: convolution as implicit GEMM), "tma_store_output"
+ * (tensor-core contractions whose output rows are one progression of
+ * 16-byte multiples, written by TMA stores when the buffer is aligned). */
 int ltb_int_property(ltb_compiled* c, const char* name, int64_t* value);
 
 /* Element counts of the I/O buffers: elems[0..n_in+n_out). */

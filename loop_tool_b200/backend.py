@@ -150,7 +150,7 @@ class Compiled:
     @property
     def int_properties(self):
         keys = ("bandwidth", "stages", "launches", "scratch_bytes", "inputs", "outputs",
-                "algorithmic_bytes", "flops", "tuned", "implicit_conv")
+                "algorithmic_bytes", "flops", "tuned", "implicit_conv", "tma_store_output")
         return {k: self.int_property(k) for k in keys}
 
     def capture(self, memory, stream=None, scratch=None):
@@ -264,7 +264,9 @@ def tune_batch(members, capture_stream=None, reps=3):
     same way.  Returns the Batch (captured on capture_stream if given), the
     tile policy and a report."""
     policies = {"current": [c.schedule(0) for c, _ in members]}
-    for v in (128, 129, 130, 256, 257):  # tile width | form (1: transposed epilogue, 2: 2 CTAs/SM)
+    # tile width | form (1: transposed epilogue, 2: 2 CTAs/SM); 258: 256 x 256
+    # tiles on CTA pairs
+    for v in (128, 129, 130, 256, 257, 258):
         policies[f"all_{v}"] = [(0, 0, v)] * len(members)
     tuned = []
     for c, bufs in members:

@@ -19,7 +19,8 @@
 // its error grows linearly with the number of K steps summed into one TMEM
 // accumulator (measured: ~1.9e-5 relative at K = 16384 with BF16-exact
 // inputs).  The K loop is therefore cut into chunks (512 elements, fewer
-// for the six-product split mode: LtbTcProblem::chunk_blocks), each
+// for the six-product split mode, the whole K for plain BF16, whose input
+// rounding outweighs the truncation by far: LtbTcProblem::chunk_blocks), each
 // accumulated from zero in one of two TMEM buffers; drain warps read a
 // finished chunk back (16 columns per tcgen05.ld) and add it into FP32
 // registers with round-to-nearest adds while the tensor core fills the other
@@ -46,6 +47,9 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <map>
+#include <mutex>
+
 #include "async.cuh"
 #include "kernels.h"
 #include "tc_api.h"
@@ -57,9 +61,9 @@ constexpr int NT = 320;
 constexpr int kChunkBlocks = 8;  // default: 8 x 64 = 512 K elements per accumulator
 constexpr int A_BYTES = BM * BK * 2;
 // epilogue: each drain warp transposes 32 x 32 blocks through a padded
-// shared buffer so global stores are whole 128-byte row segments
+// shared buffer so global stores are whole 128-byte row segments (outputs
+// that TMA cannot store)
 constexpr int kEpiPitch = 33;
-constexpr int kEpiBytes = 8 * 32 * kEpiPitch * 4;
 
 // Tile shapes: BM x BN output tiles, BN = 256 (4-stage ring of 48 KB) or
 // BN = 128 (6-stage ring of 32 KB; narrow outputs and small problems).
@@ -98,6 +102,31 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
       " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
       : "memory");
+}
+
+// 2-D box shared -> global (the output tile's 32 x 32 FP32 blocks), in this
+// thread's bulk async-group; the parts of the box outside the tensor are
+// not written.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// this thread's bulk stores have read their shared-memory sources
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// this thread's bulk stores are complete
+__device__ __forceinline__ void bulk_wait() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+// generic-proxy shared-memory writes made visible to the TMA (async proxy)
+__device__ __forceinline__ void fence_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // Output row of tile row tr (0..127) of m-tile m0 / BM, and whether the row
@@ -192,6 +221,87 @@ __device__ __forceinline__ void tile_coords(const LtbTcProblem& p, int64_t lt, i
   *n0 = (idx / gm) * BN;
 }
 
+// Writes a drain warp's share of a finished tile: rows m0 + 32*quad .. +31
+// (row m0 + 32*quad + lane in this thread's run[]) and HALF columns from
+// cbase.  Three forms: TMA stores of 32 x 32 blocks staged 128-byte
+// swizzled in the warp's 4 KB of shared memory (kTma, outputs whose rows are
+// one progression of 16-byte multiples: LtbTcProblem::c_tma), whole-row
+// stores through a padded 32 x 32 transpose (kTE, unit columns), or each
+// thread's own row (32-byte sector stores where aligned, else float4 or
+// scalar, through the column table when columns are not unit).
+template <int HALF, bool kTma, bool kTE>
+__device__ __forceinline__ void write_tile(const LtbTcProblem& p, const CUtensorMap* mc,
+                                           float* c_override, const float (&run)[HALF],
+                                           float* epi, int ew, int m0, int cbase, bool rvalid,
+                                           int64_t rbase) {
+  const int lane = threadIdx.x & 31, quad = threadIdx.x >> 5 & 3;
+  float* cb = c_override ? c_override : p.c;
+  if (kTma && p.c_tma && !c_override) {
+    // 16-byte chunk q of row r at chunk q ^ (r % 8): conflict-free float4
+    // writes; the stores run on while the warp drains the next tile, and the
+    // buffer is rewritten once the previous store has read it
+    float* stage = epi + ew * 1024;
+    if (m0 + 32 * quad >= p.M) return;  // no row of this warp's blocks exists
+#pragma unroll
+    for (int c = 0; c < HALF; c += 32) {
+      if (cbase + c >= p.N) break;  // nor any column from here on
+      if (lane == 0) bulk_wait_read();
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        *reinterpret_cast<float4*>(stage + lane * 32 + ((q ^ (lane & 7)) << 2)) =
+            make_float4(run[c + 4 * q], run[c + 4 * q + 1], run[c + 4 * q + 2],
+                        run[c + 4 * q + 3]);
+      fence_async_shared();
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_2d(mc, smem_u32(stage), cbase + c, m0 + 32 * quad);
+        bulk_commit();
+      }
+    }
+  } else if (kTE && p.unit_cols) {
+    float* stage = epi + ew * (32 * kEpiPitch);
+    const int64_t rb = rbase;
+#pragma unroll
+    for (int c = 0; c < HALF; c += 32) {
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < 32; ++j) stage[lane * kEpiPitch + j] = run[c + j];
+      __syncwarp();
+      const int col = cbase + c + lane;
+      const bool cok = col < p.N;
+#pragma unroll 8
+      for (int i = 0; i < 32; ++i) {  // row i of the block: 32 consecutive columns
+        const int64_t rbi = __shfl_sync(0xffffffffu, rb, i);
+        const int vi = __shfl_sync(0xffffffffu, (int)rvalid, i);
+        if (vi && cok) cb[rbi + col] = stage[i * kEpiPitch + lane];
+      }
+    }
+  } else if (rvalid) {  // this thread's row: 32-byte (whole sector) stores where aligned
+    float* dst = cb + rbase;
+#pragma unroll
+    for (int c = 0; c < HALF; c += 8) {
+      const int j = cbase + c;
+      if (p.unit_cols && j + 8 <= p.N && (reinterpret_cast<uintptr_t>(dst + j) & 31) == 0) {
+        st_global_v8(dst + j, &run[c]);
+        continue;
+      }
+#pragma unroll
+      for (int h = 0; h < 8; h += 4) {
+        const int jh = j + h;
+        if (p.unit_cols && jh + 4 <= p.N && ((rbase + jh) & 3) == 0) {
+          *reinterpret_cast<float4*>(dst + jh) =
+              make_float4(run[c + h], run[c + h + 1], run[c + h + 2], run[c + h + 3]);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (jh + e < p.N) dst[p.unit_cols ? jh + e : p.ccol[jh + e]] = run[c + h + e];
+        }
+      }
+    }
+  }
+}
+
 // 10 warps per CTA: the SM's four register partitions (16K each) hold up to
 // three warps each, so at most 168 registers per thread.
 // Halo tiles: resident B' (every 64-wide k block of the 128-row panel) and
@@ -212,7 +322,8 @@ __global__ void __launch_bounds__(NT, CTAS)
               const __grid_constant__ CUtensorMap single_a,
               const __grid_constant__ CUtensorMap single_b,
               const __grid_constant__ CUtensorMap single_a2,
-              const __grid_constant__ CUtensorMap single_a3) {
+              const __grid_constant__ CUtensorMap single_a3,
+              const __grid_constant__ CUtensorMap single_c) {
   // probs == nullptr: one problem passed by value with its tensor maps as
   // kernel parameters (encoded at launch over per-run scratch)
   using T = Tile<BN, CTAS>;
@@ -238,8 +349,12 @@ __global__ void __launch_bounds__(NT, CTAS)
   uint64_t* chunk_full = b_full + (kHalo ? kbt : 1);  // [2] MMA -> drain
   uint64_t* chunk_empty = chunk_full + 2;    // [2] drain -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(chunk_empty + 2);
-  __shared__ float epi[kTransposeEpi ? 8 * 32 * kEpiPitch : 1];  // drain warps' transposes
-  static_assert(T::SMEM + kEpiBytes <= 227 * 1024, "shared memory per CTA");
+  // drain warps' staging: 32 x 32 transposes (padded pitch) or the 4 KB
+  // swizzled blocks of the TMA-store epilogue, one region per warp
+  constexpr bool kTmaEpi = CTAS == 1 && !kHalo;
+  constexpr int kEpiFloats = kTransposeEpi ? 8 * 32 * kEpiPitch : kTmaEpi ? 8 * 1024 : 1;
+  __shared__ __align__(1024) float epi[kEpiFloats];
+  static_assert(kHalo || T::SMEM + kEpiFloats * 4 <= 227 * 1024, "shared memory per CTA");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -302,6 +417,13 @@ __global__ void __launch_bounds__(NT, CTAS)
       }
       first = false;
     }
+    // the last round of each ring slot and the resident B' blocks loaded
+    // (those of the first tile's first g channel blocks) have landed
+    // before the CTA winds down
+    for (uint32_t i = g > (uint32_t)nst ? g - nst : 0; i < g; ++i)
+      mbar_drain(smem_u32(&full[i % nst]), (i / nst) & 1u);
+    for (int kb = 0; kb < kbt; ++kb)
+      if ((uint32_t)(kb % p.img_cblocks) < g) mbar_drain(smem_u32(&b_full[kb]), 0u);
   } else if (kHalo && warp == 1 && lane == 0) {
     // ----------------------------------------------- MMA issuer (halo tiles)
     const LtbTcProblem& p = single;
@@ -309,6 +431,7 @@ __global__ void __launch_bounds__(NT, CTAS)
     bool alive = true;
     bool first = true;  // B' blocks are waited for on first use
     const int nkb = kbt;
+    const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       int issued = 0, buf = 0;
       uint32_t acc = tmem;
@@ -322,7 +445,7 @@ __global__ void __launch_bounds__(NT, CTAS)
         const uint32_t a_slot = smem_u32(ring + (size_t)s * slot_bytes);
         for (int kh = 0; kh < p.img_kh && alive; ++kh)
           for (int kw = 0; kw < p.img_kw; ++kw) {
-            if (issued % kChunkBlocks == 0) {  // a new accumulation chunk
+            if (issued % cbk == 0) {  // a new accumulation chunk
               buf = (int)(q & 1u);
               if (!mbar_wait(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
                 alive = false;
@@ -343,9 +466,9 @@ __global__ void __launch_bounds__(NT, CTAS)
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk)
               mma_bf16(acc, ad + 2 * kk, bd + 2 * kk, T::IDESC,
-                       (issued % kChunkBlocks != 0) || (kk != 0));
+                       (issued % cbk != 0) || (kk != 0));
             ++issued;
-            if (issued % kChunkBlocks == 0 || issued == nkb) {
+            if (issued % cbk == 0 || issued == nkb) {
               mma_commit(smem_u32(&chunk_full[buf]));  // chunk complete in TMEM
               ++q;
             }
@@ -404,6 +527,9 @@ __global__ void __launch_bounds__(NT, CTAS)
         tma_load_2d(smem_u32(sa + A_BYTES), mb, fb, kb * BK, n0);
       }
     }
+    // the last round of each stage has landed before the CTA winds down
+    for (uint32_t i = g > (uint32_t)STAGES ? g - STAGES : 0; i < g; ++i)
+      mbar_drain(smem_u32(&full[i % STAGES]), (i / STAGES) & 1u);
   } else if (!kHalo && warp == 1 && lane == 0) {
     // ---------------------------------------------------------- MMA issuer
     uint32_t g = 0, q = 0;  // k blocks consumed, chunks produced
@@ -486,51 +612,12 @@ __global__ void __launch_bounds__(NT, CTAS)
       }
       if (!alive) break;
       // epilogue: this warp owns rows m0 + 32*quad .. +31 (row m0 + 32*quad
-      // + lane in this thread's registers) and HALF columns from cbase
-      float* cb = c_override ? c_override : p.c;
-      const int cbase = n0 + half * T::HALF;
-      if (kTransposeEpi && p.unit_cols) {
-        float* stage = epi + (warp - 2) * (32 * kEpiPitch);
-        const int64_t rb = rbase;
-#pragma unroll
-        for (int c = 0; c < T::HALF; c += 32) {
-          __syncwarp();
-#pragma unroll
-          for (int j = 0; j < 32; ++j) stage[lane * kEpiPitch + j] = run[c + j];
-          __syncwarp();
-          const int col = cbase + c + lane;
-          const bool cok = col < p.N;
-#pragma unroll 8
-          for (int i = 0; i < 32; ++i) {  // row i of the block: 32 consecutive columns
-            const int64_t rbi = __shfl_sync(0xffffffffu, rb, i);
-            const int vi = __shfl_sync(0xffffffffu, (int)rvalid, i);
-            if (vi && cok) cb[rbi + col] = stage[i * kEpiPitch + lane];
-          }
-        }
-      } else if (rvalid) {  // this thread's row: 32-byte (whole sector) stores where aligned
-        float* dst = cb + rbase;
-#pragma unroll
-        for (int c = 0; c < T::HALF; c += 8) {
-          const int j = cbase + c;
-          if (p.unit_cols && j + 8 <= p.N && (reinterpret_cast<uintptr_t>(dst + j) & 31) == 0) {
-            st_global_v8(dst + j, &run[c]);
-            continue;
-          }
-#pragma unroll
-          for (int h = 0; h < 8; h += 4) {
-            const int jh = j + h;
-            if (p.unit_cols && jh + 4 <= p.N && ((rbase + jh) & 3) == 0) {
-              *reinterpret_cast<float4*>(dst + jh) =
-                  make_float4(run[c + h], run[c + h + 1], run[c + h + 2], run[c + h + 3]);
-            } else {
-#pragma unroll
-              for (int e = 0; e < 4; ++e)
-                if (jh + e < p.N) dst[p.unit_cols ? jh + e : p.ccol[jh + e]] = run[c + h + e];
-            }
-          }
-        }
-      }
+      // + lane in this thread's registers) and HALF columns from n0 + half*HALF
+      write_tile<T::HALF, kTmaEpi, kTransposeEpi>(
+          p, probs ? static_cast<const CUtensorMap*>(p.map_c) : &single_c, c_override, run, epi,
+          warp - 2, m0, n0 + half * T::HALF, rvalid, rbase);
     }
+    if (kTmaEpi && lane == 0) bulk_wait();  // the tile stores have landed
   }
   __syncwarp();
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -538,6 +625,286 @@ __global__ void __launch_bounds__(NT, CTAS)
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(T::TMEM_COLS));
+}
+
+// ------------------------------------------------------------ CTA pairs
+// 256 x 256 output tiles on a cluster of two CTAs (tcgen05 cta_group::2):
+// CTA rank r loads A rows m0 + 128 r and B' rows n0 + 128 r of every k block
+// (16 + 16 KB a stage, its own shared memory), the leader (rank 0) issues
+// M = 256, N = 256 MMAs that read both CTAs' stages, and each CTA's TMEM
+// receives its own 128 rows of the tile (all 256 columns).  Per SM a k
+// block moves 32 KB for the MMA work that costs the single-CTA 128 x 256
+// tile 48 KB: the operand stream from L2, not the tensor core, bounds the
+// single-CTA form on long K.
+//   warp 0 lane 0 (both CTAs): TMA producer; both CTAs' loads complete on
+//     the leader's full[s], which alone expects the stage's 64 KB
+//   warp 1 lane 0 (leader): MMA issuer; each commit arrives on the barrier
+//     at the same offset in both CTAs (empty[s], chunk_full[b])
+//   warps 2..9 (both CTAs): drain + epilogue of the CTA's 128 rows; their
+//     chunk_empty arrivals go to the leader's barrier (2 x 256 a phase)
+// Waits are bounded as in the single-CTA kernel; a cluster barrier after
+// set-up and before teardown keeps either CTA from signalling or reading
+// the other's shared memory outside its lifetime.
+constexpr int kPairStages = 6;
+constexpr int kPairStageBytes = 2 * 128 * BK * 2;  // A half + B' half
+constexpr size_t kPairSmem = (size_t)kPairStages * kPairStageBytes + 1024 + 256;
+constexpr uint32_t kPairTmemCols = 512;  // two 256-column accumulator buffers
+// kind::f16: FP32 accumulator, BF16 A and B, both K-major, M = 256, N = 256
+constexpr uint32_t kPairIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) | ((256u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_index() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+  return r;
+}
+// the same shared-memory offset in the cluster's rank-0 CTA
+__device__ __forceinline__ uint32_t rank0_addr(uint32_t addr) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, 0;" : "=r"(r) : "r"(addr));
+  return r;
+}
+// every thread of both CTAs
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_cl(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n"
+      " mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait on a barrier that other CTAs of the cluster arrive on
+__device__ __forceinline__ bool mbar_wait_cl(uint32_t bar, uint32_t parity, int* err) {
+  if (mbar_try_cl(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_cl(bar, parity)) {
+    const long long dt = clock64() - t0;
+    if (dt > kWaitCycles || (dt > kFlagCycles && *(volatile int*)err)) {
+      atomicExch(err, 1);
+      return false;
+    }
+  }
+  return true;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+// 2-D TMA load into this CTA's shared memory completing on a barrier of
+// either CTA of the pair (cluster address)
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map,
+                                                 uint32_t bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void mma_bf16_pair(uint32_t tmem_d, uint64_t a, uint64_t b,
+                                              uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(kPairIdesc), "r"(accumulate));
+}
+// arrives on the barrier at this offset in both CTAs once the leader's
+// MMAs issued so far are complete
+__device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(bar),
+      "h"((unsigned short)3)
+      : "memory");
+}
+
+// Pair tile index -> (m0, n0) of the 256 x 256 tile (tiles_m, tiles_n in
+// pair tiles), raster as tile_coords
+__device__ __forceinline__ void pair_coords(const LtbTcProblem& p, int64_t lt, int* m0, int* n0) {
+  const int gmax = p.group_m > 0 ? p.group_m : 16;
+  const int64_t per_group = (int64_t)gmax * p.tiles_n;
+  const int g = (int)(lt / per_group);
+  const int idx = (int)(lt - (int64_t)g * per_group);
+  const int gm = p.tiles_m - g * gmax < gmax ? p.tiles_m - g * gmax : gmax;
+  *m0 = (g * gmax + idx % gm) * 256;
+  *n0 = (idx / gm) * 256;
+}
+
+__global__ void __launch_bounds__(NT, 1)
+    k_gemm_tc_pair(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
+                   int* err, const __grid_constant__ LtbTcProblem single,
+                   const __grid_constant__ CUtensorMap single_a,
+                   const __grid_constant__ CUtensorMap single_b,
+                   const __grid_constant__ CUtensorMap single_c) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)kPairStages * kPairStageBytes);
+  uint64_t* empty = full + kPairStages;
+  uint64_t* chunk_full = empty + kPairStages;  // [2] MMA -> drain (both CTAs)
+  uint64_t* chunk_empty = chunk_full + 2;      // [2] drain -> MMA (the leader's)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(chunk_empty + 2);
+  __shared__ __align__(1024) float epi[8 * 1024];  // drain warps' TMA-store staging
+  static_assert(kPairSmem + sizeof(float) * 8 * 1024 <= 227 * 1024, "shared memory per CTA");
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kPairStages; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);   // the leader's expect_tx
+      mbar_init(smem_u32(&empty[s]), 1);  // one commit
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&chunk_full[b]), 1);
+      mbar_init(smem_u32(&chunk_empty[b]), 2 * 8 * 32);  // both CTAs' drain threads
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {  // the same warp in both CTAs allocates for the pair
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kPairTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  cluster_sync_all();  // both CTAs' barriers initialised and TMEM allocated
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const int64_t first = cluster_index(), step = cluster_count();
+
+  if (warp == 0 && lane == 0) {
+    // ------------------------------------------------------------ producer
+    uint32_t g = 0;
+    bool alive = true;
+    for (int64_t t = first; t < total_tiles && alive; t += step) {
+      const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
+      const CUtensorMap* ma = probs ? static_cast<const CUtensorMap*>(p.map_a) : &single_a;
+      const CUtensorMap* mb = probs ? static_cast<const CUtensorMap*>(p.map_b) : &single_b;
+      int m0, n0;
+      pair_coords(p, t - p.tile_start, &m0, &n0);
+      const int nk = (int)((p.Kp + BK - 1) / BK);
+      for (int kb = 0; kb < nk; ++kb, ++g) {
+        const int s = g % kPairStages;
+        if (!mbar_wait_cl(smem_u32(&empty[s]), ((g / kPairStages) & 1u) ^ 1u, err)) {
+          alive = false;
+          break;
+        }
+        const uint32_t fb = smem_u32(&full[s]);
+        if (leader) mbar_expect_tx(fb, 2 * kPairStageBytes);
+        const uint32_t sa = smem_u32(smem + (size_t)s * kPairStageBytes);
+        const uint32_t fb0 = rank0_addr(fb);
+        tma_load_2d_pair(sa, ma, fb0, kb * BK, m0 + 128 * (int)rank);
+        tma_load_2d_pair(sa + A_BYTES, mb, fb0, kb * BK, n0 + 128 * (int)rank);
+      }
+    }
+    // the last round of each stage has landed (both CTAs' loads complete on
+    // the leader's barriers; the closing cluster barrier holds the peer)
+    if (leader)
+      for (uint32_t i = g > (uint32_t)kPairStages ? g - kPairStages : 0; i < g; ++i)
+        mbar_drain(smem_u32(&full[i % kPairStages]), (i / kPairStages) & 1u);
+  } else if (warp == 1 && lane == 0 && leader) {
+    // ---------------------------------------------------------- MMA issuer
+    uint32_t g = 0, q = 0;
+    bool alive = true;
+    for (int64_t t = first; t < total_tiles && alive; t += step) {
+      const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
+      const int nk = (int)((p.Kp + BK - 1) / BK);
+      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
+      for (int c0 = 0; c0 < nk && alive; c0 += cbk, ++q) {
+        const int buf = q & 1;
+        if (!mbar_wait_cl(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(buf * 256);
+        const int c1 = c0 + cbk < nk ? c0 + cbk : nk;
+        for (int kb = c0; kb < c1; ++kb, ++g) {
+          const int s = g % kPairStages;
+          if (!mbar_wait_cl(smem_u32(&full[s]), (g / kPairStages) & 1u, err)) {
+            alive = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(smem + (size_t)s * kPairStageBytes);
+          const uint64_t ad = sw128_desc(a0), bd = sw128_desc(a0 + A_BYTES);
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk)
+            mma_bf16_pair(acc, ad + 2 * kk, bd + 2 * kk, (kb != c0) || (kk != 0));
+          mma_commit_pair(smem_u32(&empty[s]));  // both CTAs' stage s reusable
+        }
+        mma_commit_pair(smem_u32(&chunk_full[buf]));  // chunk complete in both TMEMs
+      }
+    }
+  } else if (warp >= 2) {
+    // ------------------------------------------------------ drain/epilogue
+    const int quad = warp & 3, half = (warp - 2) >> 2;
+    uint32_t q = 0;
+    bool alive = true;
+    for (int64_t t = first; t < total_tiles && alive; t += step) {
+      const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
+      int m0, n0;
+      pair_coords(p, t - p.tile_start, &m0, &n0);
+      const int m0c = m0 + 128 * (int)rank;  // this CTA's rows of the tile
+      const int nk = (int)((p.Kp + BK - 1) / BK);
+      int row;
+      const bool rvalid = tile_row(p, m0c, quad * 32 + lane, &row);
+      const int64_t rbase = rvalid ? p.crow[row] : 0;
+      float run[128];
+#pragma unroll
+      for (int i = 0; i < 128; ++i) run[i] = 0.f;
+      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
+      for (int c0 = 0; c0 < nk; c0 += cbk, ++q) {
+        const int buf = q & 1;
+        const bool ok = mbar_wait_cl(smem_u32(&chunk_full[buf]), (q >> 1) & 1u, err);
+        if (!__all_sync(0xffffffffu, ok)) {
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t base =
+            tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * 256 + half * 128);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          uint32_t r[16];
+          tmem_ld16(base + (uint32_t)(c * 16), r);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) run[c * 16 + i] += __uint_as_float(r[i]);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive_remote(rank0_addr(smem_u32(&chunk_empty[buf])));  // buffer free
+      }
+      if (!alive) break;
+      write_tile<128, true, false>(p, probs ? static_cast<const CUtensorMap*>(p.map_c) : &single_c,
+                                   nullptr, run, epi, warp - 2, m0c, n0 + half * 128, rvalid,
+                                   rbase);
+    }
+    if (lane == 0) bulk_wait();  // the tile stores have landed
+  }
+  __syncwarp();
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  cluster_sync_all();  // no MMA, commit or arrival of either CTA still in flight
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kPairTmemCols));
 }
 
 // ------------------------------------------------------------ packing
@@ -967,6 +1334,21 @@ cudaError_t ltb_make_tmap(void* map, const void* base, int64_t rows, int64_t Kp,
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+cudaError_t ltb_make_tmap_c(void* map, float* base, int64_t M, int64_t N, int64_t ld) {
+  auto fn = encode_fn();
+  if (!fn || M < 1 || N < 1 || ld < N || ld % 4 || reinterpret_cast<uintptr_t>(base) % 16)
+    return cudaErrorInvalidValue;
+  const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)M};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  const cuuint32_t box[2] = {32, 32};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(reinterpret_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base,
+                  dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 cudaError_t ltb_make_tmap_image(void* map, const void* base, int n, int hp, int wp, int c,
                                 int wo, int rows) {
   auto fn = encode_fn();
@@ -1103,7 +1485,7 @@ template <int BN, bool TE, int CTAS = 1, bool HALO = false>
 static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b,
-                             const void* map_a2, const void* map_a3) {
+                             const void* map_a2, const void* map_a3, const void* map_c) {
   size_t smem = Tile<BN, CTAS>::SMEM;
   if (HALO) {
     if (d_probs || !single || !single->img_halo) return cudaErrorInvalidValue;
@@ -1118,7 +1500,7 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
   const int64_t slots = (int64_t)sms * CTAS;
   const int grid = (int)(total_tiles < slots ? total_tiles : slots);
   LtbTcProblem one{};
-  CUtensorMap ma{}, mb{}, ma2{}, ma3{};
+  CUtensorMap ma{}, mb{}, ma2{}, ma3{}, mc{};
   if (!d_probs) {
     if (!single || !map_a || !map_b) return cudaErrorInvalidValue;
     one = *single;
@@ -1126,20 +1508,92 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
     mb = *static_cast<const CUtensorMap*>(map_b);
     ma2 = map_a2 ? *static_cast<const CUtensorMap*>(map_a2) : ma;
     ma3 = map_a3 ? *static_cast<const CUtensorMap*>(map_a3) : ma2;
+    if (map_c) mc = *static_cast<const CUtensorMap*>(map_c);
+    else one.c_tma = 0;
   }
   k_gemm_tc<BN, TE, CTAS, HALO><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override,
-                                                        err, one, ma, mb, ma2, ma3);
+                                                        err, one, ma, mb, ma2, ma3, mc);
   return cudaGetLastError();
+}
+
+// Clusters of two CTAs the pair kernel can hold resident at once on a
+// device (its persistent grid): asked once per device.
+static int pair_clusters(int dev) {
+  static std::mutex mu;
+  static std::map<int, int> known;
+  std::lock_guard<std::mutex> g(mu);
+  auto it = known.find(dev);
+  if (it != known.end()) return it->second;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(NT, 1, 1);
+  cfg.dynamicSmemBytes = kPairSmem;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_gemm_tc_pair, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  known[dev] = n;
+  return n;
+}
+
+static cudaError_t launch_pair(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
+                               int* err, cudaStream_t st, const LtbTcProblem* single,
+                               const void* map_a, const void* map_b, const void* map_c) {
+  {
+    const cudaError_t e = ltb_smem_optin((const void*)k_gemm_tc_pair, kPairSmem);
+    if (e != cudaSuccess) return e;
+  }
+  int dev = 0;
+  {
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+  }
+  int64_t clusters = pair_clusters(dev);
+  if (clusters <= 0) return cudaErrorInvalidConfiguration;
+  if (total_tiles < clusters) clusters = total_tiles;
+  LtbTcProblem one{};
+  CUtensorMap ma{}, mb{}, mc{};
+  if (!d_probs) {
+    if (!single || !map_a || !map_b || single->img) return cudaErrorInvalidValue;
+    one = *single;
+    ma = *static_cast<const CUtensorMap*>(map_a);
+    mb = *static_cast<const CUtensorMap*>(map_b);
+    if (map_c) mc = *static_cast<const CUtensorMap*>(map_c);
+    else one.c_tma = 0;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(2 * clusters), 1, 1);
+  cfg.blockDim = dim3(NT, 1, 1);
+  cfg.dynamicSmemBytes = kPairSmem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_gemm_tc_pair, d_probs, nprob, total_tiles, err, one, ma, mb,
+                            mc);
 }
 
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single, const void* map_a,
-                               const void* map_b, const void* map_a2, const void* map_a3) {
+                               const void* map_b, const void* map_a2, const void* map_a3,
+                               const void* map_c) {
   if (total_tiles == 0) return cudaSuccess;
 #define LTB_TC(BN, TE)                                                                      \
   return launch_tc<BN, TE>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a, \
-                           map_b, map_a2, map_a3)
+                           map_b, map_a2, map_a3, map_c)
   switch (bn) {
     case 128: LTB_TC(128, false);
     case 129: LTB_TC(128, true);
@@ -1147,10 +1601,13 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
     case 257: LTB_TC(256, true);
     case 130:  // 128 wide, two CTAs per SM
       return launch_tc<128, false, 2>(d_probs, nprob, total_tiles, c_override, sms, err, st,
-                                      single, map_a, map_b, map_a2, map_a3);
+                                      single, map_a, map_b, map_a2, map_a3, map_c);
     case 131:  // 128 wide halo image tiles, resident weights
       return launch_tc<128, false, 1, true>(d_probs, nprob, total_tiles, c_override, sms, err,
-                                            st, single, map_a, map_b, map_a2, map_a3);
+                                            st, single, map_a, map_b, map_a2, map_a3, map_c);
+    case 258:  // 256 x 256 tiles on CTA pairs (plain operands, B' boxes of 128 rows)
+      if (c_override) return cudaErrorInvalidValue;
+      return launch_pair(d_probs, nprob, total_tiles, err, st, single, map_a, map_b, map_c);
   }
 #undef LTB_TC
   return cudaErrorInvalidValue;

@@ -86,6 +86,10 @@ struct GemmTables {
   int a_slot = -1, b_slot = -1;       // scratch slots of the packed operands
   LtbTcProblem prob{};                // launch template (maps/c bound per run)
   bool a_kcontig = true, b_kcontig = true, unit_cols = false;
+  // output rows crow[r] = c_row0 + r * c_ld with unit columns, ld and every
+  // offset a multiple of 4 floats: written by TMA stores (LtbTcProblem::c_tma)
+  bool c_tma = false;
+  int64_t c_row0 = 0, c_ld = 0;
   bool a_off32 = false, b_off32 = false;  // operand offsets fit in int32
   bool a_k32 = false, b_k32 = false;      // k offsets alone fit in int32
   // implicit-GEMM convolution: A packed as NHWC BF16 image(s) read by 4-D
@@ -96,22 +100,35 @@ struct GemmTables {
   LtbImageJob ijob{};                 // base / hi / lo / lo2 bound at launch
   int bn = 256;                       // tensor-core tile width (128 or 256)
   int epi = 0;                        // 1: shared-memory transposed epilogue,
-                                      // 2: two CTAs per SM, 3: halo image tiles
+                                      // 2: two CTAs per SM, 3: halo image tiles,
+                                      // 4: 256 x 256 tiles on CTA pairs
   // halo image tiles (single-segment image operands, N <= 128): the launch
   // template in halo geometry, valid when halo_ok
   LtbTcProblem halo{};
   bool halo_ok = false;
 };
 
-// Tile width of a tensor-core contraction: output tiles are 128 x bn.
+// Tile form of a tensor-core contraction: output tiles are 128 x bn, or
+// 256 x 256 on CTA pairs (epi 4, plain operands).
 void set_tile_n(GemmTables& t, int bn, int epi) {
   if (epi == 3 && !(t.halo_ok && bn == 128)) epi = 0;
+  if (epi == 4 && (t.img || bn != 256)) epi = 0;
   t.bn = bn;
   t.epi = epi;
+  if (!t.img) t.prob.tiles_m = (int)((t.prob.M + (epi == 4 ? 255 : 127)) / (epi == 4 ? 256 : 128));
   const int64_t tn = (t.prob.N + bn - 1) / bn;
   t.prob.tiles_n = (int)tn;
   t.tiles = epi == 3 ? (int64_t)t.halo.tiles_m : (int64_t)t.prob.tiles_m * tn;
 }
+
+// Launch variant of a tile form (ltb_launch_gemm_tc, schedules): tile
+// width | form, or 258 for CTA pairs.
+int variant_code(const GemmTables& t) { return t.epi == 4 ? 258 : t.bn | t.epi; }
+
+// Rows of a B' tensor-map box: the tile width, or half of it on CTA pairs.
+int b_box_rows(const GemmTables& t) { return t.epi == 4 ? 128 : t.bn; }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // The image repack job of a run: the operand's buffer and the A slot, which
 // holds the hi image, then the lo and lo2 images when the split has them.
@@ -415,6 +432,16 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
   auto ctab = table(nd, d.out_coef, 0);
   t.unit_cols = true;
   for (size_t j = 0; j < ctab.size(); ++j) t.unit_cols = t.unit_cols && ctab[j] == (int64_t)j;
+  {
+    auto rc = table(md, d.out_coef, d.out_off);
+    int64_t ld = 0;
+    const bool affine = arith(rc, &ld);
+    if (rc.size() == 1) ld = (con.N + 3) / 4 * 4;  // one row: any pitch
+    t.c_row0 = rc[0];
+    t.c_ld = ld;
+    t.c_tma = affine && t.unit_cols && ld >= con.N && ld % 4 == 0 && rc[0] >= 0 && rc[0] % 4 == 0;
+    for (auto o : t.c_boff) t.c_tma = t.c_tma && o % 4 == 0;
+  }
   if (c->opt.precision != ltb::Precision::fp32 && c->opt.use_tensor_cores &&
       con.M < (1LL << 31) && con.N < (1LL << 31)) {
     t.tc = true;
@@ -453,15 +480,21 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     e.N = (int)con.N;
     e.tiles_m = tm;
     e.unit_cols = t.unit_cols ? 1 : 0;
+    e.c_tma = t.c_tma ? 1 : 0;  // and per run: C + c_row0 16-byte aligned
+    e.map_c = nullptr;
     // the six-product mode drains every 2 k blocks (128 K): its pieces
     // carry FP32's whole significand, so the accumulation's truncation is
-    // what is left to bound
-    e.chunk_blocks = t.nseg >= 6 ? 2 : 0;
+    // what is left to bound; plain BF16 accumulates the whole K in TMEM
+    // (its inputs' rounding, 2^-9 of each product, outweighs the
+    // truncation, ~2^-24 a K=16 step), so a tile is drained once
+    e.chunk_blocks = t.nseg >= 6 ? 2 : t.nseg == 1 ? (int)((t.Kp + 63) / 64) : 0;
     ImageGeom ig;
     if (t.nbatch == 1 && t.Kp == t.nseg * con.K && detect_image(d, A, md, kd, ig)) {
       // implicit GEMM: A' never materialises; the A slot holds the padded
       // NHWC image(s), hi (+ lo for split modes, + lo2 for three-piece ones)
       t.img = true;
+      t.c_tma = false;  // image tiles' rows are not one progression
+      e.c_tma = 0;
       const int segs = (1 << t.nseg) - 1;
       t.img_kinds = ((t.a_mask >> 8) & segs) ? 3 : (~t.a_mask & segs) ? 2 : 1;
       const int64_t hp = ig.ho + ig.kh - 1, wp = ig.wo + ig.kw - 1;
@@ -493,6 +526,9 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
       e.tiles_m = (int)(ig.nimg * e.img_hgroups);
       if (t.nseg == 1) {
         t.halo = e;
+        // halo tiles keep 512-element chunks: their first chunk drains while
+        // the tile's last k blocks run (measured faster than one chunk)
+        t.halo.chunk_blocks = 0;
         t.halo_ok = ltb_tc_halo_geometry(t.halo, (int)wp);
       }
       // B' in the image's K order: k' = (kh * KW + kw) * C + c
@@ -740,7 +776,7 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         }
         void* ap = bt.p[t.a_slot];
         void* bp = bt.p[t.b_slot];
-        alignas(64) unsigned char maps[512];  // A (hi image), B, A lo image, A lo2 image
+        alignas(64) unsigned char maps[640];  // A (hi image), B, A lo, A lo2, C
         if (t.img) {
           LtbImageJob j = image_job(t, p.a.base, ap);
           e = ltb_launch_pack_conv(j, p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig,
@@ -763,17 +799,22 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
         if (e == cudaSuccess && !t.img)  // image operands packed B' with the image
           e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, t.b_off32,
                               c->sms, st);
-        if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, t.bn);
+        if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, b_box_rows(t));
+        const bool c_tma = t.c_tma && t.epi != 3 && aligned16(p.c + t.c_row0);
+        if (e == cudaSuccess && c_tma)
+          e = ltb_make_tmap_c(maps + 512, p.c + t.c_row0, p.M, p.N, t.c_ld);
         if (e == cudaSuccess) {
           LtbTcProblem one = t.epi == 3 ? t.halo : t.prob;
+          one.c_tma = c_tma ? 1 : 0;
           one.group_m = t.prob.group_m;
           one.c = p.c;
           one.crow = t.c_row;
           one.ccol = t.c_col;
-          e = ltb_launch_gemm_tc(t.bn | t.epi, nullptr, 1, t.tiles, nullptr, c->sms,
+          e = ltb_launch_gemm_tc(variant_code(t), nullptr, 1, t.tiles, nullptr, c->sms,
                                  timeout_flag(c->device, st), st,
                                  &one, maps, maps + 128, t.img ? maps + 256 : nullptr,
-                                 t.img_kinds == 3 ? maps + 384 : nullptr);
+                                 t.img_kinds == 3 ? maps + 384 : nullptr,
+                                 c_tma ? maps + 512 : nullptr);
         }
       }
       break;
@@ -834,13 +875,14 @@ void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
   pin_cfg(c, i);
   const int g = c->gemm_of[i];
   if (g >= 0 && c->gemms[g].tc) {
-    // variant: tile width | form, form 0: row-store epilogue, 1: transposed
-    // epilogue, 2: two CTAs per SM (128 wide only)
+    // variant: tile width | form, form 0: row-store (or TMA-store)
+    // epilogue, 1: transposed epilogue, 2: two CTAs per SM (128 wide only),
+    // 3: halo image tiles; 258: 256 x 256 tiles on CTA pairs
     const int v = cfg.variant;
-    const int bn = v == 256 || v == 257 ? 256 : 128;
-    const int epi = v == 129 || v == 257 ? 1 : v == 130 ? 2 : v == 131 ? 3 : 0;
-    set_tile_n(c->gemms[g], bn, epi);  // 131 falls back to 128 without halo geometry
-    c->cfg[i].variant = bn | c->gemms[g].epi;
+    const int bn = v == 256 || v == 257 || v == 258 ? 256 : 128;
+    const int epi = v == 129 || v == 257 ? 1 : v == 130 ? 2 : v == 131 ? 3 : v == 258 ? 4 : 0;
+    set_tile_n(c->gemms[g], bn, epi);  // 131 and 258 fall back where they do not apply
+    c->cfg[i].variant = variant_code(c->gemms[g]);
     // cta_per_sm of a contraction: the raster group (row blocks swept together)
     c->gemms[g].prob.group_m = cfg.cta_per_sm;
   }
@@ -1060,9 +1102,11 @@ std::string describe(ltb_compiled* c, int i) {
   if (s.family == ltb::Family::contraction) {
     const auto& t = c->gemms[c->gemm_of[i]];
     if (t.tc)
-      o << "tile(128x" << t.bn << "x64) tensor_cores(tcgen05) parallel(persistent, "
-        << t.tiles << " tiles) raster(" << (t.prob.group_m ? t.prob.group_m : 16)
-        << " row blocks) epilogue("
+      o << (t.epi == 4 ? "tile(256x256x64 on CTA pairs, cta_group::2)" : "tile(128x")
+        << (t.epi == 4 ? "" : std::to_string(t.bn) + "x64)")
+        << " tensor_cores(tcgen05) parallel(persistent, " << t.tiles << " tiles) raster("
+        << (t.prob.group_m ? t.prob.group_m : 16) << " row blocks) epilogue("
+        << (t.c_tma && t.epi != 2 && t.epi != 3 ? "TMA stores where aligned, else " : "")
         << (t.epi == 1 ? "smem transpose" : t.epi == 2 ? "row stores, 2 CTAs/SM" : "row stores")
         << ")"
         << (t.epi == 3 ? " implicit_conv(halo tiles: one 4-D TMA box per tile and channel block, "
@@ -1111,8 +1155,9 @@ std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
     }
     case ltb::Family::contraction:
       if (c->gemms[c->gemm_of[i]].tc) {
-        for (int v : {128, 129, 130, 256, 257})
-          for (int gm : {0, 8, 32}) buf[n++] = LtbCfg{gm, 0, v};
+        for (int v : {128, 129, 130, 256, 257, 258})
+          if (v != 258 || !c->gemms[c->gemm_of[i]].img)
+            for (int gm : {0, 8, 32}) buf[n++] = LtbCfg{gm, 0, v};
         if (c->gemms[c->gemm_of[i]].halo_ok) buf[n++] = LtbCfg{0, 0, 131};
       } else {  // CUDA-core tiles
         buf[n++] = LtbCfg{0, 0, 64};
@@ -1328,9 +1373,9 @@ struct ltb_batch {
   std::vector<LtbImageJob> img_jobs;        // image operands, repacked before the pack
   // tensor-core problems grouped by schedule variant (kGroupCode), one
   // persistent launch per non-empty group
-  LtbTcProblem* d_tc[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  int ntc[5] = {0, 0, 0, 0, 0};
-  int64_t tc_tiles[5] = {0, 0, 0, 0, 0};
+  LtbTcProblem* d_tc[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int ntc[6] = {0, 0, 0, 0, 0, 0};
+  int64_t tc_tiles[6] = {0, 0, 0, 0, 0, 0};
   LtbGemmProblem* d_simt = nullptr;
   int64_t* d_simt_start = nullptr;
   int64_t simt_tiles = 0;
@@ -1344,17 +1389,18 @@ struct ltb_batch {
 
 namespace {
 
-constexpr int kGroupCode[5] = {128, 129, 256, 257, 130};  // launch variant per group
+constexpr int kGroups = 6;
+constexpr int kGroupCode[kGroups] = {128, 129, 256, 257, 130, 258};  // launch variant per group
 
 int group_of(const GemmTables& t) {
-  const int v = t.bn | t.epi;
-  for (int g = 0; g < 5; ++g)
+  const int v = variant_code(t);
+  for (int g = 0; g < kGroups; ++g)
     if (kGroupCode[g] == v) return g;
   return 0;
 }
 
 void batch_gemms(ltb_batch* b, cudaStream_t st) {
-  for (int g = 0; g < 5; ++g)
+  for (int g = 0; g < kGroups; ++g)
     if (b->ntc[g])
       CUDA_TRY(ltb_launch_gemm_tc(kGroupCode[g], b->d_tc[g], b->ntc[g],
                                   b->tc_tiles[g], nullptr,
@@ -1401,8 +1447,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->device = cs[0]->device;
     b->sms = cs[0]->sms;
     std::vector<LtbPackJob> jobs;
-    std::vector<LtbTcProblem> tcp[5];
-    std::vector<unsigned char> maps[5];  // two 128-byte CUtensorMaps per problem
+    std::vector<LtbTcProblem> tcp[kGroups];
+    std::vector<unsigned char> maps[kGroups];  // five 128-byte CUtensorMaps per problem
     std::vector<LtbGemmProblem> sp;
     std::vector<int64_t> sstart;
     for (int i = 0; i < n; ++i) {
@@ -1466,8 +1512,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         job(p.b, p.N, bp, t.b_mask, t.b_kcontig, t.b_off32);
         const int grp = group_of(t);
         auto& mv = maps[grp];
-        mv.resize(mv.size() + 512);  // A (hi image), B, A lo image, A lo2 image
-        unsigned char* m = mv.data() + mv.size() - 512;
+        mv.resize(mv.size() + 640);  // A (hi image), B, A lo image, A lo2 image, C
+        unsigned char* m = mv.data() + mv.size() - 640;
         if (t.img) {
           const LtbImageJob j = image_job(t, p.a.base, ap);
           b->img_jobs.push_back(j);
@@ -1479,8 +1525,10 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         } else {
           CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
         }
-        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, t.bn));
+        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, b_box_rows(t)));
         LtbTcProblem q = t.prob;
+        q.c_tma = t.c_tma && aligned16(p.c + t.c_row0) ? 1 : 0;
+        if (q.c_tma) CUDA_TRY(ltb_make_tmap_c(m + 512, p.c + t.c_row0, p.M, p.N, t.c_ld));
         q.c = p.c;
         q.crow = t.c_row;
         q.ccol = t.c_col;
@@ -1499,14 +1547,15 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->njobs = (int)jobs.size();
     if (b->tc) {
       b->d_jobs = upload(jobs, b->owned);
-      for (int g = 0; g < 5; ++g) {
+      for (int g = 0; g < kGroups; ++g) {
         // tensor maps in device memory (cudaMalloc is 256-byte aligned)
         unsigned char* d_maps = upload(maps[g], b->owned);
         for (size_t i = 0; i < tcp[g].size(); ++i) {
-          tcp[g][i].map_a = d_maps + 512 * i;
-          tcp[g][i].map_b = d_maps + 512 * i + 128;
-          tcp[g][i].map_a2 = d_maps + 512 * i + 256;
-          tcp[g][i].map_a3 = d_maps + 512 * i + 384;
+          tcp[g][i].map_a = d_maps + 640 * i;
+          tcp[g][i].map_b = d_maps + 640 * i + 128;
+          tcp[g][i].map_a2 = d_maps + 640 * i + 256;
+          tcp[g][i].map_a3 = d_maps + 640 * i + 384;
+          tcp[g][i].map_c = d_maps + 640 * i + 512;
         }
         b->ntc[g] = (int)tcp[g].size();
         b->d_tc[g] = upload(tcp[g], b->owned);
@@ -1796,6 +1845,11 @@ int ltb_int_property(ltb_compiled* c, const char* name, int64_t* value) {
   else if (k == "implicit_conv") {
     int64_t n = 0;
     for (const auto& t : c->gemms) n += t.img ? 1 : 0;
+    *value = n;
+  }
+  else if (k == "tma_store_output") {  // tensor-core contractions whose C TMA can store
+    int64_t n = 0;
+    for (const auto& t : c->gemms) n += t.tc && t.c_tma ? 1 : 0;
     *value = n;
   }
   else return fail(LTB_ERR_INVALID, "unknown property " + k);

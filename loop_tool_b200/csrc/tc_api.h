@@ -19,6 +19,12 @@ struct LtbTcProblem {
   int tiles_m, tiles_n;
   int unit_cols;         // ccol[j] == j
   int group_m;           // raster: row blocks swept together (0: 16)
+  // Output by TMA stores: C rows are an arithmetic progression
+  // (crow[r] = crow[0] + r * ld, ld % 4 == 0) of unit columns, and map_c is
+  // a CUtensorMap over C + crow[0] (ltb_make_tmap_c); single-CTA plain tiles
+  // only (0: per-thread row stores)
+  int c_tma;
+  const void* map_c;
   // Image operand (implicit-GEMM convolution, stride 1): A is read straight
   // from a zero-padded NHWC BF16 image [n, Hp, Wp, C] through 4-D boxes of
   // 64 channels x wo output columns, one box per output image row; a
@@ -68,6 +74,9 @@ cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st);
 cudaError_t ltb_launch_pack_conv(const LtbImageJob& j, const LtbGemmOperand& bop, int64_t rows,
                                  int64_t K, void* out, int64_t Kp, int nseg, int seg_mask,
                                  int k_contig, int off32, cudaStream_t st);
+// CUtensorMap over an FP32 output [M, N] with row pitch ld (floats) in
+// 32 x 32 boxes, 128-byte swizzled: base 16-byte aligned, ld % 4 == 0.
+cudaError_t ltb_make_tmap_c(void* map, float* base, int64_t M, int64_t N, int64_t ld);
 // CUtensorMap over an NHWC BF16 image [n, hp, wp, c] with boxes of
 // 64 channels x wo columns x rows image rows (128-byte swizzle):
 // c % 64 == 0, wo <= 256, rows <= 256.
@@ -122,11 +131,12 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
 // 130: 128 wide, two CTAs per SM; 131: 128 wide halo image tiles with
 // resident weights, single problems only).
 // c_override, if not null, replaces every problem's output pointer.
-// d_probs == nullptr: a single problem passed by value with its two tensor
-// maps (host copies, passed as kernel parameters).
+// d_probs == nullptr: a single problem passed by value with its tensor maps
+// (host copies, passed as kernel parameters; no map_c: row stores).
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single = nullptr,
                                const void* map_a = nullptr, const void* map_b = nullptr,
-                               const void* map_a2 = nullptr, const void* map_a3 = nullptr);
+                               const void* map_a2 = nullptr, const void* map_a3 = nullptr,
+                               const void* map_c = nullptr);
 int ltb_tc_tile_m();

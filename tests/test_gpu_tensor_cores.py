@@ -107,6 +107,122 @@ def test_pack_layouts(shape, precision, cuda_dev):
     assert err <= TOL[precision], f"{shape} {precision}: normwise error {err:.3g}"
 
 
+# Output tiles written by TMA stores: C rows one progression whose pitch
+# is a multiple of 4 floats.  Ragged M and N edges (boxes clipped at the
+# tensor), a single row, a 4-float pitch, and N % 4 != 0 (per-thread row
+# stores); every tile form, so the two-CTA form's row stores and the
+# transposed form's staging share the checks.  (M, K, N, TMA-stored)
+TMA_STORE = [(300, 64, 200, 1), (1, 64, 36, 1), (70, 32, 4, 1), (130, 96, 66, 0),
+             (256, 128, 512, 1)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16"])
+@pytest.mark.parametrize("variant", [256, 257, 128, 129, 130, 258])
+@pytest.mark.parametrize("shape", TMA_STORE)
+def test_tma_store_epilogue(shape, variant, precision, cuda_dev):
+    import torch
+
+    import loop_tool_b200 as lt
+    from programs import mm
+
+    M, K, N, tma = shape
+    T, _ = mm(M, K, N)
+    c = lt.cuda(T.ir, precision=precision)
+    assert c.int_property("tma_store_output") == tma
+    c.set_schedule(0, variant=variant)
+    g = torch.Generator(device=cuda_dev).manual_seed(M + 5 * N + 11 * K)
+    A = torch.randn(M * K, device=cuda_dev, generator=g)
+    B = torch.randn(K * N, device=cuda_dev, generator=g)
+    # the output at a 16-byte offset into a larger buffer, guarded on both sides
+    buf = torch.full((M * N + 8,), float("nan"), device=cuda_dev)
+    C = buf[4:4 + M * N]
+    for _ in range(2):
+        c([A, B, C])
+    torch.cuda.synchronize()
+    exact = (A.cpu().numpy().reshape(M, K).astype(np.float64) @
+             B.cpu().numpy().reshape(K, N).astype(np.float64))
+    got = C.cpu().numpy().reshape(M, N)
+    assert np.isfinite(got).all()
+    assert np.isnan(buf[:4].cpu().numpy()).all() and np.isnan(buf[4 + M * N:].cpu().numpy()).all()
+    err = normwise(got, exact)
+    assert err <= TOL[precision], f"{shape} {precision} {variant}: normwise error {err:.3g}"
+
+
+# 256 x 256 tiles on CTA pairs (variant 258, tcgen05 cta_group::2): each CTA
+# of the pair loads half of A's and half of B's rows and receives its 128
+# rows of the tile.  A tile whose second CTA has no rows (M <= 128), whose
+# second B' half is out of range (N <= 128), a single k block, many
+# accumulation chunks, a ragged edge everywhere, and N % 4 != 0 (row stores).
+PAIR = [(100, 64, 90), (200, 64, 120), (256, 64, 256), (300, 2048, 520), (513, 200, 259),
+        (1000, 96, 1030)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["bf16x6", "bf16x3", "bf16"])
+@pytest.mark.parametrize("shape", PAIR)
+def test_cta_pair_tiles(shape, precision, cuda_dev):
+    import torch
+
+    import loop_tool_b200 as lt
+    from programs import mm
+
+    M, K, N = shape
+    T, _ = mm(M, K, N)
+    c = lt.cuda(T.ir, precision=precision)
+    c.set_schedule(0, variant=258)
+    assert c.schedule(0)[2] == 258
+    g = torch.Generator(device=cuda_dev).manual_seed(M * 3 + N + 7 * K)
+    A = torch.randn(M * K, device=cuda_dev, generator=g)
+    B = torch.randn(K * N, device=cuda_dev, generator=g)
+    C = torch.full((M * N,), float("nan"), device=cuda_dev)
+    for _ in range(2):
+        c([A, B, C])
+    torch.cuda.synchronize()
+    exact = (A.cpu().numpy().reshape(M, K).astype(np.float64) @
+             B.cpu().numpy().reshape(K, N).astype(np.float64))
+    got = C.cpu().numpy().reshape(M, N)
+    assert np.isfinite(got).all()
+    err = normwise(got, exact)
+    assert err <= TOL[precision], f"{shape} {precision}: normwise error {err:.3g}"
+    # the same contraction on 128 x 256 single-CTA tiles: equal up to the
+    # order the tensor core sums each K=16 step in (BF16 products are exact)
+    c.set_schedule(0, variant=256)
+    C2 = torch.full((M * N,), float("nan"), device=cuda_dev)
+    c([A, B, C2])
+    torch.cuda.synchronize()
+    assert normwise(C2.cpu().numpy().reshape(M, N), got.astype(np.float64)) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_cta_pair_tiles_in_batch(cuda_dev):
+    """CTA-pair members beside single-CTA members in one grouped launch."""
+    import torch
+
+    import loop_tool_b200 as ltb
+    from programs import mm
+
+    g = torch.Generator(device=cuda_dev).manual_seed(23)
+    members, shapes = [], [(300, 128, 520, 258), (96, 64, 48, 128), (700, 256, 300, 258),
+                           (130, 96, 66, 256)]
+    for M, K, N, v in shapes:
+        T, _ = mm(M, K, N)
+        c = ltb.Compiled(T.ir, precision="bf16x3")
+        c.set_schedule(0, variant=v)
+        members.append((c, [torch.randn(M * K, device=cuda_dev, generator=g) / K ** 0.5,
+                            torch.randn(K * N, device=cuda_dev, generator=g),
+                            torch.full((M * N,), float("nan"), device=cuda_dev)]))
+    stream = torch.cuda.Stream()
+    b = ltb.Batch(members, capture_stream=stream.cuda_stream)
+    b.run(stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    for (c, (A, B, C)), (M, K, N, v) in zip(members, shapes):
+        exact = A.view(M, K).double() @ B.view(K, N).double()
+        got = C.view(M, N).double()
+        assert torch.isfinite(got).all()
+        assert float((got - exact).norm() / exact.norm()) <= TOL["bf16x3"], (M, K, N, v)
+
+
 # Convolution as implicit GEMM: NCHW inputs with 64-channel blocks and output
 # widths that are multiples of 8 are read by the tensor-core kernel straight
 # from a padded NHWC image (4-D TMA boxes per output image row); the other

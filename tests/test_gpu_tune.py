@@ -124,7 +124,8 @@ def test_tile_widths_agree(name, precision, cuda_dev):
     ins = [torch.from_numpy(a).to(cuda_dev) for a in case["inputs"]]
     stage = [i for i in range(c.int_property("stages")) if c.schedule(i)[2] in (128, 256)][0]
     # tile width (+1: shared-memory transposed epilogue) x raster group
-    for bn, gm in ((128, 0), (129, 8), (130, 0), (130, 16), (256, 32), (257, 0), (256, 1)):
+    for bn, gm in ((128, 0), (129, 8), (130, 0), (130, 16), (256, 32), (257, 0), (256, 1),
+                   (258, 0), (258, 4)):
         c.set_schedule(stage, cta_per_sm=gm, variant=bn)
         assert c.schedule(stage) == (gm, 0, bn)
         out = torch.full((c.io_sizes[-1],), float("nan"), device=cuda_dev)
