@@ -83,6 +83,9 @@ struct Tile {
   // dynamic: ring + alignment slack + barriers (the epilogue buffers are
   // static shared memory, kEpiBytes more per CTA)
   static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 + 256;
+  // launches with TMA-stored outputs and no transposed-epilogue buffer:
+  // 32 KB of staging 1024 bytes after the ring (past its barriers)
+  static constexpr size_t SMEM_TMA = (size_t)STAGES * STAGE_BYTES + 1024 + 1024 + 8 * 4096;
 };
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
                                             int x, int y) {
@@ -349,12 +352,18 @@ __global__ void __launch_bounds__(NT, CTAS)
   uint64_t* chunk_full = b_full + (kHalo ? kbt : 1);  // [2] MMA -> drain
   uint64_t* chunk_empty = chunk_full + 2;    // [2] drain -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(chunk_empty + 2);
-  // drain warps' staging: 32 x 32 transposes (padded pitch) or the 4 KB
-  // swizzled blocks of the TMA-store epilogue, one region per warp
+  // drain warps' staging, one region per warp: the transposed form's 32 x
+  // 32 transposes (padded pitch), and the 4 KB swizzled blocks of the
+  // TMA-store epilogue in the same buffer, or else in 32 KB of dynamic
+  // shared memory after the ring's barriers, present only in launches with
+  // TMA-stored outputs (SMEM_TMA): image operands keep the L1 capacity
   constexpr bool kTmaEpi = CTAS == 1 && !kHalo;
-  constexpr int kEpiFloats = kTransposeEpi ? 8 * 32 * kEpiPitch : kTmaEpi ? 8 * 1024 : 1;
+  constexpr int kEpiFloats = kTransposeEpi ? 8 * 32 * kEpiPitch : 1;
   __shared__ __align__(1024) float epi[kEpiFloats];
+  float* tma_stage =
+      kTransposeEpi ? epi : reinterpret_cast<float*>(smem + (size_t)STAGES * STAGE_BYTES + 1024);
   static_assert(kHalo || T::SMEM + kEpiFloats * 4 <= 227 * 1024, "shared memory per CTA");
+  static_assert(T::SMEM_TMA <= 227 * 1024, "shared memory per CTA");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -431,7 +440,9 @@ __global__ void __launch_bounds__(NT, CTAS)
     bool alive = true;
     bool first = true;  // B' blocks are waited for on first use
     const int nkb = kbt;
-    const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
+    // halo problems keep the default chunk (a compile-time divisor: this
+    // single issuing thread is on the MMA's critical path)
+    constexpr int cbk = kChunkBlocks;
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       int issued = 0, buf = 0;
       uint32_t acc = tmem;
@@ -614,8 +625,9 @@ __global__ void __launch_bounds__(NT, CTAS)
       // epilogue: this warp owns rows m0 + 32*quad .. +31 (row m0 + 32*quad
       // + lane in this thread's registers) and HALF columns from n0 + half*HALF
       write_tile<T::HALF, kTmaEpi, kTransposeEpi>(
-          p, probs ? static_cast<const CUtensorMap*>(p.map_c) : &single_c, c_override, run, epi,
-          warp - 2, m0, n0 + half * T::HALF, rvalid, rbase);
+          p, probs ? static_cast<const CUtensorMap*>(p.map_c) : &single_c, c_override, run,
+          p.c_tma && !kTransposeEpi ? tma_stage : epi, warp - 2, m0, n0 + half * T::HALF, rvalid,
+          rbase);
     }
     if (kTmaEpi && lane == 0) bulk_wait();  // the tile stores have landed
   }
@@ -1485,16 +1497,20 @@ template <int BN, bool TE, int CTAS = 1, bool HALO = false>
 static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b,
-                             const void* map_a2, const void* map_a3, const void* map_c) {
-  size_t smem = Tile<BN, CTAS>::SMEM;
+                             const void* map_a2, const void* map_a3, const void* map_c,
+                             bool c_tma_any) {
+  // TMA-stored outputs in this launch: the staging in dynamic shared memory
+  const bool tma = !TE && CTAS == 1 && !HALO && (d_probs ? c_tma_any : single && single->c_tma && map_c);
+  size_t smem = tma ? Tile<BN, CTAS>::SMEM_TMA : Tile<BN, CTAS>::SMEM;
   if (HALO) {
     if (d_probs || !single || !single->img_halo) return cudaErrorInvalidValue;
     smem = halo_smem(*single);
     if (smem > kHaloSmemMax) return cudaErrorInvalidValue;
   }
   {
-    const cudaError_t e = ltb_smem_optin((const void*)k_gemm_tc<BN, TE, CTAS, HALO>,
-                                         HALO ? kHaloSmemMax : smem);
+    const cudaError_t e = ltb_smem_optin(
+        (const void*)k_gemm_tc<BN, TE, CTAS, HALO>,
+        HALO ? kHaloSmemMax : !TE && CTAS == 1 ? Tile<BN, CTAS>::SMEM_TMA : smem);
     if (e != cudaSuccess) return e;
   }
   const int64_t slots = (int64_t)sms * CTAS;
@@ -1589,11 +1605,11 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single, const void* map_a,
                                const void* map_b, const void* map_a2, const void* map_a3,
-                               const void* map_c) {
+                               const void* map_c, int c_tma_any) {
   if (total_tiles == 0) return cudaSuccess;
 #define LTB_TC(BN, TE)                                                                      \
   return launch_tc<BN, TE>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a, \
-                           map_b, map_a2, map_a3, map_c)
+                           map_b, map_a2, map_a3, map_c, c_tma_any)
   switch (bn) {
     case 128: LTB_TC(128, false);
     case 129: LTB_TC(128, true);
@@ -1601,10 +1617,11 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
     case 257: LTB_TC(256, true);
     case 130:  // 128 wide, two CTAs per SM
       return launch_tc<128, false, 2>(d_probs, nprob, total_tiles, c_override, sms, err, st,
-                                      single, map_a, map_b, map_a2, map_a3, map_c);
+                                      single, map_a, map_b, map_a2, map_a3, map_c, false);
     case 131:  // 128 wide halo image tiles, resident weights
       return launch_tc<128, false, 1, true>(d_probs, nprob, total_tiles, c_override, sms, err,
-                                            st, single, map_a, map_b, map_a2, map_a3, map_c);
+                                            st, single, map_a, map_b, map_a2, map_a3, map_c,
+                                            false);
     case 258:  // 256 x 256 tiles on CTA pairs (plain operands, B' boxes of 128 rows)
       if (c_override) return cudaErrorInvalidValue;
       return launch_pair(d_probs, nprob, total_tiles, err, st, single, map_a, map_b, map_c);

@@ -1376,6 +1376,7 @@ struct ltb_batch {
   LtbTcProblem* d_tc[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   int ntc[6] = {0, 0, 0, 0, 0, 0};
   int64_t tc_tiles[6] = {0, 0, 0, 0, 0, 0};
+  int tc_tma[6] = {0, 0, 0, 0, 0, 0};  // a problem of the group has a TMA-stored output
   LtbGemmProblem* d_simt = nullptr;
   int64_t* d_simt_start = nullptr;
   int64_t simt_tiles = 0;
@@ -1402,9 +1403,9 @@ int group_of(const GemmTables& t) {
 void batch_gemms(ltb_batch* b, cudaStream_t st) {
   for (int g = 0; g < kGroups; ++g)
     if (b->ntc[g])
-      CUDA_TRY(ltb_launch_gemm_tc(kGroupCode[g], b->d_tc[g], b->ntc[g],
-                                  b->tc_tiles[g], nullptr,
-                                  b->sms, b->d_err, st));
+      CUDA_TRY(ltb_launch_gemm_tc(kGroupCode[g], b->d_tc[g], b->ntc[g], b->tc_tiles[g], nullptr,
+                                  b->sms, b->d_err, st, nullptr, nullptr, nullptr, nullptr,
+                                  nullptr, nullptr, b->tc_tma[g]));
 }
 
 void batch_launch(ltb_batch* b, cudaStream_t st) {
@@ -1529,6 +1530,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         LtbTcProblem q = t.prob;
         q.c_tma = t.c_tma && aligned16(p.c + t.c_row0) ? 1 : 0;
         if (q.c_tma) CUDA_TRY(ltb_make_tmap_c(m + 512, p.c + t.c_row0, p.M, p.N, t.c_ld));
+        b->tc_tma[grp] |= q.c_tma;
         q.c = p.c;
         q.crow = t.c_row;
         q.ccol = t.c_col;

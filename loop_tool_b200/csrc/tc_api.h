@@ -133,10 +133,12 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
 // c_override, if not null, replaces every problem's output pointer.
 // d_probs == nullptr: a single problem passed by value with its tensor maps
 // (host copies, passed as kernel parameters; no map_c: row stores).
+// c_tma_any: some problem of d_probs has c_tma set (the launch reserves the
+// TMA-store staging).
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single = nullptr,
                                const void* map_a = nullptr, const void* map_b = nullptr,
                                const void* map_a2 = nullptr, const void* map_a3 = nullptr,
-                               const void* map_c = nullptr);
+                               const void* map_c = nullptr, int c_tma_any = 0);
 int ltb_tc_tile_m();
