@@ -1236,9 +1236,11 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
 // reads the 64 channel rows of x (coalesced along w) into shared memory and
 // writes the padded row [wp, 64] of BF16 channel pairs (coalesced along c)
 // into the hi image, and into the lo and lo2 images when the job has them.
-// The reads of a 160-column chunk are all issued before any is stored, so
-// each thread has up to 40 loads in flight.
-constexpr int kImgChunkJ = 5;  // 32-column slices per chunk
+// The reads of a chunk of CJ 32-column slices are all issued before any is
+// stored (8 x CJ loads in flight per thread); CJ = ceil(wp / 32) up to 5,
+// so a narrow image keeps no idle slices and few registers, and more of its
+// rows are in flight on an SM.
+template <int CJ>
 __device__ __forceinline__ void pack_image_row(const LtbImageJob& J, int cb, int h, int n,
                                                float* tile /* [64][wp + 1] */) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1248,12 +1250,12 @@ __device__ __forceinline__ void pack_image_row(const LtbImageJob& J, int cb, int
   // warp per channel row (8 rows per warp), lanes along the columns
   const float* src = J.base + J.off + (int64_t)n * J.ns + (int64_t)(cb * 64 + warp) * J.cs +
                      (int64_t)h * J.wx;
-  for (int w0 = 0; w0 < J.wp; w0 += 32 * kImgChunkJ) {
-    float v[8][kImgChunkJ];
+  for (int w0 = 0; w0 < J.wp; w0 += 32 * CJ) {
+    float v[8][CJ];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < kImgChunkJ; ++j) {
+      for (int j = 0; j < CJ; ++j) {
         const int w = w0 + lane + 32 * j, ws = w + J.off_w;
         v[i][j] = row_ok && w < J.wp && ws >= 0 && ws < J.ub_w
                       ? __ldg(src + (int64_t)(8 * i) * J.cs + w)
@@ -1262,7 +1264,7 @@ __device__ __forceinline__ void pack_image_row(const LtbImageJob& J, int cb, int
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < kImgChunkJ; ++j) {
+      for (int j = 0; j < CJ; ++j) {
         const int w = w0 + lane + 32 * j;
         if (w < J.wp) tile[(warp + 8 * i) * pitch + w] = v[i][j];
       }
@@ -1293,15 +1295,20 @@ __device__ __forceinline__ void pack_image_row(const LtbImageJob& J, int cb, int
   }
 }
 
+template <int CJ>
 __global__ void __launch_bounds__(256) k_pack_image(const __grid_constant__ LtbImageJob J) {
   extern __shared__ float tile[];  // [64][wp + 1]
-  pack_image_row(J, blockIdx.x, blockIdx.y, blockIdx.z, tile);
+  pack_image_row<CJ>(J, blockIdx.x, blockIdx.y, blockIdx.z, tile);
 }
+
+// 32-column slices per repack chunk for a padded width
+inline int image_chunk_slices(int wp) { return wp <= 32 ? 1 : wp <= 64 ? 2 : wp <= 128 ? 4 : 5; }
 
 // A convolution's two operands in one launch: the first nb CTAs pack the
 // weight tiles (B'), the rest repack one image row each; the small weight
 // job runs beside the image instead of as a launch of its own.
-__global__ void __launch_bounds__(256, 3)
+template <int CJ>
+__global__ void __launch_bounds__(256, CJ <= 2 ? 5 : 3)
     k_pack_conv(const __grid_constant__ LtbImageJob J, const __grid_constant__ LtbPackJob JB,
                 int64_t b_tiles, int nb) {
   extern __shared__ float tile[];  // image: [64][wp + 1]; weights: [64][65]
@@ -1314,7 +1321,7 @@ __global__ void __launch_bounds__(256, 3)
     return;
   }
   const int cblocks = J.c / 64, r = (b - nb) / cblocks;
-  pack_image_row(J, (b - nb) - r * cblocks, r % J.hp, r / J.hp, tile);
+  pack_image_row<CJ>(J, (b - nb) - r * cblocks, r % J.hp, r / J.hp, tile);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -1400,13 +1407,23 @@ bool ltb_tc_halo_geometry(LtbTcProblem& p, int wp) {
 cudaError_t ltb_launch_pack_image(const LtbImageJob& j, cudaStream_t st) {
   if (j.c % 64 || j.wp < 1 || j.wp > 1024) return cudaErrorInvalidValue;
   const size_t smem = (size_t)64 * (j.wp + 1) * sizeof(float);
-  if (smem > 48 * 1024) {
-    const cudaError_t e = ltb_smem_optin((const void*)k_pack_image, smem);
-    if (e != cudaSuccess) return e;
+  const dim3 grid((unsigned)(j.c / 64), (unsigned)j.hp, (unsigned)j.nimg);
+#define LTB_IMG(CJ)                                                                       \
+  {                                                                                       \
+    if (smem > 48 * 1024) {                                                               \
+      const cudaError_t e = ltb_smem_optin((const void*)k_pack_image<CJ>, smem);          \
+      if (e != cudaSuccess) return e;                                                     \
+    }                                                                                     \
+    k_pack_image<CJ><<<grid, 256, smem, st>>>(j);                                         \
+    return cudaGetLastError();                                                            \
   }
-  dim3 grid((unsigned)(j.c / 64), (unsigned)j.hp, (unsigned)j.nimg);
-  k_pack_image<<<grid, 256, smem, st>>>(j);
-  return cudaGetLastError();
+  switch (image_chunk_slices(j.wp)) {
+    case 1: LTB_IMG(1)
+    case 2: LTB_IMG(2)
+    case 4: LTB_IMG(4)
+    default: LTB_IMG(5)
+  }
+#undef LTB_IMG
 }
 
 static LtbPackJob make_pack_job(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
@@ -1423,12 +1440,22 @@ cudaError_t ltb_launch_pack_conv(const LtbImageJob& j, const LtbGemmOperand& bop
   if (img_ctas + nb > 0x7fffffff) return cudaErrorInvalidValue;
   size_t smem = (size_t)64 * (j.wp + 1) * sizeof(float);
   if (smem < (size_t)PKT * (PR + 1) * sizeof(float)) smem = (size_t)PKT * (PR + 1) * sizeof(float);
-  if (smem > 40 * 1024) {  // 48 KB less the static pack tables
-    const cudaError_t e = ltb_smem_optin((const void*)k_pack_conv, smem);
-    if (e != cudaSuccess) return e;
+#define LTB_CONV(CJ)                                                                      \
+  {                                                                                       \
+    if (smem > 40 * 1024) { /* 48 KB less the static pack tables */                       \
+      const cudaError_t e = ltb_smem_optin((const void*)k_pack_conv<CJ>, smem);           \
+      if (e != cudaSuccess) return e;                                                     \
+    }                                                                                     \
+    k_pack_conv<CJ><<<(unsigned)(img_ctas + nb), 256, smem, st>>>(j, JB, b_tiles, nb);    \
+    return cudaGetLastError();                                                            \
   }
-  k_pack_conv<<<(unsigned)(img_ctas + nb), 256, smem, st>>>(j, JB, b_tiles, nb);
-  return cudaGetLastError();
+  switch (image_chunk_slices(j.wp)) {
+    case 1: LTB_CONV(1)
+    case 2: LTB_CONV(2)
+    case 4: LTB_CONV(4)
+    default: LTB_CONV(5)
+  }
+#undef LTB_CONV
 }
 
 int ltb_tc_tile_m() { return BM; }
