@@ -290,7 +290,7 @@ def tune_batch(members, capture_stream=None, reps=3):
     # then the grouped packing's launch shape (chunk of tiles, CTAs per SM)
     b = Batch(members)
     pack = {}
-    for chunk, per_sm in ((4, 4), (1, 4), (16, 4), (64, 4), (16, 2), (64, 8)):
+    for chunk, per_sm in ((4, 4), (1, 4), (16, 4), (64, 4), (16, 2), (4, 6), (16, 6), (64, 8)):
         b.set_schedule(chunk, per_sm)
         b.run_timed()
         pack[(chunk, per_sm)] = min(b.run_timed()[0] for _ in range(reps))

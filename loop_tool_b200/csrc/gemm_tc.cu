@@ -1047,6 +1047,9 @@ __device__ __forceinline__ void gather_fill(const LtbPackJob& J, const PackTable
   }
 }
 
+// kDense: the dense modes alone (a launch whose every job is dense); the
+// gather branch is compiled out, so the kernel fits more CTAs per SM.
+template <bool kDense>
 __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
                                           float (*sm)[PR + 1], PackTables* tabs) {
   const int tid = threadIdx.x;
@@ -1091,7 +1094,7 @@ __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
           v = __ldg(reinterpret_cast<const float4*>(J.op.base + k * J.op.ld_k + r));
         sm[kl][rl] = v.x; sm[kl][rl + 1] = v.y; sm[kl][rl + 2] = v.z; sm[kl][rl + 3] = v.w;
       }
-    } else {
+    } else if constexpr (!kDense) {
       // guarded gather: the tile's row and k tables staged in shared memory
       // (offsets and guard partials), so each element costs one global load
       PackTables& tb = *tabs;
@@ -1169,22 +1172,38 @@ __device__ __forceinline__ void tile_range(int64_t total, int64_t& t0, int64_t& 
   t1 = total * (blockIdx.x + 1) / gridDim.x;
 }
 
-__global__ void __launch_bounds__(PACK_THREADS, 4)
+// Dense launches can hold 6 CTAs per SM (40 registers, no spills), half as
+// many loads again in flight as the general form's 4; single-segment (BF16)
+// packing runs them (8192^2 operands: 156 -> 137 us), the split modes, whose
+// stores outnumber their loads, keep 4 (measured slower with 6).
+constexpr int kPackCtasDense = 6, kPackCtas = 4;
+
+template <bool kDense>
+__global__ void __launch_bounds__(PACK_THREADS, kDense ? kPackCtasDense : kPackCtas)
     k_pack_one(const __grid_constant__ LtbPackJob J, int64_t total_tiles) {
   __shared__ float sm[PKT][PR + 1];
-  __shared__ PackTables tabs;
+  PackTables* tabs = nullptr;  // the gather tables (general form only)
+  if constexpr (!kDense) {
+    __shared__ PackTables tb;
+    tabs = &tb;
+  }
   int64_t t0, t1;
   tile_range(total_tiles, t0, t1);
-  for (int64_t t = t0; t < t1; ++t) pack_tile(J, t, sm, &tabs);
+  for (int64_t t = t0; t < t1; ++t) pack_tile<kDense>(J, t, sm, tabs);
 }
 
 // Every operand of a batch in one launch; the job of a tile is found by
 // binary search on tile_start once per CTA, then by stepping forward.
-__global__ void __launch_bounds__(PACK_THREADS, 4)
+template <bool kDense>
+__global__ void __launch_bounds__(PACK_THREADS, kDense ? kPackCtasDense : kPackCtas)
     k_pack_grouped(const LtbPackJob* __restrict__ jobs, int njobs, int64_t total_tiles,
                    int kGroupChunk) {
   __shared__ float sm[PKT][PR + 1];
-  __shared__ PackTables tabs;
+  PackTables* tabs = nullptr;  // the gather tables (general form only)
+  if constexpr (!kDense) {
+    __shared__ PackTables tb;
+    tabs = &tb;
+  }
   __shared__ LtbPackJob sj;  // the current job, read from shared memory
   // chunks of kGroupChunk consecutive tiles dealt round-robin to the CTAs:
   // every CTA sees a mix of the jobs (fast and slow layouts alike), and its
@@ -1227,7 +1246,7 @@ __global__ void __launch_bounds__(PACK_THREADS, 4)
       // a register copy of the job: fields read through shared memory on
       // every use cost the tile loop a quarter of its speed
       const LtbPackJob Jl = sj;
-      pack_tile(Jl, t - Jl.tile_start, sm, &tabs);
+      pack_tile<kDense>(Jl, t - Jl.tile_start, sm, tabs);
     }
   }
 }
@@ -1317,7 +1336,7 @@ __global__ void __launch_bounds__(256, CJ <= 2 ? 5 : 3)
   if (b < nb) {
     const int64_t t0 = b_tiles * b / nb, t1 = b_tiles * (b + 1) / nb;
     for (int64_t t = t0; t < t1; ++t)
-      pack_tile(JB, t, reinterpret_cast<float (*)[PR + 1]>(tile), &tabs);
+      pack_tile<false>(JB, t, reinterpret_cast<float (*)[PR + 1]>(tile), &tabs);
     return;
   }
   const int cblocks = J.c / 64, r = (b - nb) / cblocks;
@@ -1473,10 +1492,12 @@ int64_t ltb_pack_tiles(int64_t rows, int64_t K) {
   return ((rows + PR - 1) / PR) * ((K + PKT - 1) / PKT);
 }
 
-static int64_t pack_grid(int64_t tiles, int sms) {
-  const int64_t g = (int64_t)sms * 4;
+static int64_t pack_grid(int64_t tiles, int sms, bool dense_one_segment) {
+  const int64_t g = (int64_t)sms * (dense_one_segment ? kPackCtasDense : kPackCtas);
   return tiles < g ? tiles : g;
 }
+
+static bool pack_dense(int mode) { return mode == kPackDenseK || mode == kPackDenseR; }
 
 static LtbPackJob make_pack_job(const LtbGemmOperand& op, int64_t rows, int64_t K, void* out,
                                 int64_t Kp, int nseg, int seg_mask, int k_contig, int off32) {
@@ -1500,18 +1521,31 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
   const LtbPackJob J = make_pack_job(op, rows, K, out, Kp, nseg, seg_mask, k_contig, off32);
   const int64_t tiles = ltb_pack_tiles(rows, K);
   if (tiles == 0) return cudaSuccess;
-  k_pack_one<<<(unsigned)pack_grid(tiles, sms), PACK_THREADS, 0, st>>>(J, tiles);
+  if (pack_dense(J.mode))
+    k_pack_one<true><<<(unsigned)pack_grid(tiles, sms, nseg == 1), PACK_THREADS, 0, st>>>(J,
+                                                                                       tiles);
+  else
+    k_pack_one<false><<<(unsigned)pack_grid(tiles, sms, false), PACK_THREADS, 0, st>>>(J, tiles);
   return cudaGetLastError();
 }
 
 cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t total_tiles,
-                                    int sms, cudaStream_t st, int chunk, int cta_per_sm) {
+                                    int sms, cudaStream_t st, int chunk, int cta_per_sm,
+                                    int all_dense, int all_one_segment) {
   if (total_tiles == 0) return cudaSuccess;
   if (chunk < 1) chunk = 4;
   const int64_t chunks = (total_tiles + chunk - 1) / chunk;
-  const int64_t cap = (int64_t)sms * (cta_per_sm > 0 ? cta_per_sm : 4);
+  const int per_sm = cta_per_sm > 0                        ? cta_per_sm
+                     : all_dense && all_one_segment ? kPackCtasDense
+                                                            : kPackCtas;
+  const int64_t cap = (int64_t)sms * per_sm;
   const int64_t grid = chunks < cap ? chunks : cap;
-  k_pack_grouped<<<(unsigned)grid, PACK_THREADS, 0, st>>>(d_jobs, njobs, total_tiles, chunk);
+  if (all_dense)
+    k_pack_grouped<true><<<(unsigned)grid, PACK_THREADS, 0, st>>>(d_jobs, njobs, total_tiles,
+                                                                  chunk);
+  else
+    k_pack_grouped<false><<<(unsigned)grid, PACK_THREADS, 0, st>>>(d_jobs, njobs, total_tiles,
+                                                                   chunk);
   return cudaGetLastError();
 }
 

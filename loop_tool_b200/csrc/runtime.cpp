@@ -1370,6 +1370,8 @@ struct ltb_batch {
   int njobs = 0;
   int64_t pack_tiles = 0;
   int pack_chunk = 0, pack_cta_per_sm = 0;  // grouped pack schedule (0: defaults)
+  bool pack_dense = false;  // every pack job of a dense mode (the faster kernel)
+  bool pack_one_seg = false;  // every pack job with one segment (plain BF16)
   std::vector<LtbImageJob> img_jobs;        // image operands, repacked before the pack
   // tensor-core problems grouped by schedule variant (kGroupCode), one
   // persistent launch per non-empty group
@@ -1412,7 +1414,7 @@ void batch_launch(ltb_batch* b, cudaStream_t st) {
   if (b->tc) {
     for (const auto& j : b->img_jobs) CUDA_TRY(ltb_launch_pack_image(j, st));
     CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st, b->pack_chunk,
-                                     b->pack_cta_per_sm));
+                                     b->pack_cta_per_sm, b->pack_dense, b->pack_one_seg));
     batch_gemms(b, st);
   } else {
     CUDA_TRY(ltb_launch_gemm_simt_grouped(b->d_simt, b->d_simt_start, b->n, b->simt_tiles,
@@ -1548,6 +1550,11 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     }
     b->njobs = (int)jobs.size();
     if (b->tc) {
+      b->pack_dense = b->pack_one_seg = true;
+      for (const auto& j : jobs) {
+        b->pack_dense = b->pack_dense && (j.mode == kPackDenseK || j.mode == kPackDenseR);
+        b->pack_one_seg = b->pack_one_seg && j.nseg == 1;
+      }
       b->d_jobs = upload(jobs, b->owned);
       for (int g = 0; g < kGroups; ++g) {
         // tensor maps in device memory (cudaMalloc is 256-byte aligned)
@@ -1648,7 +1655,8 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
     for (const auto& j : b->img_jobs) CUDA_TRY(ltb_launch_pack_image(j, st));
     if (b->tc)
       CUDA_TRY(ltb_launch_pack_grouped(b->d_jobs, b->njobs, b->pack_tiles, b->sms, st,
-                                       b->pack_chunk, b->pack_cta_per_sm));
+                                       b->pack_chunk, b->pack_cta_per_sm, b->pack_dense,
+                                       b->pack_one_seg));
     CUDA_TRY(cudaEventRecord(e1, st));
     if (b->tc)
       batch_gemms(b, st);
@@ -1702,7 +1710,10 @@ int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   else if (k == "tiles_256") *value = b->tc_tiles[2] + b->tc_tiles[3];
   else if (k == "graph") *value = b->exec ? 1 : 0;
   else if (k == "pack_chunk") *value = b->pack_chunk ? b->pack_chunk : 4;
-  else if (k == "pack_cta_per_sm") *value = b->pack_cta_per_sm ? b->pack_cta_per_sm : 4;
+  else if (k == "pack_cta_per_sm")
+    *value = b->pack_cta_per_sm  ? b->pack_cta_per_sm
+             : b->pack_dense && b->pack_one_seg ? 6
+                                                 : 4;
   else return fail(LTB_ERR_INVALID, "unknown property " + k);
   return LTB_OK;
 }

@@ -107,9 +107,12 @@ struct LtbPackJob {
 int ltb_pack_mode(const LtbGemmOperand& op, int64_t rows, int64_t K, int k_contig);
 int64_t ltb_pack_tiles(int64_t rows, int64_t K);
 // Tiles are dealt to the CTAs in round-robin chunks of `chunk` consecutive
-// tiles (0: 4); grid = SMs x cta_per_sm CTAs (0: 4).
+// tiles (0: 4); grid = SMs x cta_per_sm CTAs (0: 4, or 6 when every job is
+// of a dense mode with one segment).  all_dense selects the kernel without
+// the gather path.
 cudaError_t ltb_launch_pack_grouped(const LtbPackJob* d_jobs, int njobs, int64_t total_tiles,
-                                    int sms, cudaStream_t st, int chunk = 0, int cta_per_sm = 0);
+                                    int sms, cudaStream_t st, int chunk = 0, int cta_per_sm = 0,
+                                    int all_dense = 0, int all_one_segment = 0);
 
 // CUtensorMap (128 bytes, 64-byte aligned) over a K-major BF16 matrix
 // [rows, Kp] (Kp a multiple of 8 so the row pitch is 16-byte aligned),

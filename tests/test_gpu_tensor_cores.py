@@ -284,10 +284,11 @@ def test_conv_implicit_every_variant(variant, cuda_dev):
 # Halo image tiles (variant 131, BF16): one TMA box per kernel row covers the
 # tile's padded image rows; the kw shifts are read in place at row offsets
 # inside the 128-byte swizzle atoms; the weights stay in shared memory.
-# Shapes: partial last row group, several images, a 2 x 2 kernel, and the
-# 56 x 56 image with 128 output channels.  (N, C, H, W, CO, K, pad)
+# Shapes: partial last row group, several images, a 2 x 2 kernel, two
+# channel blocks, and the 56 x 56 image with 128 output channels.
+# (N, C, H, W, CO, K, pad)
 HALO = [(2, 64, 8, 8, 16, 3, 1), (2, 64, 16, 16, 40, 3, 1), (2, 64, 17, 17, 24, 2, 0),
-        (4, 64, 32, 32, 128, 3, 1), (1, 64, 56, 56, 128, 3, 1)]
+        (2, 128, 15, 15, 32, 2, 1), (4, 64, 32, 32, 128, 3, 1), (1, 64, 56, 56, 128, 3, 1)]
 
 
 @pytest.mark.gpu
