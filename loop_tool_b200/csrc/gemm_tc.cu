@@ -49,6 +49,7 @@
 
 #include <map>
 #include <mutex>
+#include <tuple>
 
 #include "async.cuh"
 #include "kernels.h"
@@ -443,19 +444,29 @@ __global__ void __launch_bounds__(NT, CTAS)
     // halo problems keep the default chunk (a compile-time divisor: this
     // single issuing thread is on the MMA's critical path)
     constexpr int cbk = kChunkBlocks;
+    // the problem's fields in registers, and the operand descriptors of the
+    // (kh, kw) shifts stepped by constants (16-byte units: one padded image
+    // row per kh, one pixel per kw, the channel blocks' weight blocks per
+    // shift): few instructions between this thread's MMAs
+    const int khn = p.img_kh, kwn = p.img_kw, ncb = p.img_cblocks;
+    const uint64_t a_kh = (uint64_t)p.img_slot * 8u;
+    const uint64_t b_blk = (uint64_t)(T::B_BYTES >> 4), b_shift = (uint64_t)ncb * b_blk;
+    const uint64_t b0 = sw128_desc(smem_u32(bres));
     for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
       int issued = 0, buf = 0;
       uint32_t acc = tmem;
-      for (int cb = 0; cb < p.img_cblocks && alive; ++cb, ++g) {
+      for (int cb = 0; cb < ncb && alive; ++cb, ++g) {
         const int s = (int)(g % (uint32_t)nst);
         if (!mbar_wait(smem_u32(&full[s]), (g / (uint32_t)nst) & 1u, err)) {
           alive = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a_slot = smem_u32(ring + (size_t)s * slot_bytes);
-        for (int kh = 0; kh < p.img_kh && alive; ++kh)
-          for (int kw = 0; kw < p.img_kw; ++kw) {
+        uint64_t arow = sw128_desc(smem_u32(ring + (size_t)s * slot_bytes));
+        uint64_t bd = b0 + (uint64_t)cb * b_blk;
+        int kb = cb;  // (kh * kw_n + kw) * cblocks + cb
+        for (int kh = 0; kh < khn && alive; ++kh, arow += a_kh)
+          for (int kw = 0; kw < kwn; ++kw, bd += b_shift, kb += ncb) {
             if (issued % cbk == 0) {  // a new accumulation chunk
               buf = (int)(q & 1u);
               if (!mbar_wait(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
@@ -465,15 +476,13 @@ __global__ void __launch_bounds__(NT, CTAS)
               asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
               acc = tmem + (uint32_t)(buf * BN);
             }
-            const int kb = (kh * p.img_kw + kw) * p.img_cblocks + cb;
             if (first && !mbar_wait(smem_u32(&b_full[kb]), 0u, err)) {
               alive = false;
               break;
             }
             // shift (kh, kw): tile row i * wp + w reads box row
-            // (i + kh) * wp + (w + kw)
-            const uint64_t ad = sw128_desc(a_slot + (uint32_t)(kh * p.img_slot + kw) * 128u);
-            const uint64_t bd = sw128_desc(smem_u32(bres + (size_t)kb * T::B_BYTES));
+            // (i + kh) * wp + (w + kw), 128 bytes a row
+            const uint64_t ad = arow + 8u * (uint64_t)kw;
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk)
               mma_bf16(acc, ad + 2 * kk, bd + 2 * kk, T::IDESC,
@@ -917,6 +926,239 @@ __global__ void __launch_bounds__(NT, 1)
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kPairTmemCols));
+}
+
+// ------------------------------------------------- halo tiles on CTA pairs
+// The halo image tiles (weights resident, one 4-D box per tile and channel
+// block, every (kh, kw) shift read in place) on a cluster of two CTAs:
+// tcgen05.mma.cta_group::2 with M = 256 (the two CTAs' 128-row tiles) and N
+// = 128.  CTA rank r holds the box of m-tile 2 pt + r and rows 64 r .. 64 r
+// + 63 of every weight block (half of the resident B', 8 KB a block), so
+// each SM moves 6 KB of operands per 128 x 128 x 16 product instead of 8
+// KB, and loads half of the weights.
+//   warp 0 lane 0 (both CTAs): producer; its box and weight loads complete
+//     on the leader's barriers, which alone expect both CTAs' bytes
+//   warp 1 lane 0 (leader): MMA issuer; commits arrive on the barrier at
+//     the same offset in both CTAs (empty[s], chunk_full[b])
+//   warps 2..9 (both CTAs): drain + epilogue of the CTA's 128 rows; their
+//     chunk_empty arrivals go to the leader's barrier (2 x 256 a phase)
+// An odd last m-tile pairs with a tile past the end: its box reads zeros
+// (coordinates past the image) and its rows are not written.
+constexpr int kPairHaloBBytes = 64 * BK * 2;  // this CTA's half of a weight block
+constexpr uint32_t kPairHaloTmemCols = 256;   // two 128-column accumulators
+// kind::f16: FP32 accumulator, BF16 A and B, both K-major, M = 256, N = 128
+constexpr uint32_t kPairHaloIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((256u >> 4) << 24);
+
+__device__ __forceinline__ void tma_load_4d_pair(uint32_t dst, const CUtensorMap* map,
+                                                 uint32_t bar, int x, int y, int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void mma_bf16_pair_n128(uint32_t tmem_d, uint64_t a, uint64_t b,
+                                                   uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(kPairHaloIdesc), "r"(accumulate));
+}
+
+// Shared memory of a pair-halo CTA: its weight halves, the box ring and the
+// barriers (full/empty per slot, one per weight block, 2 + 2 chunk
+// barriers, the TMEM address word).
+__host__ __device__ inline size_t pair_halo_fixed_bytes(int kbt) {
+  return (size_t)kbt * kPairHaloBBytes + 1024 + (size_t)(2 * kMaxHaloStages + kbt + 4) * 8 + 8;
+}
+
+__global__ void __launch_bounds__(NT, 1)
+    k_gemm_tc_pair_halo(int64_t pair_tiles, int* err, const __grid_constant__ LtbTcProblem single,
+                        const __grid_constant__ CUtensorMap single_a,
+                        const __grid_constant__ CUtensorMap single_b) {
+  const LtbTcProblem& p = single;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int kbt = (int)(p.Kp / BK), nst = p.img_stages;
+  const uint32_t slot_bytes = (uint32_t)p.img_slot_bytes;
+  uint8_t* bres = smem;  // weight block kb's half at bres + kb * 8 KB
+  uint8_t* ring = smem + (size_t)kbt * kPairHaloBBytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)nst * slot_bytes);
+  uint64_t* empty = full + nst;
+  uint64_t* b_full = empty + nst;            // [kbt] (the leader's count both halves)
+  uint64_t* chunk_full = b_full + kbt;       // [2] MMA -> drain (both CTAs)
+  uint64_t* chunk_empty = chunk_full + 2;    // [2] drain -> MMA (the leader's)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(chunk_empty + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < nst; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);   // the leader's expect_tx
+      mbar_init(smem_u32(&empty[s]), 1);  // one commit
+    }
+    for (int kb = 0; kb < kbt; ++kb) mbar_init(smem_u32(&b_full[kb]), 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&chunk_full[b]), 1);
+      mbar_init(smem_u32(&chunk_empty[b]), 2 * 8 * 32);  // both CTAs' drain threads
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {  // the same warp in both CTAs allocates for the pair
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kPairHaloTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  cluster_sync_all();  // both CTAs' barriers initialised and TMEM allocated
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const int64_t first = cluster_index(), step = cluster_count();
+  const int ncb = p.img_cblocks, nsh = p.img_kh * p.img_kw;
+
+  if (warp == 0 && lane == 0) {
+    // ------------------------------------------------------------ producer
+    const uint32_t box_bytes = (uint32_t)((p.img_rows + p.img_kh - 1) * p.img_slot * 128);
+    bool first_tile = true;  // the first tile also loads the weight halves, in first-use order
+    uint32_t g = 0;          // stages issued
+    bool alive = true;
+    for (int64_t pt = first; pt < pair_tiles && alive; pt += step) {
+      const int mt = (int)(2 * pt) + (int)rank;  // halo tiles: one column of tiles, no raster
+      const int n_img = mt / p.img_hgroups;
+      const int ho0 = (mt - n_img * p.img_hgroups) * p.img_rows;
+      for (int cb = 0; cb < ncb; ++cb, ++g) {
+        const int s = (int)(g % (uint32_t)nst);
+        if (!mbar_wait_cl(smem_u32(&empty[s]), ((g / (uint32_t)nst) & 1u) ^ 1u, err)) {
+          alive = false;
+          break;
+        }
+        if (first_tile)
+          for (int sh = 0; sh < nsh; ++sh) {
+            const int kb = sh * ncb + cb;
+            const uint32_t bb = smem_u32(&b_full[kb]);
+            if (leader) mbar_expect_tx(bb, 2u * kPairHaloBBytes);
+            tma_load_2d_pair(smem_u32(bres + (size_t)kb * kPairHaloBBytes), &single_b,
+                             rank0_addr(bb), kb * BK, 64 * (int)rank);
+          }
+        const uint32_t fb = smem_u32(&full[s]);
+        if (leader) mbar_expect_tx(fb, 2u * box_bytes);
+        tma_load_4d_pair(smem_u32(ring + (size_t)s * slot_bytes), &single_a, rank0_addr(fb),
+                         cb * 64, 0, ho0, n_img);
+      }
+      first_tile = false;
+    }
+    // both CTAs' loads complete on the leader's barriers: the leader waits
+    // for the last round of each slot and the weight blocks loaded (those
+    // of the first tile's first g channel blocks); the closing cluster
+    // barrier holds the peer until then
+    if (leader) {
+      for (uint32_t i = g > (uint32_t)nst ? g - nst : 0; i < g; ++i)
+        mbar_drain(smem_u32(&full[i % nst]), (i / nst) & 1u);
+      for (int kb = 0; kb < kbt; ++kb)
+        if ((uint32_t)(kb % ncb) < g) mbar_drain(smem_u32(&b_full[kb]), 0u);
+    }
+  } else if (warp == 1 && lane == 0 && leader) {
+    // ---------------------------------------------------------- MMA issuer
+    uint32_t g = 0, q = 0;  // stages consumed, chunks produced
+    bool alive = true;
+    bool first_tile = true;  // weight blocks are waited for on first use
+    constexpr int cbk = kChunkBlocks;
+    const uint64_t a_kh = (uint64_t)p.img_slot * 8u;  // descriptor steps, 16-byte units
+    const uint64_t b_blk = (uint64_t)(kPairHaloBBytes >> 4), b_shift = (uint64_t)ncb * b_blk;
+    const uint64_t b0 = sw128_desc(smem_u32(bres));
+    for (int64_t pt = first; pt < pair_tiles && alive; pt += step) {
+      int issued = 0, buf = 0;
+      uint32_t acc = tmem;
+      for (int cb = 0; cb < ncb && alive; ++cb, ++g) {
+        const int s = (int)(g % (uint32_t)nst);
+        if (!mbar_wait_cl(smem_u32(&full[s]), (g / (uint32_t)nst) & 1u, err)) {
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint64_t arow = sw128_desc(smem_u32(ring + (size_t)s * slot_bytes));
+        uint64_t bd = b0 + (uint64_t)cb * b_blk;
+        int kb = cb;
+        for (int kh = 0; kh < p.img_kh && alive; ++kh, arow += a_kh)
+          for (int kw = 0; kw < p.img_kw; ++kw, bd += b_shift, kb += ncb) {
+            if (issued % cbk == 0) {  // a new accumulation chunk
+              buf = (int)(q & 1u);
+              if (!mbar_wait_cl(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
+                alive = false;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+              acc = tmem + (uint32_t)(buf * 128);
+            }
+            if (first_tile && !mbar_wait_cl(smem_u32(&b_full[kb]), 0u, err)) {
+              alive = false;
+              break;
+            }
+            const uint64_t ad = arow + 8u * (uint64_t)kw;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+              mma_bf16_pair_n128(acc, ad + 2 * kk, bd + 2 * kk, (issued % cbk != 0) || (kk != 0));
+            ++issued;
+            if (issued % cbk == 0 || issued == kbt) {
+              mma_commit_pair(smem_u32(&chunk_full[buf]));  // chunk complete in both TMEMs
+              ++q;
+            }
+          }
+        mma_commit_pair(smem_u32(&empty[s]));  // both CTAs' slot s reusable
+      }
+      first_tile = false;
+    }
+  } else if (warp >= 2) {
+    // ------------------------------------------------------ drain/epilogue
+    const int quad = warp & 3, half = (warp - 2) >> 2;
+    uint32_t q = 0;
+    bool alive = true;
+    for (int64_t pt = first; pt < pair_tiles && alive; pt += step) {
+      const int mt = (int)(2 * pt) + (int)rank;
+      const int m0 = mt * BM;
+      int row;
+      const bool rvalid = mt < p.tiles_m && tile_row(p, m0, quad * 32 + lane, &row);
+      const int64_t rbase = rvalid ? p.crow[row] : 0;
+      float run[64];
+#pragma unroll
+      for (int i = 0; i < 64; ++i) run[i] = 0.f;
+      for (int c0 = 0; c0 < kbt; c0 += kChunkBlocks, ++q) {
+        const int buf = q & 1;
+        const bool ok = mbar_wait_cl(smem_u32(&chunk_full[buf]), (q >> 1) & 1u, err);
+        if (!__all_sync(0xffffffffu, ok)) {
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t base =
+            tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(buf * 128 + half * 64);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          uint32_t r[32];
+          tmem_ld16(base + (uint32_t)(c * 32), r);
+          tmem_ld16(base + (uint32_t)(c * 32 + 16), r + 16);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 32; ++i) run[c * 32 + i] += __uint_as_float(r[i]);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive_remote(rank0_addr(smem_u32(&chunk_empty[buf])));  // buffer free
+      }
+      if (!alive) break;
+      write_tile<64, false, false>(p, nullptr, nullptr, run, nullptr, warp - 2, m0, half * 64,
+                                   rvalid, rbase);
+    }
+  }
+  __syncwarp();
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  cluster_sync_all();  // no MMA, commit or arrival of either CTA still in flight
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kPairHaloTmemCols));
 }
 
 // ------------------------------------------------------------ packing
@@ -1593,18 +1835,20 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
   return cudaGetLastError();
 }
 
-// Clusters of two CTAs the pair kernel can hold resident at once on a
-// device (its persistent grid): asked once per device.
-static int pair_clusters(int dev) {
+// Clusters of two CTAs a pair kernel can hold resident at once on a device
+// with this much dynamic shared memory (its persistent grid): asked once per
+// kernel, size and device.
+static int pair_clusters(const void* fn, size_t smem, int dev) {
   static std::mutex mu;
-  static std::map<int, int> known;
+  static std::map<std::tuple<const void*, size_t, int>, int> known;
   std::lock_guard<std::mutex> g(mu);
-  auto it = known.find(dev);
+  const auto key = std::make_tuple(fn, smem, dev);
+  auto it = known.find(key);
   if (it != known.end()) return it->second;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(2, 1, 1);
   cfg.blockDim = dim3(NT, 1, 1);
-  cfg.dynamicSmemBytes = kPairSmem;
+  cfg.dynamicSmemBytes = smem;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = 2;
@@ -1613,11 +1857,11 @@ static int pair_clusters(int dev) {
   cfg.attrs = at;
   cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_gemm_tc_pair, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) {
     cudaGetLastError();
     n = 0;
   }
-  known[dev] = n;
+  known[key] = n;
   return n;
 }
 
@@ -1633,7 +1877,7 @@ static cudaError_t launch_pair(const LtbTcProblem* d_probs, int nprob, int64_t t
     const cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
   }
-  int64_t clusters = pair_clusters(dev);
+  int64_t clusters = pair_clusters((const void*)k_gemm_tc_pair, kPairSmem, dev);
   if (clusters <= 0) return cudaErrorInvalidConfiguration;
   if (total_tiles < clusters) clusters = total_tiles;
   LtbTcProblem one{};
@@ -1662,6 +1906,51 @@ static cudaError_t launch_pair(const LtbTcProblem* d_probs, int nprob, int64_t t
                             mc);
 }
 
+// Halo tiles on CTA pairs: the halo problem with the ring re-sized for the
+// halved weight residency; tiles = its m-tiles, run two to a cluster.
+static cudaError_t launch_pair_halo(int64_t tiles, int* err, cudaStream_t st,
+                                    const LtbTcProblem* single, const void* map_a,
+                                    const void* map_b) {
+  if (!single || !single->img_halo || !map_a || !map_b || single->N > 128)
+    return cudaErrorInvalidValue;
+  LtbTcProblem one = *single;
+  const int kbt = (int)(one.Kp / BK);
+  const size_t fixed = pair_halo_fixed_bytes(kbt);
+  if (kbt > kMaxHaloKb || fixed + 2 * (size_t)one.img_slot_bytes > kHaloSmemMax)
+    return cudaErrorInvalidValue;
+  const int stages = (int)((kHaloSmemMax - fixed) / (size_t)one.img_slot_bytes);
+  one.img_stages = stages < kMaxHaloStages ? stages : kMaxHaloStages;
+  const size_t smem = fixed + (size_t)one.img_stages * (size_t)one.img_slot_bytes;
+  {
+    const cudaError_t e = ltb_smem_optin((const void*)k_gemm_tc_pair_halo, kHaloSmemMax);
+    if (e != cudaSuccess) return e;
+  }
+  int dev = 0;
+  {
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+  }
+  int64_t clusters = pair_clusters((const void*)k_gemm_tc_pair_halo, smem, dev);
+  if (clusters <= 0) return cudaErrorInvalidConfiguration;
+  const int64_t pair_tiles = (tiles + 1) / 2;
+  if (pair_tiles < clusters) clusters = pair_tiles;
+  const CUtensorMap ma = *static_cast<const CUtensorMap*>(map_a);
+  const CUtensorMap mb = *static_cast<const CUtensorMap*>(map_b);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(2 * clusters), 1, 1);
+  cfg.blockDim = dim3(NT, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_gemm_tc_pair_halo, pair_tiles, err, one, ma, mb);
+}
+
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single, const void* map_a,
@@ -1686,6 +1975,9 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
     case 258:  // 256 x 256 tiles on CTA pairs (plain operands, B' boxes of 128 rows)
       if (c_override) return cudaErrorInvalidValue;
       return launch_pair(d_probs, nprob, total_tiles, err, st, single, map_a, map_b, map_c);
+    case 133:  // halo image tiles on CTA pairs (M = 256, B' boxes of 64 rows)
+      if (c_override || d_probs) return cudaErrorInvalidValue;
+      return launch_pair_halo(total_tiles, err, st, single, map_a, map_b);
   }
 #undef LTB_TC
   return cudaErrorInvalidValue;

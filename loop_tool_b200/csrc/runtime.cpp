@@ -101,32 +101,36 @@ struct GemmTables {
   int bn = 256;                       // tensor-core tile width (128 or 256)
   int epi = 0;                        // 1: shared-memory transposed epilogue,
                                       // 2: two CTAs per SM, 3: halo image tiles,
-                                      // 4: 256 x 256 tiles on CTA pairs
+                                      // 4: 256 x 256 tiles on CTA pairs,
+                                      // 5: halo image tiles on CTA pairs
   // halo image tiles (single-segment image operands, N <= 128): the launch
   // template in halo geometry, valid when halo_ok
   LtbTcProblem halo{};
   bool halo_ok = false;
 };
 
+bool halo_form(int epi) { return epi == 3 || epi == 5; }
+
 // Tile form of a tensor-core contraction: output tiles are 128 x bn, or
-// 256 x 256 on CTA pairs (epi 4, plain operands).
+// 256 x 256 on CTA pairs (epi 4, plain operands); halo tiles (epi 3, 5) are
+// the halo geometry's m-tiles.
 void set_tile_n(GemmTables& t, int bn, int epi) {
-  if (epi == 3 && !(t.halo_ok && bn == 128)) epi = 0;
+  if (halo_form(epi) && !(t.halo_ok && bn == 128)) epi = 0;
   if (epi == 4 && (t.img || bn != 256)) epi = 0;
   t.bn = bn;
   t.epi = epi;
   if (!t.img) t.prob.tiles_m = (int)((t.prob.M + (epi == 4 ? 255 : 127)) / (epi == 4 ? 256 : 128));
   const int64_t tn = (t.prob.N + bn - 1) / bn;
   t.prob.tiles_n = (int)tn;
-  t.tiles = epi == 3 ? (int64_t)t.halo.tiles_m : (int64_t)t.prob.tiles_m * tn;
+  t.tiles = halo_form(epi) ? (int64_t)t.halo.tiles_m : (int64_t)t.prob.tiles_m * tn;
 }
 
 // Launch variant of a tile form (ltb_launch_gemm_tc, schedules): tile
-// width | form, or 258 for CTA pairs.
+// width | form (133: halo tiles on CTA pairs), or 258 for CTA pairs.
 int variant_code(const GemmTables& t) { return t.epi == 4 ? 258 : t.bn | t.epi; }
 
 // Rows of a B' tensor-map box: the tile width, or half of it on CTA pairs.
-int b_box_rows(const GemmTables& t) { return t.epi == 4 ? 128 : t.bn; }
+int b_box_rows(const GemmTables& t) { return t.epi == 4 ? 128 : t.epi == 5 ? 64 : t.bn; }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
@@ -781,7 +785,7 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           LtbImageJob j = image_job(t, p.a.base, ap);
           e = ltb_launch_pack_conv(j, p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig,
                                    t.b_off32, st);
-          if (e == cudaSuccess && t.epi == 3)  // halo boxes: the tile's rows + kh - 1, full width
+          if (e == cudaSuccess && halo_form(t.epi))  // halo boxes: the tile's rows + kh - 1, full width
             e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.halo.img_slot,
                                     t.halo.img_rows + t.halo.img_kh - 1);
           else if (e == cudaSuccess)
@@ -800,11 +804,11 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           e = ltb_launch_pack(p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig, t.b_off32,
                               c->sms, st);
         if (e == cudaSuccess) e = ltb_make_tmap(maps + 128, bp, p.N, t.Kp, b_box_rows(t));
-        const bool c_tma = t.c_tma && t.epi != 3 && aligned16(p.c + t.c_row0);
+        const bool c_tma = t.c_tma && !halo_form(t.epi) && aligned16(p.c + t.c_row0);
         if (e == cudaSuccess && c_tma)
           e = ltb_make_tmap_c(maps + 512, p.c + t.c_row0, p.M, p.N, t.c_ld);
         if (e == cudaSuccess) {
-          LtbTcProblem one = t.epi == 3 ? t.halo : t.prob;
+          LtbTcProblem one = halo_form(t.epi) ? t.halo : t.prob;
           one.c_tma = c_tma ? 1 : 0;
           one.group_m = t.prob.group_m;
           one.c = p.c;
@@ -877,11 +881,17 @@ void apply_cfg(ltb_compiled* c, int i, const LtbCfg& cfg) {
   if (g >= 0 && c->gemms[g].tc) {
     // variant: tile width | form, form 0: row-store (or TMA-store)
     // epilogue, 1: transposed epilogue, 2: two CTAs per SM (128 wide only),
-    // 3: halo image tiles; 258: 256 x 256 tiles on CTA pairs
+    // 3: halo image tiles, 5: halo image tiles on CTA pairs (133); 258:
+    // 256 x 256 tiles on CTA pairs
     const int v = cfg.variant;
     const int bn = v == 256 || v == 257 || v == 258 ? 256 : 128;
-    const int epi = v == 129 || v == 257 ? 1 : v == 130 ? 2 : v == 131 ? 3 : v == 258 ? 4 : 0;
-    set_tile_n(c->gemms[g], bn, epi);  // 131 and 258 fall back where they do not apply
+    const int epi = v == 129 || v == 257 ? 1
+                    : v == 130              ? 2
+                    : v == 131              ? 3
+                    : v == 258              ? 4
+                    : v == 133              ? 5
+                                            : 0;
+    set_tile_n(c->gemms[g], bn, epi);  // 131, 133 and 258 fall back where they do not apply
     c->cfg[i].variant = variant_code(c->gemms[g]);
     // cta_per_sm of a contraction: the raster group (row blocks swept together)
     c->gemms[g].prob.group_m = cfg.cta_per_sm;
@@ -1106,10 +1116,11 @@ std::string describe(ltb_compiled* c, int i) {
         << (t.epi == 4 ? "" : std::to_string(t.bn) + "x64)")
         << " tensor_cores(tcgen05) parallel(persistent, " << t.tiles << " tiles) raster("
         << (t.prob.group_m ? t.prob.group_m : 16) << " row blocks) epilogue("
-        << (t.c_tma && t.epi != 2 && t.epi != 3 ? "TMA stores where aligned, else " : "")
+        << (t.c_tma && t.epi != 2 && !halo_form(t.epi) ? "TMA stores where aligned, else " : "")
         << (t.epi == 1 ? "smem transpose" : t.epi == 2 ? "row stores, 2 CTAs/SM" : "row stores")
         << ")"
-        << (t.epi == 3 ? " implicit_conv(halo tiles: one 4-D TMA box per tile and channel block, "
+        << (t.epi == 5 ? " on CTA pairs (cta_group::2, M = 256, half the weights per CTA)" : "")
+        << (halo_form(t.epi) ? " implicit_conv(halo tiles: one 4-D TMA box per tile and channel block, "
                          "every (kh, kw) shift read in place; weights resident in shared memory)"
             : t.img   ? " implicit_conv(A from NHWC image via 4-D TMA)"
                       : "");
@@ -1158,7 +1169,10 @@ std::vector<LtbCfg> candidates(ltb_compiled* c, int i) {
         for (int v : {128, 129, 130, 256, 257, 258})
           if (v != 258 || !c->gemms[c->gemm_of[i]].img)
             for (int gm : {0, 8, 32}) buf[n++] = LtbCfg{gm, 0, v};
-        if (c->gemms[c->gemm_of[i]].halo_ok) buf[n++] = LtbCfg{0, 0, 131};
+        if (c->gemms[c->gemm_of[i]].halo_ok) {
+          buf[n++] = LtbCfg{0, 0, 131};
+          buf[n++] = LtbCfg{0, 0, 133};
+        }
       } else {  // CUDA-core tiles
         buf[n++] = LtbCfg{0, 0, 64};
         buf[n++] = LtbCfg{0, 0, 128};
@@ -1528,7 +1542,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         } else {
           CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
         }
-        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, b_box_rows(t)));
+        // (a halo-form member runs the per-row tiles of its width here)
+        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, halo_form(t.epi) ? t.bn : b_box_rows(t)));
         LtbTcProblem q = t.prob;
         q.c_tma = t.c_tma && aligned16(p.c + t.c_row0) ? 1 : 0;
         if (q.c_tma) CUDA_TRY(ltb_make_tmap_c(m + 512, p.c + t.c_row0, p.M, p.N, t.c_ld));
@@ -1539,7 +1554,7 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         q.tile_start = b->tc_tiles[grp];
         // halo tiles are a single-launch form: in a group the member runs
         // its per-row image tiles at the same width
-        b->tc_tiles[grp] += t.epi == 3 ? (int64_t)t.prob.tiles_m * t.prob.tiles_n : t.tiles;
+        b->tc_tiles[grp] += halo_form(t.epi) ? (int64_t)t.prob.tiles_m * t.prob.tiles_n : t.tiles;
         tcp[grp].push_back(q);
       } else {
         if (p.K > kSimtMaxK) throw ltb::Error("contraction too long for the FP32 kernel");

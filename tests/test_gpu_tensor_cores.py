@@ -233,16 +233,24 @@ IMPLICIT = [(2, 64, 8, 8, 16, 3, 1, True), (2, 64, 16, 16, 40, 3, 1, True),
             (2, 32, 16, 16, 16, 3, 1, False)]
 
 
-def _conv_check(c, N, C, H, W, CO, K, pad, dev, tol):
+def _conv_check(c, N, C, H, W, CO, K, pad, dev, tol, batch=False):
+    """Runs c twice (through a one-member Batch with batch=True) and checks
+    the output against torch's FP64 convolution, normwise."""
     import torch
+
+    import loop_tool_b200 as lt
 
     g = torch.Generator(device=dev).manual_seed(N * 1000 + C + H + CO + K)
     x = torch.randn(N * C * H * W, device=dev, generator=g)
     w = torch.randn(CO * C * K * K, device=dev, generator=g) / (C * K * K) ** 0.5
     Ho, Wo = H + 2 * pad - K + 1, W + 2 * pad - K + 1
     y = torch.full((N * Ho * Wo * CO,), float("nan"), device=dev)
+    b = lt.Batch([(c, [x, w, y])]) if batch else None
     for _ in range(2):  # scratch reused: the padded image must be rewritten whole
-        c([x, w, y])
+        if b is not None:
+            b.run()
+        else:
+            c([x, w, y])
     torch.cuda.synchronize()
     ref = torch.nn.functional.conv2d(x.view(N, C, H, W).double(),
                                      w.view(CO, C, K, K).double(), padding=pad)
@@ -281,9 +289,10 @@ def test_conv_implicit_every_variant(variant, cuda_dev):
     _conv_check(c, 2, 64, 16, 16, 40, 3, 1, cuda_dev, TOL["bf16x3"])
 
 
-# Halo image tiles (variant 131, BF16): one TMA box per kernel row covers the
-# tile's padded image rows; the kw shifts are read in place at row offsets
-# inside the 128-byte swizzle atoms; the weights stay in shared memory.
+# Halo image tiles (variant 131, BF16; 133 on CTA pairs): one TMA box per
+# kernel row covers the tile's padded image rows; the kw shifts are read in
+# place at row offsets inside the 128-byte swizzle atoms; the weights stay in
+# shared memory (half of them in each CTA of a pair).
 # Shapes: partial last row group, several images, a 2 x 2 kernel, two
 # channel blocks, and the 56 x 56 image with 128 output channels.
 # (N, C, H, W, CO, K, pad)
@@ -303,6 +312,12 @@ def test_conv_halo_tiles(shape, cuda_dev):
     c.set_schedule(0, variant=131)
     assert c.schedule(0)[2] == 131
     _conv_check(c, N, C, H, W, CO, K, pad, cuda_dev, TOL["bf16"])
+    # the same tiles two to a CTA pair (M = 256, half the weights per CTA)
+    c.set_schedule(0, variant=133)
+    assert c.schedule(0)[2] == 133
+    _conv_check(c, N, C, H, W, CO, K, pad, cuda_dev, TOL["bf16"])
+    # a batch runs a halo-form member as per-row image tiles of its width
+    _conv_check(c, N, C, H, W, CO, K, pad, cuda_dev, TOL["bf16"], batch=True)
     # and back to the per-row image tiles on the same compiled object
     c.set_schedule(0, variant=128)
     assert c.schedule(0)[2] == 128
@@ -321,6 +336,8 @@ def test_conv_halo_not_applicable(cuda_dev):
     c.set_schedule(0, variant=131)
     assert c.schedule(0)[2] == 128
     _conv_check(c, 1, 128, 10, 10, 24, 3, 0, cuda_dev, TOL["bf16"])
+    c.set_schedule(0, variant=133)  # the CTA-pair form likewise
+    assert c.schedule(0)[2] == 128
     T, _ = conv(2, 64, 16, 16, 40, 3, 1, 1)
     c = lt.cuda(T.ir, precision="bf16x3")
     c.set_schedule(0, variant=131)
