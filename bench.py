@@ -828,13 +828,15 @@ NCU_CASES = ("add", "add_2p28", "softmax", "maxpool", "mm_bf16", "mm_bf16x3", "m
              "conv_fp32", "batch_bf16", "mm_bf16_batch")
 
 
-def ncu_case(name, reps, tune=True, schedules=None):
+def ncu_case(name, reps, tune=True, schedules=None, variant=0):
     """One workload at a profiling size (inputs above L2, about 1 GB on the
     device), autotuned as in the benchmark, then run `reps` times inside the
     NVTX range "profile" (capture with ncu --nvtx --nvtx-include profile/).
     With `schedules` (a file path): if the file exists its schedules are
     loaded and nothing is tuned, else the tuned schedules are written there,
-    so a capture under ncu runs what the plain run before it chose."""
+    so a capture under ncu runs what the plain run before it chose.  With
+    `variant`, single-program cases run that launch variant on their first
+    stage instead of tuning (e.g. 133: halo tiles on CTA pairs)."""
     import torch
 
     import loop_tool_b200 as ltb
@@ -897,6 +899,9 @@ def ncu_case(name, reps, tune=True, schedules=None):
     c = ltb.Compiled(ir, **opts)
     bufs = [torch.randn(n, device=dev, generator=g) for n in c.io_sizes[:c.n_inputs]]
     bufs += [torch.empty(n, device=dev) for n in c.io_sizes[c.n_inputs:]]
+    if variant:
+        c.set_schedule(0, variant=variant)
+        tune = False
     if tune:
         print(c.tune(bufs, reps=3))
         if schedules:
@@ -925,6 +930,8 @@ def main():
     ap.add_argument("--ncu-case", choices=NCU_CASES,
                     help="run one workload at a profiling size and exit")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--variant", type=int, default=0,
+                    help="--ncu-case: run this launch variant on the first stage (no tuning)")
     ap.add_argument("--schedules",
                     help="with --ncu-case: schedule file written by a tuning run and loaded "
                          "(no tuning) by a later run, e.g. the same case under ncu")
@@ -932,7 +939,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.ncu_case:
-        return ncu_case(args.ncu_case, args.reps, args.tune, args.schedules)
+        return ncu_case(args.ncu_case, args.reps, args.tune, args.schedules, args.variant)
 
     import torch
 
