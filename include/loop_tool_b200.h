@@ -213,7 +213,9 @@ int ltb_tune(ltb_compiled* c, void* const* memory, int n, void* stream, int reps
  * epilogue, 129 / 257 shared-memory transposed epilogue, 130 two 128-wide
  * CTAs per SM, 131 halo image tiles with resident weights (single-segment
  * convolutions whose weights fit in shared memory; elsewhere it reads back
- * as 128); cta_per_sm is the raster group.  For a CUDA-core (FP32)
+ * as 128), 133 the same halo tiles two to a CTA pair (M = 256, half of the
+ * weights in each CTA; elsewhere 128), 258 256 x 256 tiles on CTA pairs
+ * (plain operands; elsewhere 256); cta_per_sm is the raster group.  For a CUDA-core (FP32)
  * contraction, variant = 64 or 128 is the CTA tile (0: 64 when the problem
  * has at most SMs / 4 tiles of 128 x 128); both give the same bits.  For a
  * pooling reduction, variant 4 runs 4 work items per thread (else 2). */
