@@ -704,6 +704,15 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------- window
+// 8 floats from a 32-byte aligned address, streamed (evict-first): one
+// whole L2 sector per thread and instruction.
+__device__ __forceinline__ void ldcs_v8(const float* p, float* v) {
+  asm volatile("ld.global.cs.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+                 "=f"(v[6]), "=f"(v[7])
+               : "l"(p));
+}
+
 // Small-window reductions of one operand (pooling): out[..., o] folds
 // x[... S*o + q] over q < K and the other reduced dims.  A thread makes 4
 // consecutive outputs; for each outer reduced coordinate it loads the
@@ -779,7 +788,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const float* p = src + base[u] + roff[rc];
-        if (nv[u] == 4 && ((base[u] + roff[rc]) & 3) == 0) {
+        if (N % 8 == 0 && nv[u] == 4 && (reinterpret_cast<uintptr_t>(p) & 31) == 0) {
+          // whole 32-byte sectors: one load per sector, so a warp's
+          // neighbouring spans do not each take half of the same sectors
+#pragma unroll
+          for (int q = 0; q + 8 <= N; q += 8) ldcs_v8(p + q, &span[u][q]);
+        } else if (nv[u] == 4 && ((base[u] + roff[rc]) & 3) == 0) {
 #pragma unroll
           for (int q = 0; q + 4 <= N; q += 4) {
             const float4 t = __ldcs(reinterpret_cast<const float4*>(p + q));
