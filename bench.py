@@ -385,10 +385,12 @@ def headline(args, world, rank, dev):
         s1.record(stream)
         torch.cuda.synchronize()
 
-    # untimed pass of the same pattern first: the staging blocks of steps in
-    # flight on three streams at once are reserved by the stream-ordered
-    # pool here, not mapped inside the timed pass
-    e2e_pass(torch.cuda.Event(), torch.cuda.Event())
+    # untimed passes of the same pattern first (as many as the warm-up
+    # steps): the staging blocks of steps in flight on three streams at once
+    # are reserved by the stream-ordered pool there, not mapped inside the
+    # timed pass
+    for _ in range(max(1, args.warmup)):
+        e2e_pass(torch.cuda.Event(), torch.cuda.Event())
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2e_pass(s0, s1)
     e2e_s = max_over_ranks(s0.elapsed_time(s1) / 1e3 / e2e_steps, dev)
