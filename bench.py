@@ -714,8 +714,9 @@ def extra_c4(dev):
                      "gemm_tflops": flops / (gemm_ms * 1e-3) / 1e12,
                      "launches_per_replay": batch.int_property("launches"),
                      "tiles": tiles,
-                     "tiles_128_256": [batch.int_property("tiles_128"),
-                                       batch.int_property("tiles_256")],
+                     "tiles_128_256_pair": [batch.int_property("tiles_128"),
+                                            batch.int_property("tiles_256"),
+                                            batch.int_property("tiles_pair")],
                      "max_normwise_err_vs_fp64_sampled": max(errs),
                      "rows_checked": "first 8 rows of all 512 members",
                      "max_elementwise_rel_err_vs_fp64": max(

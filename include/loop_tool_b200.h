@@ -155,7 +155,8 @@ int ltb_batch_run_timed(ltb_batch* b, void* stream, float* pack_ms, float* gemm_
  * (capture again). */
 int ltb_batch_set_schedule(ltb_batch* b, int pack_chunk, int pack_cta_per_sm);
 /* "problems", "flops", "launches", "tiles", "tiles_128", "tiles_256",
- * "graph", "pack_chunk", "pack_cta_per_sm". */
+ * "tiles_pair" (256 x 256 tiles on CTA pairs), "graph", "pack_chunk",
+ * "pack_cta_per_sm". */
 int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value);
 int ltb_batch_release(ltb_batch* b);
 

@@ -211,6 +211,23 @@ __device__ __forceinline__ int find_problem(const LtbTcProblem* __restrict__ P, 
   return lo;
 }
 
+// The i-th tile of work unit u (a CTA, or a cluster of two CTAs): from the
+// unit's span of a host-built order when there is one (a batch's
+// longest-first assignment of uneven tiles to units), else tile u + i *
+// step.  False past the unit's last tile.
+__device__ __forceinline__ bool tile_at(const int* __restrict__ order,
+                                        const int* __restrict__ ostart, int64_t u, int64_t step,
+                                        int64_t total, int64_t i, int64_t* t) {
+  if (order) {
+    const int64_t b = ostart[u];
+    if (i >= ostart[u + 1] - b) return false;
+    *t = order[b + i];
+    return true;
+  }
+  *t = u + i * step;
+  return *t < total;
+}
+
 // Grouped raster: tiles advance along M in groups of group_m row blocks (a
 // per-problem schedule, 16 by default), so the ~148 tiles in flight cover a
 // compact block region whose A and B panels stay resident in L2.
@@ -322,7 +339,8 @@ constexpr size_t kHaloBarBytes = (2 * kMaxHaloStages + kMaxHaloKb + 4) * 8 + 8;
 template <int BN, bool kTransposeEpi, int CTAS, bool kHalo = false>
 __global__ void __launch_bounds__(NT, CTAS)
     k_gemm_tc(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
-              float* c_override, int* err, const __grid_constant__ LtbTcProblem single,
+              float* c_override, int* err, const int* __restrict__ order,
+              const int* __restrict__ ostart, const __grid_constant__ LtbTcProblem single,
               const __grid_constant__ CUtensorMap single_a,
               const __grid_constant__ CUtensorMap single_b,
               const __grid_constant__ CUtensorMap single_a2,
@@ -501,7 +519,8 @@ __global__ void __launch_bounds__(NT, CTAS)
     // ------------------------------------------------------------ producer
     uint32_t g = 0;  // k blocks issued by this CTA so far
     bool alive = true;
-    for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
+    for (int64_t i = 0, t;
+         alive && tile_at(order, ostart, blockIdx.x, gridDim.x, total_tiles, i, &t); ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const CUtensorMap* ma =
           probs ? static_cast<const CUtensorMap*>(p.map_a) : &single_a;
@@ -554,7 +573,8 @@ __global__ void __launch_bounds__(NT, CTAS)
     // ---------------------------------------------------------- MMA issuer
     uint32_t g = 0, q = 0;  // k blocks consumed, chunks produced
     bool alive = true;
-    for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
+    for (int64_t i = 0, t;
+         alive && tile_at(order, ostart, blockIdx.x, gridDim.x, total_tiles, i, &t); ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const int nk = (int)((p.Kp + BK - 1) / BK);
       const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
@@ -590,7 +610,8 @@ __global__ void __launch_bounds__(NT, CTAS)
     const int half = (warp - 2) >> 2;     // columns HALF*half .. +HALF-1
     uint32_t q = 0;
     bool alive = true;
-    for (int64_t t = blockIdx.x; t < total_tiles && alive; t += gridDim.x) {
+    for (int64_t i = 0, t;
+         alive && tile_at(order, ostart, blockIdx.x, gridDim.x, total_tiles, i, &t); ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       int m0, n0;
       tile_coords<BN>(p, t - p.tile_start, &m0, &n0);
@@ -769,7 +790,8 @@ __device__ __forceinline__ void pair_coords(const LtbTcProblem& p, int64_t lt, i
 
 __global__ void __launch_bounds__(NT, 1)
     k_gemm_tc_pair(const LtbTcProblem* __restrict__ probs, int nprob, int64_t total_tiles,
-                   int* err, const __grid_constant__ LtbTcProblem single,
+                   int* err, const int* __restrict__ order, const int* __restrict__ ostart,
+                   const __grid_constant__ LtbTcProblem single,
                    const __grid_constant__ CUtensorMap single_a,
                    const __grid_constant__ CUtensorMap single_b,
                    const __grid_constant__ CUtensorMap single_c) {
@@ -814,7 +836,8 @@ __global__ void __launch_bounds__(NT, 1)
     // ------------------------------------------------------------ producer
     uint32_t g = 0;
     bool alive = true;
-    for (int64_t t = first; t < total_tiles && alive; t += step) {
+    for (int64_t i = 0, t; alive && tile_at(order, ostart, first, step, total_tiles, i, &t);
+         ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const CUtensorMap* ma = probs ? static_cast<const CUtensorMap*>(p.map_a) : &single_a;
       const CUtensorMap* mb = probs ? static_cast<const CUtensorMap*>(p.map_b) : &single_b;
@@ -844,7 +867,8 @@ __global__ void __launch_bounds__(NT, 1)
     // ---------------------------------------------------------- MMA issuer
     uint32_t g = 0, q = 0;
     bool alive = true;
-    for (int64_t t = first; t < total_tiles && alive; t += step) {
+    for (int64_t i = 0, t; alive && tile_at(order, ostart, first, step, total_tiles, i, &t);
+         ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const int nk = (int)((p.Kp + BK - 1) / BK);
       const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
@@ -879,7 +903,8 @@ __global__ void __launch_bounds__(NT, 1)
     const int quad = warp & 3, half = (warp - 2) >> 2;
     uint32_t q = 0;
     bool alive = true;
-    for (int64_t t = first; t < total_tiles && alive; t += step) {
+    for (int64_t i = 0, t; alive && tile_at(order, ostart, first, step, total_tiles, i, &t);
+         ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       int m0, n0;
       pair_coords(p, t - p.tile_start, &m0, &n0);
@@ -1801,7 +1826,8 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
                              float* c_override, int sms, int* err, cudaStream_t st,
                              const LtbTcProblem* single, const void* map_a, const void* map_b,
                              const void* map_a2, const void* map_a3, const void* map_c,
-                             bool c_tma_any) {
+                             bool c_tma_any, const int* order = nullptr,
+                             const int* ostart = nullptr) {
   // TMA-stored outputs in this launch: the staging in dynamic shared memory
   const bool tma = !TE && CTAS == 1 && !HALO && (d_probs ? c_tma_any : single && single->c_tma && map_c);
   size_t smem = tma ? Tile<BN, CTAS>::SMEM_TMA : Tile<BN, CTAS>::SMEM;
@@ -1831,7 +1857,8 @@ static cudaError_t launch_tc(const LtbTcProblem* d_probs, int nprob, int64_t tot
     else one.c_tma = 0;
   }
   k_gemm_tc<BN, TE, CTAS, HALO><<<grid, NT, smem, st>>>(d_probs, nprob, total_tiles, c_override,
-                                                        err, one, ma, mb, ma2, ma3, mc);
+                                                        err, order, ostart, one, ma, mb, ma2, ma3,
+                                                        mc);
   return cudaGetLastError();
 }
 
@@ -1867,7 +1894,8 @@ static int pair_clusters(const void* fn, size_t smem, int dev) {
 
 static cudaError_t launch_pair(const LtbTcProblem* d_probs, int nprob, int64_t total_tiles,
                                int* err, cudaStream_t st, const LtbTcProblem* single,
-                               const void* map_a, const void* map_b, const void* map_c) {
+                               const void* map_a, const void* map_b, const void* map_c,
+                               const int* order, const int* ostart) {
   {
     const cudaError_t e = ltb_smem_optin((const void*)k_gemm_tc_pair, kPairSmem);
     if (e != cudaSuccess) return e;
@@ -1902,8 +1930,8 @@ static cudaError_t launch_pair(const LtbTcProblem* d_probs, int nprob, int64_t t
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_gemm_tc_pair, d_probs, nprob, total_tiles, err, one, ma, mb,
-                            mc);
+  return cudaLaunchKernelEx(&cfg, k_gemm_tc_pair, d_probs, nprob, total_tiles, err, order, ostart,
+                            one, ma, mb, mc);
 }
 
 // Halo tiles on CTA pairs: the halo problem with the ring re-sized for the
@@ -1951,15 +1979,32 @@ static cudaError_t launch_pair_halo(int64_t tiles, int* err, cudaStream_t st,
   return cudaLaunchKernelEx(&cfg, k_gemm_tc_pair_halo, pair_tiles, err, one, ma, mb);
 }
 
+int64_t ltb_tc_units(int bn, int64_t total_tiles, int sms) {
+  if (total_tiles <= 0) return 0;
+  int64_t units = (int64_t)sms * (bn == 130 ? 2 : 1);
+  if (bn == 258) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    units = pair_clusters((const void*)k_gemm_tc_pair, kPairSmem, dev);
+  }
+  return total_tiles < units ? total_tiles : units;
+}
+
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single, const void* map_a,
                                const void* map_b, const void* map_a2, const void* map_a3,
-                               const void* map_c, int c_tma_any) {
+                               const void* map_c, int c_tma_any, const int* order,
+                               const int* ostart) {
   if (total_tiles == 0) return cudaSuccess;
+  if (order && bn != 128 && bn != 129 && bn != 256 && bn != 257 && bn != 130 && bn != 258)
+    return cudaErrorInvalidValue;  // an order is for the batch (problem-table) forms
 #define LTB_TC(BN, TE)                                                                      \
   return launch_tc<BN, TE>(d_probs, nprob, total_tiles, c_override, sms, err, st, single, map_a, \
-                           map_b, map_a2, map_a3, map_c, c_tma_any)
+                           map_b, map_a2, map_a3, map_c, c_tma_any, order, ostart)
   switch (bn) {
     case 128: LTB_TC(128, false);
     case 129: LTB_TC(128, true);
@@ -1967,14 +2012,16 @@ cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
     case 257: LTB_TC(256, true);
     case 130:  // 128 wide, two CTAs per SM
       return launch_tc<128, false, 2>(d_probs, nprob, total_tiles, c_override, sms, err, st,
-                                      single, map_a, map_b, map_a2, map_a3, map_c, false);
+                                      single, map_a, map_b, map_a2, map_a3, map_c, false, order,
+                                      ostart);
     case 131:  // 128 wide halo image tiles, resident weights
       return launch_tc<128, false, 1, true>(d_probs, nprob, total_tiles, c_override, sms, err,
                                             st, single, map_a, map_b, map_a2, map_a3, map_c,
                                             false);
     case 258:  // 256 x 256 tiles on CTA pairs (plain operands, B' boxes of 128 rows)
       if (c_override) return cudaErrorInvalidValue;
-      return launch_pair(d_probs, nprob, total_tiles, err, st, single, map_a, map_b, map_c);
+      return launch_pair(d_probs, nprob, total_tiles, err, st, single, map_a, map_b, map_c,
+                         order, ostart);
     case 133:  // halo image tiles on CTA pairs (M = 256, B' boxes of 64 rows)
       if (c_override || d_probs) return cudaErrorInvalidValue;
       return launch_pair_halo(total_tiles, err, st, single, map_a, map_b);

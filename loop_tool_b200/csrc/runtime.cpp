@@ -9,6 +9,7 @@
 #include <limits>
 #include <map>
 #include <mutex>
+#include <queue>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -1393,6 +1394,11 @@ struct ltb_batch {
   int ntc[6] = {0, 0, 0, 0, 0, 0};
   int64_t tc_tiles[6] = {0, 0, 0, 0, 0, 0};
   int tc_tma[6] = {0, 0, 0, 0, 0, 0};  // a problem of the group has a TMA-stored output
+  // each group's tiles dealt longest first to the least-loaded work unit of
+  // its persistent launch (tile_order): unit u runs order[ostart[u] ..
+  // ostart[u + 1])
+  int* d_order[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int* d_ostart[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   LtbGemmProblem* d_simt = nullptr;
   int64_t* d_simt_start = nullptr;
   int64_t simt_tiles = 0;
@@ -1416,12 +1422,54 @@ int group_of(const GemmTables& t) {
   return 0;
 }
 
+// A tile's cost for the assignment: its k blocks plus a fixed share for
+// the drain and epilogue (about 4 k blocks of MMA time, measured on the
+// batch's small-K tiles).
+constexpr int64_t kTileFixedCost = 4;
+
+// Longest-processing-time assignment of a group's tiles (problems in tile
+// order, each with tiles_m x tiles_n tiles of ceil(Kp / 64) k blocks) to
+// `units` work units: tiles by descending cost (stable, so a problem's
+// tiles keep their raster order and run side by side), each to the unit
+// with the least work so far.  Returns the per-unit tile lists
+// concatenated and their start offsets.  Round-robin dealing leaves the
+// slowest unit of the 512-matmul batch ~10% above the mean in a model of
+// these costs; this leaves it at the mean.
+void tile_order(const std::vector<LtbTcProblem>& probs, int64_t units, std::vector<int>* order,
+                std::vector<int>* ostart) {
+  std::vector<int64_t> cost;
+  for (const auto& q : probs) {
+    const int64_t n = (int64_t)q.tiles_m * q.tiles_n, kb = (q.Kp + 63) / 64;
+    cost.insert(cost.end(), (size_t)n, kb + kTileFixedCost);
+  }
+  std::vector<int> idx(cost.size());
+  for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  using Load = std::pair<int64_t, int64_t>;  // (work so far, unit)
+  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+  for (int64_t u = 0; u < units; ++u) heap.push({0, u});
+  std::vector<std::vector<int>> lists((size_t)units);
+  for (int t : idx) {
+    Load l = heap.top();
+    heap.pop();
+    lists[(size_t)l.second].push_back(t);
+    heap.push({l.first + cost[t], l.second});
+  }
+  order->clear();
+  ostart->assign(1, 0);
+  for (const auto& l : lists) {
+    order->insert(order->end(), l.begin(), l.end());
+    ostart->push_back((int)order->size());
+  }
+}
+
 void batch_gemms(ltb_batch* b, cudaStream_t st) {
   for (int g = 0; g < kGroups; ++g)
     if (b->ntc[g])
       CUDA_TRY(ltb_launch_gemm_tc(kGroupCode[g], b->d_tc[g], b->ntc[g], b->tc_tiles[g], nullptr,
                                   b->sms, b->d_err, st, nullptr, nullptr, nullptr, nullptr,
-                                  nullptr, nullptr, b->tc_tma[g]));
+                                  nullptr, nullptr, b->tc_tma[g], b->d_order[g],
+                                  b->d_ostart[g]));
 }
 
 void batch_launch(ltb_batch* b, cudaStream_t st) {
@@ -1583,6 +1631,13 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
         }
         b->ntc[g] = (int)tcp[g].size();
         b->d_tc[g] = upload(tcp[g], b->owned);
+        const int64_t units = ltb_tc_units(kGroupCode[g], b->tc_tiles[g], b->sms);
+        if (b->ntc[g] && units > 0) {
+          std::vector<int> order, ostart;
+          tile_order(tcp[g], units, &order, &ostart);
+          b->d_order[g] = upload(order, b->owned);
+          b->d_ostart[g] = upload(ostart, b->owned);
+        }
       }
     } else {
       b->d_simt = upload(sp, b->owned);
@@ -1713,16 +1768,19 @@ int ltb_batch_int_property(ltb_batch* b, const char* name, int64_t* value) {
   std::string k = name;
   if (k == "problems") *value = b->n;
   else if (k == "flops") *value = (int64_t)b->flops;
-  else if (k == "launches")
-    *value = b->tc ? 1 + (b->ntc[0] > 0) + (b->ntc[1] > 0) + (b->ntc[2] > 0) + (b->ntc[3] > 0) +
-                         (b->ntc[4] > 0)
-                   : 1;
-  else if (k == "tiles")
-    *value = b->tc ? b->tc_tiles[0] + b->tc_tiles[1] + b->tc_tiles[2] + b->tc_tiles[3] +
-                         b->tc_tiles[4]
-                   : b->simt_tiles;
-  else if (k == "tiles_128") *value = b->tc_tiles[0] + b->tc_tiles[1] + b->tc_tiles[4];
+  else if (k == "launches") {  // image repacks, the grouped pack, one per non-empty group
+    int64_t n = b->tc ? 1 + (int64_t)b->img_jobs.size() : 1;
+    if (b->tc)
+      for (int g = 0; g < kGroups; ++g) n += b->ntc[g] > 0;
+    *value = n;
+  } else if (k == "tiles") {
+    int64_t n = b->tc ? 0 : b->simt_tiles;
+    if (b->tc)
+      for (int g = 0; g < kGroups; ++g) n += b->tc_tiles[g];
+    *value = n;
+  } else if (k == "tiles_128") *value = b->tc_tiles[0] + b->tc_tiles[1] + b->tc_tiles[4];
   else if (k == "tiles_256") *value = b->tc_tiles[2] + b->tc_tiles[3];
+  else if (k == "tiles_pair") *value = b->tc_tiles[5];  // 256 x 256 tiles on CTA pairs
   else if (k == "graph") *value = b->exec ? 1 : 0;
   else if (k == "pack_chunk") *value = b->pack_chunk ? b->pack_chunk : 4;
   else if (k == "pack_cta_per_sm")

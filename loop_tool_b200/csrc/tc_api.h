@@ -138,10 +138,18 @@ cudaError_t ltb_launch_pack(const LtbGemmOperand& op, int64_t rows, int64_t K, v
 // (host copies, passed as kernel parameters; no map_c: row stores).
 // c_tma_any: some problem of d_probs has c_tma set (the launch reserves the
 // TMA-store staging).
+// order / ostart (device arrays, batch forms only): the tiles of work unit u
+// (a CTA, or a cluster of two for 258) are order[ostart[u] .. ostart[u+1]),
+// for ltb_tc_units(bn, total_tiles, sms) units; without them unit u takes
+// tiles u, u + units, ...
 cudaError_t ltb_launch_gemm_tc(int bn, const LtbTcProblem* d_probs, int nprob,
                                int64_t total_tiles, float* c_override, int sms, int* err,
                                cudaStream_t st, const LtbTcProblem* single = nullptr,
                                const void* map_a = nullptr, const void* map_b = nullptr,
                                const void* map_a2 = nullptr, const void* map_a3 = nullptr,
-                               const void* map_c = nullptr, int c_tma_any = 0);
+                               const void* map_c = nullptr, int c_tma_any = 0,
+                               const int* order = nullptr, const int* ostart = nullptr);
+// Work units (CTAs, or CTA pairs for 258) of the persistent launch of a
+// batch form over total_tiles tiles on this device.
+int64_t ltb_tc_units(int bn, int64_t total_tiles, int sms);
 int ltb_tc_tile_m();
