@@ -1199,8 +1199,8 @@ __global__ void __launch_bounds__(NT, 1)
 //   kPackDenseK   dense, k-contiguous: float4 loads, 16-byte BF16 stores,
 //                 no shared memory
 //   kPackDenseR   dense, row-contiguous (B[k, n] feeding B'[n, k]): float4
-//                 loads along rows into a shared tile, transposed on the
-//                 way out
+//                 loads along rows into a swizzled shared tile (no bank
+//                 conflicts), transposed on the way out
 //   kPackGatherK / kPackGatherR  guarded gathers (padding, views), lanes
 //                 along k or along rows, through the shared tile
 constexpr int PR = 64, PKT = 64, PACK_THREADS = 256;
@@ -1348,20 +1348,42 @@ __device__ __forceinline__ void pack_tile(const LtbPackJob& J, int64_t lt,
       const int64_t r = r0 + (tid >> 3) + 32 * i, k = k0 + (tid & 7) * 8;
       if (r < J.rows && k < J.K) pack_store8(J, r, k, x[i]);
     }
+  } else if (J.mode == kPackDenseR) {
+    // Transposed through the shared tile viewed as [64 k][64 r] floats with
+    // r stored at r ^ 4 * ((k / 8) % 8): the float4 writes of a quarter-warp
+    // (one k, 32 consecutive r) fill one 128-byte line, and the 8 reads of
+    // a thread (8 consecutive k of one r, k / 8 differing across the warp)
+    // hit 32 distinct banks -- no bank conflicts either way.  Loads: a warp
+    // reads two k rows of 64 contiguous floats; stores: 8 threads write one
+    // row's 64 k (128 bytes of BF16).
+    float* t = &sm[0][0];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = tid + PACK_THREADS * q;
+      const int kl = idx >> 4, rl = (idx & 15) * 4;
+      const int64_t k = k0 + kl, r = r0 + rl;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (k < J.K && r < J.rows)  // rows % 4 == 0 in this mode
+        v = __ldg(reinterpret_cast<const float4*>(J.op.base + k * J.op.ld_k + r));
+      *reinterpret_cast<float4*>(t + kl * 64 + (rl ^ ((kl >> 3) << 2))) = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int c = tid + PACK_THREADS * i;
+      const int rl = c >> 3, kc = c & 7;
+      const int64_t r = r0 + rl, k = k0 + kc * 8;
+      if (r < J.rows && k < J.K) {
+        float x[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) x[e] = t[(kc * 8 + e) * 64 + (rl ^ (kc << 2))];
+        pack_store8(J, r, k, x);
+      }
+    }
+    __syncthreads();  // the next tile overwrites the shared tile
   } else {
     // shared tile sm[k][r], row pitch 65 floats
-    if (J.mode == kPackDenseR) {
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int idx = tid + PACK_THREADS * q;
-        const int kl = idx >> 4, rl = (idx & 15) * 4;
-        const int64_t k = k0 + kl, r = r0 + rl;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (k < J.K && r < J.rows)  // rows % 4 == 0 in this mode
-          v = __ldg(reinterpret_cast<const float4*>(J.op.base + k * J.op.ld_k + r));
-        sm[kl][rl] = v.x; sm[kl][rl + 1] = v.y; sm[kl][rl + 2] = v.z; sm[kl][rl + 3] = v.w;
-      }
-    } else if constexpr (!kDense) {
+    if constexpr (!kDense) {
       // guarded gather: the tile's row and k tables staged in shared memory
       // (offsets and guard partials), so each element costs one global load
       PackTables& tb = *tabs;
