@@ -365,7 +365,7 @@ def headline(args, world, rank, dev):
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 10))
     # device time from the first upload to the last download: each nest runs
     # on its own stream (asynchronous runs on pinned host buffers), so one
     # nest's downloads overlap another's uploads on the host link

@@ -943,7 +943,7 @@ int run_impl(ltb_compiled* c, void* const* memory, int n, int sync,
     }
     if (scratch && (reinterpret_cast<uintptr_t>(scratch) & 255))
       return fail(LTB_ERR_INVALID, "caller scratch must be 256-byte aligned");
-    constexpr int64_t kChunk = int64_t(1) << 24;  // elements per chunk (64 MB of FP32)
+    constexpr int64_t kChunk = int64_t(1) << 23;  // elements per chunk (32 MB of FP32)
     const int64_t total = P.n_out ? P.io_elems[P.n_in] : 0;
     bool same = true;
     for (int i = 0; i < n; ++i) same = same && P.io_elems[i] == total;

@@ -194,7 +194,7 @@ def test_host_buffers_pipelined(op, cuda_dev):
     import loop_tool_b200 as ltb
     import loop_tool_b200.lazy as lt
 
-    n = (1 << 25) + 12344  # two full 2^24 chunks and a ragged third
+    n = (1 << 25) + 12344  # four full 2^23-element chunks and a ragged fifth
     A, B = lt.Tensor(n), lt.Tensor(n)
     N = lt.Symbol("N")
     T = A.to(N) + B.to(N) if op == "add" else A.to(N).exp()
