@@ -786,7 +786,8 @@ cudaError_t launch_stage(ltb_compiled* c, int i, const LtbBufTable& bt, cudaStre
           LtbImageJob j = image_job(t, p.a.base, ap);
           e = ltb_launch_pack_conv(j, p.b, p.N, p.K, bp, t.Kp, t.nseg, t.b_mask, t.b_kcontig,
                                    t.b_off32, st);
-          if (e == cudaSuccess && halo_form(t.epi))  // halo boxes: the tile's rows + kh - 1, full width
+          // halo boxes: the tile's rows + kh - 1, full width
+          if (e == cudaSuccess && halo_form(t.epi))
             e = ltb_make_tmap_image(maps, j.hi, j.nimg, j.hp, j.wp, j.c, t.halo.img_slot,
                                     t.halo.img_rows + t.halo.img_kh - 1);
           else if (e == cudaSuccess)
@@ -1121,10 +1122,11 @@ std::string describe(ltb_compiled* c, int i) {
         << (t.epi == 1 ? "smem transpose" : t.epi == 2 ? "row stores, 2 CTAs/SM" : "row stores")
         << ")"
         << (t.epi == 5 ? " on CTA pairs (cta_group::2, M = 256, half the weights per CTA)" : "")
-        << (halo_form(t.epi) ? " implicit_conv(halo tiles: one 4-D TMA box per tile and channel block, "
-                         "every (kh, kw) shift read in place; weights resident in shared memory)"
-            : t.img   ? " implicit_conv(A from NHWC image via 4-D TMA)"
-                      : "");
+        << (halo_form(t.epi)
+                ? " implicit_conv(halo tiles: one 4-D TMA box per tile and channel block, "
+                  "every (kh, kw) shift read in place; weights resident in shared memory)"
+            : t.img ? " implicit_conv(A from NHWC image via 4-D TMA)"
+                    : "");
     else {
       LtbGemmProblem q{};
       q.M = s.con.M;
@@ -1591,7 +1593,8 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
           CUDA_TRY(ltb_make_tmap(m, ap, p.M, t.Kp, ltb_tc_tile_m()));
         }
         // (a halo-form member runs the per-row tiles of its width here)
-        CUDA_TRY(ltb_make_tmap(m + 128, bp, p.N, t.Kp, halo_form(t.epi) ? t.bn : b_box_rows(t)));
+        CUDA_TRY(
+            ltb_make_tmap(m + 128, bp, p.N, t.Kp, halo_form(t.epi) ? t.bn : b_box_rows(t)));
         LtbTcProblem q = t.prob;
         q.c_tma = t.c_tma && aligned16(p.c + t.c_row0) ? 1 : 0;
         if (q.c_tma) CUDA_TRY(ltb_make_tmap_c(m + 512, p.c + t.c_row0, p.M, p.N, t.c_ld));
