@@ -211,6 +211,19 @@ __device__ __forceinline__ int find_problem(const LtbTcProblem* __restrict__ P, 
   return lo;
 }
 
+// Length of the accumulation chunk that starts at k block c0 of nk:
+// chunk_blocks (0: kChunkBlocks) within the first main_blocks, rest_blocks
+// past them when rest_blocks is set (the main part's last chunk ends with
+// it).  The MMA issuer and the drain warps cut K the same way.
+__device__ __forceinline__ int chunk_len(const LtbTcProblem& p, int c0, int nk) {
+  int len = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
+  if (p.rest_blocks > 0) {
+    if (c0 >= p.main_blocks) len = p.rest_blocks;
+    else if (c0 + len > p.main_blocks) len = p.main_blocks - c0;
+  }
+  return c0 + len < nk ? len : nk - c0;
+}
+
 // The i-th tile of work unit u (a CTA, or a cluster of two CTAs): from the
 // unit's span of a host-built order when there is one (a batch's
 // longest-first assignment of uneven tiles to units), else tile u + i *
@@ -577,8 +590,8 @@ __global__ void __launch_bounds__(NT, CTAS)
          alive && tile_at(order, ostart, blockIdx.x, gridDim.x, total_tiles, i, &t); ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const int nk = (int)((p.Kp + BK - 1) / BK);
-      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
-      for (int c0 = 0; c0 < nk && alive; c0 += cbk, ++q) {
+      for (int c0 = 0, cl = 0; c0 < nk && alive; c0 += cl, ++q) {
+        cl = chunk_len(p, c0, nk);
         const int buf = q & 1;
         if (!mbar_wait(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
           alive = false;
@@ -586,7 +599,7 @@ __global__ void __launch_bounds__(NT, CTAS)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t acc = tmem + (uint32_t)(buf * BN);
-        const int c1 = c0 + cbk < nk ? c0 + cbk : nk;
+        const int c1 = c0 + cl;
         for (int kb = c0; kb < c1; ++kb, ++g) {
           const int s = g % STAGES;
           if (!mbar_wait(smem_u32(&full[s]), (g / STAGES) & 1u, err)) {
@@ -624,8 +637,8 @@ __global__ void __launch_bounds__(NT, CTAS)
       float run[T::HALF];
 #pragma unroll
       for (int i = 0; i < T::HALF; ++i) run[i] = 0.f;
-      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
-      for (int c0 = 0; c0 < nk; c0 += cbk, ++q) {
+      for (int c0 = 0, cl = 0; c0 < nk; c0 += cl, ++q) {
+        cl = chunk_len(p, c0, nk);
         const int buf = q & 1;
         const bool ok = mbar_wait(smem_u32(&chunk_full[buf]), (q >> 1) & 1u, err);
         if (!__all_sync(0xffffffffu, ok)) {
@@ -871,8 +884,8 @@ __global__ void __launch_bounds__(NT, 1)
          ++i) {
       const LtbTcProblem& p = probs ? probs[find_problem(probs, nprob, t)] : single;
       const int nk = (int)((p.Kp + BK - 1) / BK);
-      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
-      for (int c0 = 0; c0 < nk && alive; c0 += cbk, ++q) {
+      for (int c0 = 0, cl = 0; c0 < nk && alive; c0 += cl, ++q) {
+        cl = chunk_len(p, c0, nk);
         const int buf = q & 1;
         if (!mbar_wait_cl(smem_u32(&chunk_empty[buf]), ((q >> 1) & 1u) ^ 1u, err)) {
           alive = false;
@@ -880,7 +893,7 @@ __global__ void __launch_bounds__(NT, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t acc = tmem + (uint32_t)(buf * 256);
-        const int c1 = c0 + cbk < nk ? c0 + cbk : nk;
+        const int c1 = c0 + cl;
         for (int kb = c0; kb < c1; ++kb, ++g) {
           const int s = g % kPairStages;
           if (!mbar_wait_cl(smem_u32(&full[s]), (g / kPairStages) & 1u, err)) {
@@ -916,8 +929,8 @@ __global__ void __launch_bounds__(NT, 1)
       float run[128];
 #pragma unroll
       for (int i = 0; i < 128; ++i) run[i] = 0.f;
-      const int cbk = p.chunk_blocks > 0 ? p.chunk_blocks : kChunkBlocks;
-      for (int c0 = 0; c0 < nk; c0 += cbk, ++q) {
+      for (int c0 = 0, cl = 0; c0 < nk; c0 += cl, ++q) {
+        cl = chunk_len(p, c0, nk);
         const int buf = q & 1;
         const bool ok = mbar_wait_cl(smem_u32(&chunk_full[buf]), (q >> 1) & 1u, err);
         if (!__all_sync(0xffffffffu, ok)) {

@@ -493,6 +493,12 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     // (its inputs' rounding, 2^-9 of each product, outweighs the
     // truncation, ~2^-24 a K=16 step), so a tile is drained once
     e.chunk_blocks = t.nseg >= 6 ? 2 : t.nseg == 1 ? (int)((t.Kp + 63) / 64) : 0;
+    // ... only within its main segment (Ah * Bh, the first K of the packed
+    // K): the five correction segments' products are 2^-8 of those, so
+    // 512-K chunks truncate them no more than the main segment's 128-K
+    // chunks (a CPU model of the arithmetic: the same error, fewer drains)
+    e.main_blocks = t.nseg >= 6 ? (int)((con.K + 63) / 64) : 0;
+    e.rest_blocks = t.nseg >= 6 ? 8 : 0;
     ImageGeom ig;
     if (t.nbatch == 1 && t.Kp == t.nseg * con.K && detect_image(d, A, md, kd, ig)) {
       // implicit GEMM: A' never materialises; the A slot holds the padded

@@ -52,6 +52,11 @@ struct LtbTcProblem {
   // accumulation truncates, so its error grows with the MMA steps of a
   // chunk: the FP32-accurate split modes drain shorter chunks.
   int chunk_blocks;
+  // Past the first main_blocks k blocks, chunks of rest_blocks when set
+  // (0: chunk_blocks throughout): the six-product mode's correction
+  // segments, whose products are 2^-8 of the main segment's and whose
+  // truncation is as far below it, drain in longer chunks.
+  int main_blocks, rest_blocks;
 };
 
 // Repacks an image operand x(n, c, h + off_h, w + off_w) (FP32 at
