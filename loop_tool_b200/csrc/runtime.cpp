@@ -1519,6 +1519,9 @@ int ltb_batch_create(ltb_compiled* const* cs, void* const* const* memories, int 
     b->n = n;
     b->device = cs[0]->device;
     b->sms = cs[0]->sms;
+    // the batch's tables live on (and its launch shapes are asked of) the
+    // members' device, whatever device is current
+    CUDA_TRY(cudaSetDevice(b->device));
     std::vector<LtbPackJob> jobs;
     std::vector<LtbTcProblem> tcp[kGroups];
     std::vector<unsigned char> maps[kGroups];  // five 128-byte CUtensorMaps per problem
