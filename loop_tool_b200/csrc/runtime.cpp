@@ -496,9 +496,11 @@ void build_gemm(ltb_compiled* c, int si, GemmTables& t, Arena& ar) {
     // ... only within its main segment (Ah * Bh, the first K of the packed
     // K): the five correction segments' products are 2^-8 of those, so
     // 512-K chunks truncate them no more than the main segment's 128-K
-    // chunks (a CPU model of the arithmetic: the same error, fewer drains)
-    e.main_blocks = t.nseg >= 6 ? (int)((con.K + 63) / 64) : 0;
-    e.rest_blocks = t.nseg >= 6 ? 8 : 0;
+    // chunks (a CPU model of the arithmetic: the same error, fewer drains);
+    // ×3 / ×4, whose error is that of the products they drop, keep 512-K
+    // chunks on the main segment and drain their corrections every 4096 K
+    e.main_blocks = t.nseg >= 3 ? (int)((con.K + 63) / 64) : 0;
+    e.rest_blocks = t.nseg >= 6 ? 8 : t.nseg >= 3 ? 64 : 0;
     ImageGeom ig;
     if (t.nbatch == 1 && t.Kp == t.nseg * con.K && detect_image(d, A, md, kd, ig)) {
       // implicit GEMM: A' never materialises; the A slot holds the padded
