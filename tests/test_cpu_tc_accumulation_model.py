@@ -112,3 +112,26 @@ def test_model_matches_the_measured_128_cube():
     over, normwise = _errors(_emulate(A, B, [128] * 6), exact, ref)
     assert abs(normwise - 1.3e-7) < 0.13e-7 * 1.5, normwise
     assert 5 <= over <= 40, over
+
+
+def test_three_product_corrections_drain_every_4096():
+    """Split-BF16 x3 (A' = [Ah|Al|Ah], B' = [Bh|Bh|Bl]): its error is that of
+    the products it drops (Al.Bl and below), so draining the two correction
+    segments every 4096 K instead of every 512 K leaves it unchanged."""
+    M = N = 64
+    K = 2048
+    rng = np.random.default_rng(7)
+    a = rng.standard_normal((M, K)).astype(np.float32)
+    b = rng.standard_normal((K, N)).astype(np.float32)
+    exact = a.astype(np.float64) @ b.astype(np.float64)
+    ref = np.zeros((M, N), np.float32)
+    for k in range(K):
+        ref = (ref + np.outer(a[:, k], b[k]).astype(np.float32)).astype(np.float32)
+    ah, al, _ = _split3(a)
+    bh, bl, _ = _split3(b)
+    A = np.concatenate([ah, al, ah], axis=1)
+    B = np.concatenate([bh, bh, bl], axis=0)
+    uniform = _errors(_emulate(A, B, [512] * (3 * K // 512)), exact, ref)
+    split = _errors(_emulate(A, B, [512] * (K // 512) + [4096]), exact, ref)
+    assert abs(split[1] - uniform[1]) <= 0.01 * uniform[1], (split, uniform)
+    assert abs(split[0] - uniform[0]) <= 0.01 * uniform[0] + 2, (split, uniform)
