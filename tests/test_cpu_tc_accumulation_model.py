@@ -1,11 +1,12 @@
 """A numpy model of the tensor-core contraction's arithmetic in the
-six-product split mode, used to choose how often the TMEM accumulator is
-drained (loop_tool_b200/csrc/gemm_tc.cu, LtbTcProblem::chunk_blocks,
-main_blocks, rest_blocks).
+split-BF16 modes (six products, and three), used to choose how often the
+TMEM accumulator is drained (loop_tool_b200/csrc/gemm_tc.cu,
+LtbTcProblem::chunk_blocks, main_blocks, rest_blocks).
 
-The model: every FP32 operand value is split into three BF16 pieces (hi, lo,
-lo2, round to nearest even); the packed K holds six segments (Ah.Bh, Al.Bh,
-Ah.Bl, Al.Bl, Al2.Bh, Ah.Bl2); each tcgen05 K = 16 step adds its products
+The model: every FP32 operand value is split into BF16 pieces (hi, lo, lo2,
+round to nearest even); the packed K holds the modes' segments (six: Ah.Bh,
+Al.Bh, Ah.Bl, Al.Bl, Al2.Bh, Ah.Bl2; three: Ah.Bh, Al.Bh, Ah.Bl); each
+tcgen05 K = 16 step adds its products
 (exact) to the FP32 accumulator and truncates toward zero, the behaviour
 measured on B200 (error growing linearly with the steps of a chunk); each
 finished chunk is added into a round-to-nearest FP32 running sum.  Against
