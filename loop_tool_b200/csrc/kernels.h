@@ -80,7 +80,8 @@ struct LtbGemmProblem {
   int64_t M, N, K;
 };
 
-// FP32 CUDA-core path (exact fp32 FMA): the "plain FP32" baseline family.
+// FP32 CUDA-core path (every multiply and add rounded on its own, in k
+// order: the reference C path's arithmetic): the "plain FP32" family.
 // Operand tile loader forms (gemm_simt.cu); ltb_simt_mode picks the fastest
 // one the operand's layout allows.
 enum { kSimtGather = 0, kSimtVecK = 1, kSimtVecR = 2, kSimtGatherT = 3 };
