@@ -18,14 +18,15 @@
 // Chunked accumulation.  The tensor core's FP32 accumulation truncates, so
 // its error grows linearly with the number of K steps summed into one TMEM
 // accumulator (measured: ~1.9e-5 relative at K = 16384 with BF16-exact
-// inputs).  The K loop is therefore cut into chunks (512 elements, fewer
-// for the six-product split mode, the whole K for plain BF16, whose input
-// rounding outweighs the truncation by far: LtbTcProblem::chunk_blocks), each
-// accumulated from zero in one of two TMEM buffers; drain warps read a
-// finished chunk back (16 columns per tcgen05.ld) and add it into FP32
-// registers with round-to-nearest adds while the tensor core fills the other
-// buffer.  The split-BF16 correction segments land in their own chunks, so
-// they are never truncated against the much larger main product.
+// inputs).  The K loop is therefore cut into chunks, each accumulated from
+// zero in one of two TMEM buffers (LtbTcProblem::chunk_blocks, main_blocks,
+// rest_blocks; chunk_len): the whole K for plain BF16, whose input rounding
+// outweighs the truncation by far; for the split modes, short chunks on the
+// main segment (Ah.Bh: 512 K, 128 K in the six-product mode) and long ones
+// (4096 K, 512 K) on the correction segments, whose products are 2^-8 of
+// the main ones.  Drain warps read a finished chunk back (16 columns per
+// tcgen05.ld) and add it into FP32 registers with round-to-nearest adds
+// while the tensor core fills the other buffer.
 //
 // Tile forms (a tuned schedule): 128 x 256 or 128 x 128 output tiles, one CTA
 // per SM (4- or 6-stage ring), or two 128 x 128 CTAs per SM (3-stage rings);
